@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark: T127 L20 spectral-transform round trips/s and radiation columns/s.
+
+One step = one pass of the gridpointa transform set (plasim.f90:2396-2486)
+over a batch of B independent T127 L20 model states (the inverse set:
+dv2uv + sp2fc x4L + sp2fc/sp2fcdmu(ln ps) + i*m d/dlambda + fc2gp of 6L+3
+fields; then the forward set: gp2fc of 9L+1 fields + fc2sp + mktend + qtend),
+on synthetic seeded inputs already resident in HBM.  value = round trips/s
+summed over all ranks (weak scaling: every rank runs its own B instances;
+the instances are independent, so there is no collective on the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+The reference arm (--impl reference) times the FP64 CPU restatement of the
+reference's legmod/fftmod (the Fortran itself cannot be compiled on these
+hosts) on all host cores, on the same workload, and prints the same line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NLAT, NLEV = 192, 20           # T127 L20: 192 x 384 Gaussian grid
+RAD_NLAT, RAD_NLEV = 64, 20    # radiation: T42 grid, 8192 columns, L20
+WORKLOAD = "T127 L20 gridpointa transform round trip (inverse + forward set)"
+
+
+def fp32_round_trip_bytes(nlat, nlev):
+    """Algorithmic bytes of one round trip at FP32: spectral in+out and grid out+in."""
+    ntru = (2 * nlat - 1) // 3
+    nrsp = (ntru + 1) * (ntru + 2)
+    nhor = nlat * 2 * nlat
+    return 2 * (4 * nlev + 1) * nrsp * 4 + (15 * nlev + 4) * nhor * 4
+
+
+def legendre_flops(nlat, nlev):
+    """Algorithmic folded Legendre flops of one round trip: (19L+3) * 2 NLAT NCSP."""
+    ntru = (2 * nlat - 1) // 3
+    ncsp = (ntru + 1) * (ntru + 2) // 2
+    return (19 * nlev + 3) * 2 * nlat * ncsp
+
+
+def args_():
+    a = argparse.ArgumentParser()
+    a.add_argument("--gpus", type=int, default=1)
+    a.add_argument("--steps", type=int, default=20)
+    a.add_argument("--warmup", type=int, default=5)
+    a.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    a.add_argument("--batch", type=int, default=8, help="T127 L20 instances per step and rank")
+    a.add_argument("--no-cpu-baseline", action="store_true")
+    return a.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_sample(rounds=1):
+    """FP64 oracle (C restatement of legmod/fftmod, OpenMP) on the same workload."""
+    from oracle import oracle as O
+    from exoplasim_b200 import synthetic as S
+    L = O.Leg(NLAT)
+    spin = S.transform_state(L.ntru, NLEV, seed=3, kind="steep")
+    gin = S.grid_tendencies(NLAT, NLEV, seed=4).reshape(9 * NLEV + 1, -1)
+    t0 = time.perf_counter()
+    for _ in range(rounds):
+        L.inverse_set(spin, NLEV, plavor=S.EZ)
+        L.forward_set(gin, NLEV)
+    dt = time.perf_counter() - t0
+    return rounds / dt, dt, O.lib().oracle_num_threads()
+
+
+def run_reference(a, rank):
+    if rank != 0:
+        return
+    rounds_per_step = 1
+    rates = []
+    for _ in range(a.warmup):
+        cpu_baseline_sample(rounds_per_step)
+    t_all = 0.0
+    for _ in range(a.steps):
+        r, dt, threads = cpu_baseline_sample(rounds_per_step)
+        rates.append(r)
+        t_all += dt
+    value = a.steps * rounds_per_step / t_all
+    line = {
+        "impl": "reference", "metric": "T127 L20 transform round-trips/s", "value": value,
+        "unit": "round-trips/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1000.0 * t_all / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, BASELINE config shapes)",
+        "config": {"workload": WORKLOAD, "batch": rounds_per_step, "nlat": NLAT, "nlon": 2 * NLAT,
+                   "ntru": (2 * NLAT - 1) // 3, "nlev": NLEV},
+        "cpu_baseline": {"value": value, "unit": "round-trips/s", "cores": threads, "kind": "port",
+                         "sample": f"{rounds_per_step} T127 L20 round trip(s) per step, FP64 C restatement "
+                                   f"of legmod/fftmod (gfortran absent), OpenMP over levels and rows"},
+        "e2e": {"value": value, "unit": "round-trips/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def relerr_fields(a, b):
+    a = a.double().reshape(a.shape[0], -1)
+    b = b.double().reshape(b.shape[0], -1)
+    num = (a - b).abs().amax(dim=1)
+    den = b.abs().amax(dim=1).clamp_min(1e-300)
+    return float((num / den).max())
+
+
+def run_ours(a, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from exoplasim_b200 import radiation as R
+    from exoplasim_b200 import synthetic as S
+    from exoplasim_b200.transforms import Plan, launch_count
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    B = a.batch
+    plan = Plan(NLAT)
+    spin64 = torch.as_tensor(S.transform_state(plan.ntru, NLEV, seed=3 + rank, kind="steep"), device=dev)
+    gin64 = torch.as_tensor(S.grid_tendencies(NLAT, NLEV, seed=4 + rank), device=dev)
+
+    def make(dtype):
+        spin = [spin64.to(dtype).clone() for _ in range(B)]
+        gin = [gin64.to(dtype).clone() for _ in range(B)]
+        gout = [plan.grid(6 * NLEV + 3, "fp64" if dtype == torch.float64 else "fp32") for _ in range(B)]
+        sout = [plan.spectral(4 * NLEV + 1, "fp64" if dtype == torch.float64 else "fp32") for _ in range(B)]
+        return spin, gin, gout, sout
+
+    def step_fn(prec, bufs):
+        spin, gin, gout, sout = bufs
+
+        def f():
+            for i in range(B):
+                plan.inverse_set(spin[i], NLEV, precision=prec, out=gout[i])
+                plan.forward_set(gin[i], NLEV, precision=prec, out=sout[i])
+        return f
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def time_graph(fn, steps, warmup):
+        fn()  # eager call: allocates work buffers and FFT tables outside capture
+        torch.cuda.synchronize()
+        n0 = launch_count()
+        fn()
+        torch.cuda.synchronize()
+        per_step = launch_count() - n0
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                fn()
+        torch.cuda.current_stream().wait_stream(s)
+        for _ in range(warmup):
+            g.replay()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        del g
+        return ms, per_step
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    # FP64 reference outputs for the error columns
+    b64 = make(torch.float64)
+    step_fn("fp64", b64)()
+    torch.cuda.synchronize()
+    ref_gout, ref_sout = b64[2][0].clone(), b64[3][0].clone()
+    precisions = ["fp32", "fp64"]
+    try:
+        from exoplasim_b200 import _lib
+        bm = make(torch.float32)
+        step_fn("mixed", bm)()
+        torch.cuda.synchronize()
+        precisions = ["mixed"] + precisions
+    except Exception as e:  # the tensor-core path is optional until built
+        results["mixed_unavailable"] = str(e)
+    clocks = Clocks(local_rank)
+    for prec in precisions:
+        bufs = b64 if prec == "fp64" else make(torch.float32)
+        fn = step_fn(prec, bufs)
+        if prec == precisions[0]:
+            clocks.start()
+        ms, per_step = time_graph(fn, a.steps, a.warmup)
+        if prec == precisions[0]:
+            clk = clocks.stop()
+        ms = max_over_ranks(ms)
+        err_g = relerr_fields(bufs[2][0], ref_gout) if prec != "fp64" else 0.0
+        err_s = relerr_fields(bufs[3][0], ref_sout) if prec != "fp64" else 0.0
+        results[prec] = {"ms_per_step": ms / a.steps, "round_trips_per_s": world * B * a.steps / (ms / 1000.0),
+                         "launches_per_step": per_step, "max_rel_err_vs_fp64": max(err_g, err_s)}
+        del bufs
+    primary = precisions[0]
+
+    # per-stage timing of the primary precision (dominant stage for the roofline)
+    bufs = make(torch.float32) if primary != "fp64" else make(torch.float64)
+    inv_ms, _ = time_graph(lambda: [plan.inverse_set(bufs[0][i], NLEV, primary, out=bufs[2][i]) for i in range(B)],
+                           a.steps, a.warmup)
+    fwd_ms, _ = time_graph(lambda: [plan.forward_set(bufs[1][i], NLEV, primary, out=bufs[3][i]) for i in range(B)],
+                           a.steps, a.warmup)
+    hbm, tc, peak_kind = peaks()
+    ntru = plan.ntru
+    nrsp = plan.nrsp
+    nhor = plan.nhor
+    esz = 4 if primary != "fp64" else 8
+    inv_bytes = ((4 * NLEV + 1) * nrsp + (6 * NLEV + 3) * nhor) * esz
+    fwd_bytes = ((4 * NLEV + 1) * nrsp + (9 * NLEV + 1) * nhor) * esz
+    if fwd_ms >= inv_ms:
+        dom, dom_ms, dom_bytes = "forward_set", fwd_ms / (a.steps * B), fwd_bytes
+    else:
+        dom, dom_ms, dom_bytes = "inverse_set", inv_ms / (a.steps * B), inv_bytes
+    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
+    del bufs
+
+    # end to end through the public API with host buffers
+    dtype = torch.float32 if primary != "fp64" else torch.float64
+    h_spin = [spin64.to(dtype).cpu().pin_memory() for _ in range(B)]
+    h_gin = [gin64.to(dtype).cpu().pin_memory() for _ in range(B)]
+    bufs = make(dtype)
+    h_gout = [torch.empty_like(bufs[2][0], device="cpu").pin_memory() for _ in range(B)]
+    h_sout = [torch.empty_like(bufs[3][0], device="cpu").pin_memory() for _ in range(B)]
+
+    def e2e_step():
+        for i in range(B):
+            bufs[0][i].copy_(h_spin[i], non_blocking=True)
+            bufs[1][i].copy_(h_gin[i], non_blocking=True)
+            plan.inverse_set(bufs[0][i], NLEV, primary, out=bufs[2][i])
+            plan.forward_set(bufs[1][i], NLEV, primary, out=bufs[3][i])
+            h_gout[i].copy_(bufs[2][i], non_blocking=True)
+            h_sout[i].copy_(bufs[3][i], non_blocking=True)
+
+    for _ in range(a.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    h2d = B * (h_spin[0].numel() + h_gin[0].numel()) * esz
+    d2h = B * (h_gout[0].numel() + h_sout[0].numel()) * esz
+    del bufs, h_spin, h_gin, h_gout, h_sout
+
+    # radiation column pass: 8192 columns at L20 (T42 grid), plain kernel
+    cols, g = S.radiation_columns(RAD_NLAT, RAD_NLEV, seed=2 + rank)
+    rad = {}
+    for rprec, rdt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        dev_cols = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=rdt, device=dev) for k, v in cols.items()}
+        params = R.default_params(RAD_NLEV, g["nhor"], g["nlon"], nsol=0)
+        outs = R.alloc_outputs(params, rdt)
+        ms, _ = time_graph(lambda: R.radstep(params, dev_cols, outs, precision=rprec), a.steps, a.warmup)
+        ms = max_over_ranks(ms)
+        rad[rprec] = {"cols_per_s": world * g["nhor"] * a.steps / (ms / 1000.0), "ms_per_pass": ms / a.steps}
+
+    if world > 1:
+        dist.barrier()
+    if rank != 0:
+        return
+    cpu = None
+    if not a.no_cpu_baseline and world == 1:
+        r, dt, threads = cpu_baseline_sample(1)
+        if dt < 10.0:
+            n = max(1, int(15.0 / dt))
+            r, dt, threads = cpu_baseline_sample(n)
+        cpu = {"value": r, "unit": "round-trips/s", "cores": threads, "kind": "port",
+               "sample": f"{max(1, round(r * dt))} T127 L20 round trip(s) in {dt:.1f} s, FP64 C restatement of "
+                         f"legmod/fftmod with OpenMP (gfortran absent, reference not buildable)"}
+    prim = results[primary]
+    line = {
+        "metric": "T127 L20 transform round-trips/s (mixed vs FP32 @<=1e-6 rel); radiation cols/s",
+        "value": prim["round_trips_per_s"], "unit": "round-trips/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": prim["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if primary != "fp64" else "f64",
+        "data": "synthetic (seeded spectra ~1/(n(n+1)), n^-3 beyond n=10; grid tendencies N(0,1e-5^2))",
+        "config": {"workload": WORKLOAD, "precision": primary, "batch_per_gpu": B, "nlat": NLAT,
+                   "nlon": 2 * NLAT, "ntru": (2 * NLAT - 1) // 3, "nlev": NLEV,
+                   "l2": f"inputs larger than L2: {B} instances x {fp32_round_trip_bytes(NLAT, NLEV) / 1e6:.0f} MB",
+                   "parallelism": f"replicas x{world} (independent instances)"},
+        "precisions": results,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": dom_bytes},
+        "stages_ms_per_instance": {"inverse_set": inv_ms / (a.steps * B), "forward_set": fwd_ms / (a.steps * B)},
+        "e2e": {"value": world * B * a.steps / (e2e_ms / 1000.0), "unit": "round-trips/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "radiation": {"metric": "radiation cols/s (T42 grid, 8192 columns, L20, plain radmod kernel)", **rad},
+        "clocks": clk,
+        "gpu_launches": prim["launches_per_step"] * a.steps,
+        "cpu_baseline": cpu,
+        "legendre_gflop_per_round_trip": legendre_flops(NLAT, NLEV) / 1e9,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = args_()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(a, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

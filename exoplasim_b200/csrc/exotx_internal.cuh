@@ -1,0 +1,120 @@
+// Internal declarations shared by the libexotx translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include "exotx.h"
+
+#define EXOTX_API extern "C" __attribute__((visibility("default")))
+
+namespace exotx {
+
+// Counts every kernel launch the library issues (reported through
+// exotx_launch_count so callers can tell the native path ran).
+void note_launch(unsigned n = 1);
+
+inline exotx_status cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return EXOTX_OK;
+    if (e == cudaErrorMemoryAllocation) return EXOTX_NO_MEM;
+    return EXOTX_CUDA_ERR;
+}
+
+#define EXOTX_CHECK_LAUNCH()                                        \
+    do {                                                            \
+        ::exotx::note_launch();                                     \
+        cudaError_t e_ = cudaGetLastError();                        \
+        if (e_ != cudaSuccess) return ::exotx::cuda_status(e_);     \
+    } while (0)
+
+#define EXOTX_TRY(expr)                                             \
+    do {                                                            \
+        exotx_status st_ = (expr);                                  \
+        if (st_ != EXOTX_OK) return st_;                            \
+    } while (0)
+
+#define EXOTX_CUDA(expr)                                            \
+    do {                                                            \
+        cudaError_t e_ = (expr);                                    \
+        if (e_ != cudaSuccess) return ::exotx::cuda_status(e_);     \
+    } while (0)
+
+// Real FFT twiddle tables for one length n, owned by a process-wide cache.
+struct FftTables {
+    int n = 0, h = 0;            // h = n/2 complex points
+    int nfac = 0, fac[16] = {};  // radix schedule of h (product = h)
+    double *w64 = nullptr;       // e^{-2 pi i k / h}, k < h   (complex, interleaved)
+    float *w32 = nullptr;
+    double *r64 = nullptr;       // e^{-2 pi i k / n}, k <= h  (complex, interleaved)
+    float *r32 = nullptr;
+};
+// Returns nullptr (and sets *st) if n is unsupported or allocation fails.
+const FftTables *fft_tables(int n, exotx_status *st);
+
+// Mixed-precision table copies built on first use (see legendre_tc.cu).
+struct TcTables;
+
+}  // namespace exotx
+
+struct exotx_plan_s {
+    exotx_grid_desc desc;
+    int nlat, nlon, ntru, ntp1, ncsp, nlath;
+    int kmax;                     // max modes per m = ntp1
+    int *d_woff = nullptr;        // first mode index of each m, [ntp1+1]
+    double *d_sid = nullptr, *d_gwd = nullptr;
+    double *d_qref = nullptr;     // 8 tables, reference layout q(NCSP,NLAT) [t][lat][w]
+    // inverse tables qi,qj,qu,qv for northern latitudes, [t][w][j] (j fastest)
+    double *d_inv64 = nullptr;
+    float *d_inv32 = nullptr;
+    // forward tables qc,qe,qm,qq for northern latitudes, per m block [t][woff*nlath + j*K + (n-m)]
+    double *d_fwd64 = nullptr;
+    float *d_fwd32 = nullptr;
+    double *d_fs64 = nullptr, *d_fg64 = nullptr;  // skspgp, skgpsp [ntp1]
+    float *d_fs32 = nullptr, *d_fg32 = nullptr;
+    // work buffer for the forward transform set (Fourier rows of gpin)
+    void *d_work = nullptr;
+    size_t work_bytes = 0;
+    exotx::TcTables *tc = nullptr;
+};
+
+namespace exotx {
+// table indices inside d_inv* and d_fwd*
+enum { INV_QI = 0, INV_QJ = 1, INV_QU = 2, INV_QV = 3 };
+enum { FWD_QC = 0, FWD_QE = 1, FWD_QM = 2, FWD_QQ = 3 };
+
+exotx_status ensure_work(exotx_plan p, size_t bytes);
+
+// Fourier-side addressing: complex element (field f, latitude l, wavenumber m)
+// at base + f*fs + l*ls + m*ms (complex units); m < mz are produced.
+struct FourierLayout {
+    long long fs, ls, ms;
+    int mz;
+};
+
+// op codes
+enum { OP_SP2FC = 0, OP_SP2FCDMU = 1, OP_DV2UV = 2, OP_SP2FC_GPMT = 3 };
+enum { OP_FC2SP = 0, OP_UV2DV = 1, OP_QTEND = 2, OP_MKTEND = 3 };
+
+// SIMT Legendre launchers (legendre_simt.cu)
+template <typename T>
+exotx_status leg_inverse_l(exotx_plan p, int op, const T *a, const T *b, T *oa, T *ob, int nlev,
+                           long long a_fs, long long b_fs, FourierLayout L, cudaStream_t s);
+template <typename T>
+exotx_status leg_forward_l(exotx_plan p, int op, const T *const *in, T *const *out, int nlev,
+                           FourierLayout L, long long o_fs, cudaStream_t s);
+
+// FFT launchers (fft.cu).  kf = Fourier coefficients read (inverse) or
+// written (forward) per row; the rest are zero.  Fourier side addressed as
+// row r, wavenumber k at r*f_rs + k*f_ms (complex units).
+template <typename T>
+exotx_status fft_forward_l(const T *in, T *out, int n, long long lot, int kout, long long f_rs, long long f_ms,
+                           cudaStream_t s);
+template <typename T>
+exotx_status fft_inverse_l(const T *in, T *out, int n, long long lot, int kin, long long f_rs, long long f_ms,
+                           cudaStream_t s);
+
+// tensor-core Legendre (legendre_tc.cu)
+exotx_status tc_inverse_set(exotx_plan p, const float *spin, float *four, int nlev, cudaStream_t s);
+exotx_status tc_forward_set(exotx_plan p, const float *four, float *spout, int nlev, cudaStream_t s);
+exotx_status tc_available();
+void tc_free(exotx_plan p);
+}  // namespace exotx

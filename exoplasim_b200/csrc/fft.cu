@@ -1,0 +1,369 @@
+// Real FFTs of grid rows with the reference's conventions (fftmod.f90,
+// fft991mod.f90:147-155):
+//   forward  c_k = (1/n) sum_j x_j e^{-2 pi i jk/n},  stored (A0, 0, A1, B1, ...),
+//            k < n/2 (the Nyquist term is not stored)
+//   inverse  x_j = A0 + 2 sum_{k=1}^{n/2-1} Re(c_k e^{+2 pi i jk/n}), B0 ignored.
+// A length-n real row is transformed as a length-h = n/2 complex sequence
+// z_j = x_{2j} + i x_{2j+1} with a self-sorting (Stockham) mixed-radix FFT in
+// shared memory, plus the usual even/odd split twiddle e^{-2 pi i k/n}.
+// One block transforms R rows; loads and stores of the grid side are
+// row-contiguous and coalesced.  The Fourier side may be row-major (the
+// reference layout) or m-major (the transform sets' intermediate).
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <vector>
+#include "exotx_internal.cuh"
+
+namespace exotx {
+
+template <typename T> struct cpx { T x, y; };
+template <typename T> __device__ __forceinline__ cpx<T> cmul(cpx<T> a, cpx<T> b) {
+    return cpx<T>{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename T> __device__ __forceinline__ cpx<T> cadd(cpx<T> a, cpx<T> b) { return cpx<T>{a.x + b.x, a.y + b.y}; }
+template <typename T> __device__ __forceinline__ cpx<T> csub(cpx<T> a, cpx<T> b) { return cpx<T>{a.x - b.x, a.y - b.y}; }
+// multiply by e^{sign * i pi/2}: sign=-1 -> -i, sign=+1 -> +i
+template <typename T, int S> __device__ __forceinline__ cpx<T> rot90(cpx<T> a) {
+    return S < 0 ? cpx<T>{a.y, -a.x} : cpx<T>{-a.y, a.x};
+}
+
+// R-point DFT in registers, V[q] = sum_r v[r] e^{S 2 pi i rq/R}
+template <typename T, int S> __device__ __forceinline__ void dft2(cpx<T> *v) {
+    cpx<T> a = v[0], b = v[1];
+    v[0] = cadd(a, b); v[1] = csub(a, b);
+}
+template <typename T, int S> __device__ __forceinline__ void dft4(cpx<T> *v) {
+    cpx<T> a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    cpx<T> b0 = cadd(v[1], v[3]), b1 = rot90<T, S>(csub(v[1], v[3]));
+    v[0] = cadd(a0, b0); v[2] = csub(a0, b0);
+    v[1] = cadd(a1, b1); v[3] = csub(a1, b1);
+}
+template <typename T, int S> __device__ __forceinline__ void dft8(cpx<T> *v) {
+    const T r = (T)0.70710678118654752440084436210484903928;
+    cpx<T> e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<T, S>(e);
+    dft4<T, S>(o);
+    // twiddles e^{S 2 pi i q/8}, q = 0..3
+    cpx<T> t1 = S < 0 ? cpx<T>{r * (o[1].x + o[1].y), r * (o[1].y - o[1].x)}
+                      : cpx<T>{r * (o[1].x - o[1].y), r * (o[1].y + o[1].x)};
+    cpx<T> t2 = rot90<T, S>(o[2]);
+    cpx<T> t3 = S < 0 ? cpx<T>{r * (-o[3].x + o[3].y), r * (-o[3].y - o[3].x)}
+                      : cpx<T>{r * (-o[3].x - o[3].y), r * (-o[3].y + o[3].x)};
+    v[0] = cadd(e[0], o[0]); v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], t1);   v[5] = csub(e[1], t1);
+    v[2] = cadd(e[2], t2);   v[6] = csub(e[2], t2);
+    v[3] = cadd(e[3], t3);   v[7] = csub(e[3], t3);
+}
+template <typename T, int S> __device__ __forceinline__ void dft3(cpx<T> *v) {
+    const T c = (T)-0.5, s = (T)(S * 0.86602540378443864676372317075293618347);
+    cpx<T> t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+    cpx<T> m0 = v[0];
+    cpx<T> a{m0.x + c * t.x, m0.y + c * t.y};
+    cpx<T> b{-s * d.y, s * d.x};  // i*s*d
+    v[0] = cadd(m0, t);
+    v[1] = cadd(a, b);
+    v[2] = csub(a, b);
+}
+template <typename T, int S> __device__ __forceinline__ void dft5(cpx<T> *v) {
+    const T c1 = (T)0.30901699437494742410229341718281905886, c2 = (T)-0.80901699437494742410229341718281905886;
+    const T s1 = (T)(S * 0.95105651629515357211643933337938214340), s2 = (T)(S * 0.58778525229247312916870595463907276860);
+    cpx<T> t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    cpx<T> d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+    cpx<T> a1{v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y};
+    cpx<T> a2{v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y};
+    // i*(s1 d1 + s2 d2) and i*(s2 d1 - s1 d2)
+    cpx<T> b1{-(s1 * d1.y + s2 * d2.y), s1 * d1.x + s2 * d2.x};
+    cpx<T> b2{-(s2 * d1.y - s1 * d2.y), s2 * d1.x - s1 * d2.x};
+    v[0] = cadd(v[0], cadd(t1, t2));
+    v[1] = cadd(a1, b1); v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2); v[3] = csub(a2, b2);
+}
+
+template <typename T, int S, int R>
+__device__ __forceinline__ void dftR(cpx<T> *v) {
+    if (R == 2) dft2<T, S>(v);
+    else if (R == 3) dft3<T, S>(v);
+    else if (R == 4) dft4<T, S>(v);
+    else if (R == 5) dft5<T, S>(v);
+    else dft8<T, S>(v);
+}
+
+// One Stockham pass over all rows of the block: src -> dst.
+template <typename T, int S, int R>
+__device__ void stockham_pass(const cpx<T> *src, cpx<T> *dst, int h, int ns, int rows,
+                              const cpx<T> *wtab) {
+    const int nq = h / R;
+    const int tw_step = h / (ns * R);
+    for (int it = threadIdx.x; it < rows * nq; it += blockDim.x) {
+        const int row = it / nq, t = it - row * nq;
+        const cpx<T> *s = src + (size_t)row * h;
+        cpx<T> *d = dst + (size_t)row * h;
+        const int k = t % ns;
+        cpx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = s[t + r * nq];
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+            cpx<T> w = wtab[r * k * tw_step];
+            if (S > 0) w.y = -w.y;
+            v[r] = cmul(v[r], w);
+        }
+        dftR<T, S, R>(v);
+        const int base = (t / ns) * ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) d[base + r * ns] = v[r];
+    }
+}
+
+template <typename T, int S>
+__device__ const cpx<T> *run_fft(cpx<T> *b0, cpx<T> *b1, int h, int rows, const int *fac, int nfac,
+                                 const cpx<T> *wtab) {
+    cpx<T> *src = b0, *dst = b1;
+    int ns = 1;
+    for (int f = 0; f < nfac; f++) {
+        const int R = fac[f];
+        if (R == 8) stockham_pass<T, S, 8>(src, dst, h, ns, rows, wtab);
+        else if (R == 4) stockham_pass<T, S, 4>(src, dst, h, ns, rows, wtab);
+        else if (R == 2) stockham_pass<T, S, 2>(src, dst, h, ns, rows, wtab);
+        else if (R == 3) stockham_pass<T, S, 3>(src, dst, h, ns, rows, wtab);
+        else stockham_pass<T, S, 5>(src, dst, h, ns, rows, wtab);
+        __syncthreads();
+        ns *= R;
+        cpx<T> *tmp = src; src = dst; dst = tmp;
+    }
+    return src;
+}
+
+struct FftLaunch {
+    int n, h, nfac, fac[16];
+    long long lot;
+    int rows_per_block;
+    int kf;                 // Fourier coefficients read (inverse) / written (forward)
+    long long f_rs, f_ms;   // Fourier addressing (complex units): row stride, m stride
+};
+
+// gp (grid rows, contiguous)  ->  Fourier side
+template <typename T>
+__global__ void __launch_bounds__(256) k_rfft_forward(const T *gp, T *fc, FftLaunch L,
+                                                       const cpx<T> *__restrict__ wtab,
+                                                       const cpx<T> *__restrict__ rtab) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int h = L.h, n = L.n;
+    cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
+    cpx<T> *b1 = b0 + (size_t)L.rows_per_block * h;
+    const long long row0 = (long long)blockIdx.x * L.rows_per_block;
+    const int rows = (int)min((long long)L.rows_per_block, L.lot - row0);
+    T *braw = reinterpret_cast<T *>(b0);
+    const T *src = gp + row0 * n;
+    for (int i = threadIdx.x; i < rows * n; i += blockDim.x) braw[i] = src[i];
+    __syncthreads();
+    const cpx<T> *Z = run_fft<T, -1>(b0, b1, h, rows, L.fac, L.nfac, wtab);
+    // split: X_k = E_k + W_n^k O_k, E = (Z_k + conj Z_{h-k})/2, O = (Z_k - conj Z_{h-k})/(2i)
+    const T scale = (T)1 / (T)n;
+    for (int it = threadIdx.x; it < rows * L.kf; it += blockDim.x) {
+        const int row = it / L.kf, k = it - row * L.kf;
+        const cpx<T> *z = Z + (size_t)row * h;
+        T re, im;
+        if (k == 0) {
+            re = (z[0].x + z[0].y) * scale;
+            im = 0;
+        } else {
+            cpx<T> a = z[k], b = z[h - k];
+            cpx<T> E{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
+            cpx<T> O{(T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x)};
+            cpx<T> w = rtab[k];
+            cpx<T> wo = cmul(w, O);
+            re = (E.x + wo.x) * scale;
+            im = (E.y + wo.y) * scale;
+        }
+        const size_t o = 2 * ((row0 + row) * L.f_rs + (long long)k * L.f_ms);
+        fc[o] = re;
+        fc[o + 1] = im;
+    }
+}
+
+// Fourier side  ->  gp (grid rows, contiguous).  in and out may alias when
+// the Fourier side uses the row layout (each block owns its rows).
+template <typename T>
+__global__ void __launch_bounds__(256) k_rfft_inverse(const T *fc, T *gp, FftLaunch L,
+                                                       const cpx<T> *__restrict__ wtab,
+                                                       const cpx<T> *__restrict__ rtab) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int h = L.h, n = L.n;
+    cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
+    cpx<T> *b1 = b0 + (size_t)L.rows_per_block * h;
+    const long long row0 = (long long)blockIdx.x * L.rows_per_block;
+    const int rows = (int)min((long long)L.rows_per_block, L.lot - row0);
+    // stage c_k (k < kf) into b1, zero above
+    for (int it = threadIdx.x; it < rows * h; it += blockDim.x) {
+        const int row = it / h, k = it - row * h;
+        cpx<T> c{0, 0};
+        if (k < L.kf) {
+            const size_t o = 2 * ((row0 + row) * L.f_rs + (long long)k * L.f_ms);
+            c.x = fc[o];
+            c.y = (k == 0) ? (T)0 : fc[o + 1];
+        }
+        b1[(size_t)row * h + k] = c;
+    }
+    __syncthreads();
+    // Z_k = E_k + i O_k with E = C_k + conj C_{h-k}, O = (C_k - conj C_{h-k}) e^{+2 pi i k/n}, C_h = 0
+    for (int it = threadIdx.x; it < rows * h; it += blockDim.x) {
+        const int row = it / h, k = it - row * h;
+        const cpx<T> *c = b1 + (size_t)row * h;
+        cpx<T> a = c[k];
+        cpx<T> b = (k == 0) ? cpx<T>{0, 0} : c[h - k];
+        cpx<T> E{a.x + b.x, a.y - b.y};
+        cpx<T> D{a.x - b.x, a.y + b.y};
+        cpx<T> w = rtab[k];
+        w.y = -w.y;
+        cpx<T> O = cmul(D, w);
+        b0[(size_t)row * h + k] = cpx<T>{E.x - O.y, E.y + O.x};
+    }
+    __syncthreads();
+    const cpx<T> *z = run_fft<T, +1>(b0, b1, h, rows, L.fac, L.nfac, wtab);
+    const T *zr = reinterpret_cast<const T *>(z);
+    T *dst = gp + row0 * n;
+    for (int i = threadIdx.x; i < rows * n; i += blockDim.x) dst[i] = zr[i];
+}
+
+// ----------------------------------------------------------------- tables
+static bool factor_h(int h, int *fac, int *nfac) {
+    int k = 0, r = h;
+    while (r % 8 == 0 && r > 8) { fac[k++] = 8; r /= 8; }
+    while (r % 4 == 0) { fac[k++] = 4; r /= 4; }
+    while (r % 2 == 0) { fac[k++] = 2; r /= 2; }
+    while (r % 3 == 0) { fac[k++] = 3; r /= 3; }
+    while (r % 5 == 0) { fac[k++] = 5; r /= 5; }
+    if (r == 8) { fac[k++] = 8; r = 1; }
+    if (r != 1 || k > 16) return false;
+    *nfac = k;
+    return true;
+}
+
+static std::mutex g_fft_mu;
+static std::map<int, FftTables *> g_fft_cache;
+
+const FftTables *fft_tables(int n, exotx_status *st) {
+    std::lock_guard<std::mutex> lk(g_fft_mu);
+    auto it = g_fft_cache.find(n);
+    if (it != g_fft_cache.end()) { *st = EXOTX_OK; return it->second; }
+    if (!exotx_fft_supported(n)) { *st = EXOTX_UNSUPPORTED_N; return nullptr; }
+    FftTables *t = new FftTables();
+    t->n = n;
+    t->h = n / 2;
+    factor_h(t->h, t->fac, &t->nfac);
+    int h = t->h;
+    // twiddles from exact integer angles, evaluated in long double
+    std::vector<double> w64(2 * h), r64(2 * (h + 1));
+    std::vector<float> w32(2 * h), r32(2 * (h + 1));
+    const long double PI_L = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < h; k++) {
+        long double a = -2.0L * PI_L * (long double)k / (long double)h;
+        w64[2 * k] = (double)cosl(a); w64[2 * k + 1] = (double)sinl(a);
+        w32[2 * k] = (float)cosl(a); w32[2 * k + 1] = (float)sinl(a);
+    }
+    for (int k = 0; k <= h; k++) {
+        long double a = -2.0L * PI_L * (long double)k / (long double)n;
+        r64[2 * k] = (double)cosl(a); r64[2 * k + 1] = (double)sinl(a);
+        r32[2 * k] = (float)cosl(a); r32[2 * k + 1] = (float)sinl(a);
+    }
+    bool ok = cudaMalloc(&t->w64, sizeof(double) * 2 * h) == cudaSuccess &&
+              cudaMalloc(&t->w32, sizeof(float) * 2 * h) == cudaSuccess &&
+              cudaMalloc(&t->r64, sizeof(double) * 2 * (h + 1)) == cudaSuccess &&
+              cudaMalloc(&t->r32, sizeof(float) * 2 * (h + 1)) == cudaSuccess;
+    ok = ok && cudaMemcpy(t->w64, w64.data(), sizeof(double) * 2 * h, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(t->w32, w32.data(), sizeof(float) * 2 * h, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(t->r64, r64.data(), sizeof(double) * 2 * (h + 1), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(t->r32, r32.data(), sizeof(float) * 2 * (h + 1), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+        cudaFree(t->w64); cudaFree(t->w32); cudaFree(t->r64); cudaFree(t->r32);
+        delete t;
+        *st = EXOTX_NO_MEM;
+        return nullptr;
+    }
+    g_fft_cache[n] = t;
+    *st = EXOTX_OK;
+    return t;
+}
+
+template <typename T> static const cpx<T> *wt(const FftTables *t);
+template <> const cpx<double> *wt<double>(const FftTables *t) { return reinterpret_cast<const cpx<double> *>(t->w64); }
+template <> const cpx<float> *wt<float>(const FftTables *t) { return reinterpret_cast<const cpx<float> *>(t->w32); }
+template <typename T> static const cpx<T> *rt(const FftTables *t);
+template <> const cpx<double> *rt<double>(const FftTables *t) { return reinterpret_cast<const cpx<double> *>(t->r64); }
+template <> const cpx<float> *rt<float>(const FftTables *t) { return reinterpret_cast<const cpx<float> *>(t->r32); }
+
+template <typename T>
+static FftLaunch make_launch(const FftTables *t, long long lot, int kf, long long f_rs, long long f_ms,
+                             size_t *smem) {
+    FftLaunch L;
+    L.n = t->n; L.h = t->h; L.nfac = t->nfac;
+    for (int i = 0; i < 16; i++) L.fac[i] = t->fac[i];
+    L.lot = lot; L.kf = kf; L.f_rs = f_rs; L.f_ms = f_ms;
+    size_t per_row = 2 * (size_t)t->n * sizeof(T);
+    int r = (int)((40 * 1024) / per_row);
+    r = r < 1 ? 1 : (r > 16 ? 16 : r);
+    L.rows_per_block = r;
+    *smem = per_row * r;
+    return L;
+}
+
+template <typename T>
+static exotx_status set_smem(const void *fn, size_t smem) {
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    return EXOTX_OK;
+}
+
+// Fourier layout helper: row-major reference layout (row stride n/2, m stride 1)
+template <typename T>
+exotx_status fft_forward_l(const T *in, T *out, int n, long long lot, int kout, long long f_rs, long long f_ms,
+                           cudaStream_t s) {
+    exotx_status st;
+    const FftTables *t = fft_tables(n, &st);
+    if (!t) return st;
+    if (lot <= 0) return EXOTX_OK;
+    size_t smem;
+    FftLaunch L = make_launch<T>(t, lot, kout, f_rs, f_ms, &smem);
+    EXOTX_TRY(set_smem<T>((const void *)k_rfft_forward<T>, smem));
+    long long nb = (lot + L.rows_per_block - 1) / L.rows_per_block;
+    k_rfft_forward<T><<<(unsigned)nb, 256, smem, s>>>(in, out, L, wt<T>(t), rt<T>(t));
+    EXOTX_CHECK_LAUNCH();
+    return EXOTX_OK;
+}
+
+template <typename T>
+exotx_status fft_inverse_l(const T *in, T *out, int n, long long lot, int kin, long long f_rs, long long f_ms,
+                           cudaStream_t s) {
+    exotx_status st;
+    const FftTables *t = fft_tables(n, &st);
+    if (!t) return st;
+    if (lot <= 0) return EXOTX_OK;
+    size_t smem;
+    FftLaunch L = make_launch<T>(t, lot, kin, f_rs, f_ms, &smem);
+    EXOTX_TRY(set_smem<T>((const void *)k_rfft_inverse<T>, smem));
+    long long nb = (lot + L.rows_per_block - 1) / L.rows_per_block;
+    k_rfft_inverse<T><<<(unsigned)nb, 256, smem, s>>>(in, out, L, wt<T>(t), rt<T>(t));
+    EXOTX_CHECK_LAUNCH();
+    return EXOTX_OK;
+}
+
+template exotx_status fft_forward_l<double>(const double *, double *, int, long long, int, long long, long long,
+                                            cudaStream_t);
+template exotx_status fft_forward_l<float>(const float *, float *, int, long long, int, long long, long long,
+                                           cudaStream_t);
+template exotx_status fft_inverse_l<double>(const double *, double *, int, long long, int, long long, long long,
+                                            cudaStream_t);
+template exotx_status fft_inverse_l<float>(const float *, float *, int, long long, int, long long, long long,
+                                           cudaStream_t);
+
+}  // namespace exotx
+
+EXOTX_API int exotx_fft_supported(int n) {
+    if (n < 4 || n > 4096 || (n & 1)) return 0;
+    int h = n / 2, fac[16], nfac;
+    return exotx::factor_h(h, fac, &nfac) ? 1 : 0;
+}

@@ -1,0 +1,172 @@
+/*
+ * exotx.h -- C ABI of the B200 spectral-transform core and radiation column
+ * pass of ExoPlaSim (libexotx.so).
+ *
+ * Plain pointers and sizes only.  Array arguments are DEVICE pointers unless
+ * a function says otherwise; the caller owns every field array, the library
+ * owns the per-resolution tables inside an exotx_plan.  Every function
+ * returns an exotx_status; none aborts the process or traps the GPU.
+ *
+ * Memory layouts are the reference's (Fortran column-major, first index
+ * fastest):
+ *   spectral  sp(2,NCSP)           re/im pairs, m-major triangle (m=0..NTRU, n=m..NTRU)
+ *   Fourier   fc(2,NLON/2,NLAT)    per latitude NLON/2 complex coefficients,
+ *                                  the same storage as a grid row gp(NLON,NLAT)
+ *   levels    x(...,NLEV)          fields of one kind stacked level by level
+ *   columns   x(NHOR,NLEV)         radiation inputs/outputs, NHOR fastest
+ * Latitudes run north to south (sid(1) > 0), as inigau returns them.
+ *
+ * Precision: EXOTX_FP64 arrays are double; EXOTX_FP32 and EXOTX_MIXED arrays
+ * are float.  EXOTX_MIXED runs the Legendre contractions on the tensor cores
+ * with 3-term BF16 splits of both operands and FP32 accumulation.
+ */
+#ifndef EXOTX_H
+#define EXOTX_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    EXOTX_OK = 0,
+    EXOTX_BAD_DIM = 1,        /* resolution / level count / size not supported */
+    EXOTX_UNSUPPORTED_N = 2,  /* FFT length not factorable by the supported radices */
+    EXOTX_BAD_ARG = 3,        /* null pointer, bad enum, misaligned pointer */
+    EXOTX_CUDA_ERR = 4,       /* a CUDA runtime call failed */
+    EXOTX_NO_MEM = 5,         /* device allocation failed */
+    EXOTX_TIMEOUT = 6,        /* a bounded device-side wait gave up */
+    EXOTX_NOT_BUILT = 7       /* the requested path is not available in this build */
+} exotx_status;
+
+typedef enum { EXOTX_FP64 = 0, EXOTX_FP32 = 1, EXOTX_MIXED = 2 } exotx_precision;
+
+typedef struct exotx_plan_s *exotx_plan;
+typedef void *exotx_stream;   /* a cudaStream_t; NULL = legacy default stream */
+
+/* Resolution and the legmod namelist knobs (plasimmod.f90:227, 309-317). */
+typedef struct {
+    int nlat;            /* NLAT; NLON = 2*NLAT, NTRU = (NLON-1)/3 (plasimmod.f90:100-101) */
+    int nfilter;         /* 0 none, 1 Cesaro, 2 exponential, 3 Lander-Hoskins, 4 Riesz-2 */
+    int ngptfilter;      /* apply the filter grid->spectral (0/1) */
+    int nspvfilter;      /* apply the filter spectral->grid (0/1) */
+    double landhoskn0;   /* Lander-Hoskins critical wavenumber */
+    double filterkappa;  /* exponential filter strength */
+    int nfilterexp;      /* exponential filter exponent */
+    int pyfft_nfs;       /* -1: model filters above; 0/1: pyfft's exp(-8(n/NTRU)^8) switch */
+    double plavor;       /* planetary vorticity removed from mode (0,1) by dv2uv */
+} exotx_grid_desc;
+
+/* Fill *d with the reference defaults for nlat (no filter, plavor = EZ). */
+exotx_status exotx_grid_desc_default(int nlat, exotx_grid_desc *d);
+
+/* Plan = device tables for one resolution, built on the GPU in FP64: the
+ * Gaussian Newton iteration (replaces inigau, gaussmod.f90:5-40) and the
+ * associated-Legendre recurrence with its eight derived tables (replaces
+ * legini, legmod.f90:30-171), plus FP32 and BF16-split copies. */
+exotx_status exotx_plan_create(const exotx_grid_desc *d, exotx_plan *out);
+exotx_status exotx_plan_destroy(exotx_plan p);
+exotx_status exotx_plan_dims(exotx_plan p, int *nlat, int *nlon, int *ntru, int *ncsp);
+/* HOST copies of sid(NLAT) and gwd(NLAT) (gaussmod.f90:5 outputs) */
+exotx_status exotx_plan_gauss(exotx_plan p, double *sid, double *gwd);
+/* HOST copy of one FP64 table q?(NCSP,NLAT) in the reference layout;
+ * which = 0..7 for qi,qj,qc,qe,qm,qq,qu,qv (legmod.f90:13-20) */
+exotx_status exotx_plan_table(exotx_plan p, int which, double *out);
+
+/* inigau (gaussmod.f90:5-40) on the device: sid(nlat), gwd(nlat) device arrays */
+exotx_status exotx_inigau(int nlat, double *sid, double *gwd, exotx_stream s);
+
+/* ---- Legendre transforms; nlev fields of the same kind, stacked ---- */
+/* sp2fc (legmod.f90:230): sp(2,NCSP,nlev) -> fc(2,NLON/2,NLAT,nlev), m>NTRU zeroed */
+exotx_status exotx_sp2fc(exotx_plan p, int prec, const void *sp, void *fc, int nlev, exotx_stream s);
+/* sp2fcdmu (legmod.f90:262): as sp2fc with the d/dmu table qj */
+exotx_status exotx_sp2fcdmu(exotx_plan p, int prec, const void *sp, void *fc, int nlev, exotx_stream s);
+/* fc2sp (legmod.f90:178), symmetric single-CPU branch: fc -> sp */
+exotx_status exotx_fc2sp(exotx_plan p, int prec, const void *fc, void *sp, int nlev, exotx_stream s);
+/* dv2uv (legmod.f90:312): (div, vort) -> (u cos, v cos) Fourier; pz is not modified */
+exotx_status exotx_dv2uv(exotx_plan p, int prec, const void *pd, const void *pz,
+                         void *pu, void *pv, int nlev, exotx_stream s);
+/* uv2dv (legmod.f90:356): (u, v) Fourier -> (div, vort) */
+exotx_status exotx_uv2dv(exotx_plan p, int prec, const void *pu, const void *pv,
+                         void *pd, void *pz, int nlev, exotx_stream s);
+/* mktend (legmod.f90:505): call-site argument order (d,t,z,tn,fu,fv,ke,ut,vt) */
+exotx_status exotx_mktend(exotx_plan p, int prec, void *d, void *t, void *z,
+                          const void *tn, const void *fu, const void *fv,
+                          const void *ke, const void *ut, const void *vt,
+                          int nlev, exotx_stream s);
+/* qtend (legmod.f90:433): (q, qn, uq, vq) */
+exotx_status exotx_qtend(exotx_plan p, int prec, void *q, const void *qn,
+                         const void *uq, const void *vq, int nlev, exotx_stream s);
+
+/* ---- real FFTs of lot rows of length n, in place ---- */
+/* gp2fc (fftmod.f90:29 / fft991mod.f90:32): grid rows -> (A0,0,A1,B1,...) x 1/n */
+exotx_status exotx_gp2fc(int prec, void *a, int n, int lot, exotx_stream s);
+/* fc2gp (fftmod.f90:64 / fft991mod.f90:60): inverse, m=0 imaginary slot ignored */
+exotx_status exotx_fc2gp(int prec, void *a, int n, int lot, exotx_stream s);
+/* 1 if n is a supported FFT length (2^a 3^b 5^c, 4 <= n <= 4096, n even) */
+int exotx_fft_supported(int n);
+
+/* ---- per-timestep transform sets (plasim.f90 gridpointa :2396-2486) ----
+ * inverse_set: spin(2*NCSP, 4L+1) = sd[L], st[L], sz[L], sq[L], sp
+ *   -> gpout(NHOR, 6L+3) = gu[L], gv[L], gt[L], gd[L], gz[L], gq[L], gpj, gpmt, gp
+ *   (invlega, i*m Fourier derivative of ln ps, fc2gp of every field)
+ * forward_set: gpin(NHOR, 9L+1) = gtn[L], gqn[L], gut[L], gvt[L], guz[L], gvz[L], gke[L], gvpp, guq[L], gvq[L]
+ *   -> spout(2*NCSP, 4L+1) = sdf[L], stf[L], szf[L], sqf[L], spf
+ *   (gp2fc of every field, fc2sp(gvpp), mktend, qtend); gpin is not modified */
+exotx_status exotx_inverse_set(exotx_plan p, int prec, const void *spin, void *gpout,
+                               int nlev, exotx_stream s);
+exotx_status exotx_forward_set(exotx_plan p, int prec, const void *gpin, void *spout,
+                               int nlev, exotx_stream s);
+
+/* ---- radiation column pass (radmod.f90 radstep :927-1110) ---- */
+typedef struct {
+    int nlev, nhor, nlon;                 /* nlon: longitudes per latitude row */
+    double ga, gascon, acpd, adv;         /* p_earth.f90:41-58, plasim.f90:1317-1318 */
+    double gsol0, gdist2, zsolar1, zsolar2, rcoeff;
+    double tswr1, tswr2, tswr3, tpofmt, acllwr, th2oc, clgray;
+    double a0o3, a1o3, aco3, bo3, co3, toffo3, o3scale;
+    double rcl1[3], rcl2[3], acl2[3];
+    int ndcycle, no3, nswrcl, nclouds, nrscat, newrsc, necham, necham6,
+        nstartemp, npbroaden, nswr, nlwr, nsol;
+    int nfixed, ncstsol, ngenkeplerian;
+    double zdecl, zmins, zrtim, rasc, dawn, solclat, solcdec, zcday;
+    double sigma[64], sigmah[64], dsigma[64];   /* nlev <= 64 */
+} exotx_rad_params;
+
+typedef struct {
+    /* per latitude row (nhor/nlon rows) */
+    const void *sid, *cola;
+    /* inputs, x(NHOR,NLEP) / x(NHOR,NLEV) */
+    const void *dt, *dq, *dcc, *dql, *dqco2;
+    const void *dp, *dls, *dicec;         /* (NHOR) */
+    void *dqo3;                           /* (NHOR,NLEV): written when no3 == 1, else read */
+    void *gmu0;                           /* (NHOR): written when nsol == 1, else read */
+    void *dalb;                           /* (NHOR) in/out */
+    void *dsalb;                          /* (2,NHOR) in/out */
+    /* outputs */
+    void *dfu, *dfd, *dftu, *dftd, *dswfl, *dlwfl, *dflux;   /* (NHOR,NLEP) */
+    void *dtdt;                           /* (NHOR,NLEV) in/out (tendency is added) */
+    void *dtdtswr, *dtdtlwr, *dconv;      /* (NHOR,NLEV) */
+} exotx_rad_io;
+
+/* Reference defaults (radmod.f90:27-100, p_earth.f90, default sigma levels
+ * plasim.f90:1554-1564) for nlev levels and nhor columns in rows of nlon. */
+exotx_status exotx_rad_params_default(int nlev, int nhor, int nlon, exotx_rad_params *p);
+/* solarini band split (radmod.f90:166-376) for a blackbody star */
+exotx_status exotx_solarini(double starbbtemp, double minwavel_m,
+                            double *zsolar1, double *zsolar2, double *rcoeff);
+/* radstep: solang (nsol=1), mko3 (no3=1), swr, lwr, heating rates.  prec is
+ * EXOTX_FP64 (double arrays) or EXOTX_FP32 (float arrays). */
+exotx_status exotx_radstep(const exotx_rad_params *p, int prec, const exotx_rad_io *io,
+                           exotx_stream s);
+
+/* Human-readable text for a status code. */
+const char *exotx_status_string(exotx_status st);
+/* Number of kernel launches this library issued so far in this process. */
+unsigned long long exotx_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,158 @@
+"""CPU checks of the FP64 oracle: known answers and independent implementations.
+
+The reference ships no golden vectors for these routines and no Fortran
+compiler exists here, so the oracle is pinned by (a) mathematical identities
+the reference's algorithms must satisfy and (b) fixtures from numpy/scipy
+(tests/golden/, made by tests/golden/make_golden.py).
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from tests._util import relerr
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_v1.npz")
+
+
+@pytest.mark.parametrize("nlat", [8, 32, 64, 96, 192])
+def test_gauss_identities(oracle, nlat):
+    sid, gwd = oracle.inigau(nlat)
+    assert abs(gwd.sum() - 2.0) < 1e-13
+    assert np.all(np.diff(sid) < 0)          # north first
+    assert np.allclose(sid, -sid[::-1], atol=0, rtol=0)
+    x, w = np.polynomial.legendre.leggauss(nlat)
+    assert np.max(np.abs(np.sort(sid) - x)) < 1e-14
+    assert np.max(np.abs(gwd[np.argsort(sid)] - w)) < 5e-14
+
+
+@pytest.mark.parametrize("nlat", [32, 64])
+def test_legendre_orthonormality(oracle, nlat):
+    L = oracle.Leg(nlat)
+    qi = L.table("qi").reshape(nlat, L.ncsp)
+    gwd = L.table("gwd")
+    w = 0
+    for m in range(L.ntru + 1):
+        k = L.ntru + 1 - m
+        P = qi[:, w:w + k]
+        G = (P * gwd[:, None]).T @ P
+        assert np.max(np.abs(G - np.eye(k))) < 1e-12
+        w += k
+
+
+def test_tables_vs_golden(oracle):
+    g = np.load(GOLDEN)
+    L = oracle.Leg(32)
+    for name in ("qi", "qj"):
+        assert relerr(L.table(name).reshape(32, L.ncsp), g[f"t21_{name}"]) < 1e-12
+
+
+def test_fft_vs_golden(oracle):
+    g = np.load(GOLDEN)
+    for n in (64, 128, 384, 512):
+        x = g[f"fft_x_{n}"]
+        assert relerr(oracle.gp2fc(x), g[f"fft_c_{n}"]) < 1e-14
+    for n in (192,):
+        x = g[f"fft_x_{n}"]
+        assert relerr(oracle.gp2fc(x, use991=True), g[f"fft_c_{n}"]) < 1e-14
+
+
+def test_sp2gp_vs_golden(oracle):
+    # spectral -> grid at T21 with scipy Legendre functions and numpy's FFT
+    g = np.load(GOLDEN)
+    L = oracle.Leg(32)
+    sp = g["t21_sp"]
+    grid = oracle.fc2gp(L.sp2fc(sp))
+    assert relerr(grid, g["t21_grid"]) < 1e-12
+
+
+def test_fftmod_n48_is_not_a_dft(oracle):
+    # documented reference defect: fftmod.f90 lists n=48 but its radix
+    # schedule cannot factor 48/8 = 6.  The restatement reproduces it.
+    x = np.random.default_rng(0).standard_normal((2, 48))
+    ref = np.fft.rfft(x, axis=-1) / 48
+    out = oracle.gp2fc(x)
+    assert np.max(np.abs(out[:, 2] - ref.real[:, 1])) > 1e-3
+
+
+def test_fft_roundtrip_and_impulse(oracle):
+    n = 64
+    x = np.zeros((1, n))
+    x[0, 5] = 1.0
+    c = oracle.gp2fc(x)
+    k = np.arange(n // 2)
+    assert np.allclose(c[0, 2::2], np.cos(2 * np.pi * 5 * k[1:] / n) / n, atol=1e-16)
+    assert np.allclose(c[0, 3::2], -np.sin(2 * np.pi * 5 * k[1:] / n) / n, atol=1e-16)
+    y = np.random.default_rng(1).standard_normal((3, n))
+    assert relerr(oracle.fc2gp(oracle.gp2fc(y)), y - (y @ ((-1.0) ** np.arange(n)))[:, None] * ((-1.0) ** np.arange(n)) / n) < 1e-14
+
+
+def test_folded_and_unfolded_fc2sp_agree(oracle):
+    L = oracle.Leg(32)
+    fc = np.random.default_rng(3).standard_normal((32, 64))
+    assert relerr(L.fc2sp(fc, folded=True), L.fc2sp(fc, folded=False)) < 1e-13
+
+
+def test_filters(oracle):
+    # pyfft physics filter is exp(-8 (n/NTRU)^8) in 4-byte reals (pyfft.f90:152-156)
+    L = oracle.Leg(32, pyfft_nfs=1)
+    f = L.table("skspgp")
+    n = np.arange(1, L.ntru + 2, dtype=np.float32)
+    assert np.allclose(f, np.exp(np.float32(-8) * (n / np.float32(L.ntru)) ** 8), rtol=1e-6)
+    L4 = oracle.Leg(32, nfilter=4, ngptfilter=1, nspvfilter=0)
+    g = L4.table("skgpsp")
+    assert np.allclose(g, (1 - np.arange(1, L4.ntru + 2) / (L4.ntru + 1)) ** 2)
+    assert np.all(L4.table("skspgp") == 1.0)
+
+
+def test_solarini_sun(oracle):
+    # the 5772 K blackbody gives the model's default split 0.517/0.483 (radmod.f90:197-198)
+    z1, z2, rc = oracle.solarini(5772.0)
+    assert abs(z1 - 0.517) < 2e-3
+    assert abs(z1 + z2 - 1) < 1e-15
+    # rcoeff is normalised to the 5772 K spectrum with the module default 0.517
+    assert abs(rc - 0.517 / z1) < 1e-9
+    z1c, _, rcc = oracle.solarini(3000.0)
+    assert z1c < z1 and rcc < rc
+
+
+def _rad_case(oracle, nlev=10, **over):
+    from exoplasim_b200 import synthetic as S
+    cols, g = S.radiation_columns(8, nlev, seed=11)
+    p = oracle.radpar(nlev, g["nhor"], g["nlon"], g["sigma"], g["sigmah"], g["dsigma"], nsol=0, **over)
+    return oracle.radstep(p, cols["sid"], cols["cola"], cols), cols, p
+
+
+def test_radstep_zero_insolation(oracle):
+    out, cols, _ = _rad_case(oracle)
+    dark = cols["gmu0"] <= 0
+    assert dark.any()
+    assert np.all(out["dswfl"][:, dark] == 0) and np.all(out["dfd"][:, dark] == 0)
+
+
+def test_radstep_energy_closure(oracle):
+    out, cols, p = _rad_case(oracle)
+    ds = np.array([p.dsigma[i] for i in range(10)])[:, None]
+    cp = p.acpd * (1 + p.adv * cols["dq"][:10])
+    heat = np.sum(out["dtdt"] * ds * cols["dp"][None, :] * cp / p.ga, axis=0)
+    assert relerr(heat, out["dflux"][0] - out["dflux"][10]) < 1e-12
+
+
+def test_radstep_transparent_isothermal_lw(oracle):
+    # no absorbers, no clouds, isothermal black surface-like column: the
+    # longwave downward flux at the top is zero and the upward flux at the
+    # surface is eps*sigma*T^4
+    from exoplasim_b200 import synthetic as S
+    cols, g = S.radiation_columns(8, 10, seed=12)
+    nhor = g["nhor"]
+    cols["dq"][:] = 0
+    cols["dcc"][:] = 0
+    cols["dql"][:] = 0
+    cols["dqco2"][:] = 0
+    cols["dt"][:] = 250.0
+    p = oracle.radpar(10, nhor, g["nlon"], g["sigma"], g["sigmah"], g["dsigma"], nsol=0, no3=0, th2oc=0.0)
+    cols["dqo3"][:] = 0
+    out = oracle.radstep(p, cols["sid"], cols["cola"], cols)
+    assert np.all(out["dftd"][0] == 0)
+    assert np.allclose(out["dftu"][10], -0.98 * 5.67e-8 * 250.0 ** 4, rtol=1e-12)

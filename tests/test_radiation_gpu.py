@@ -1,0 +1,78 @@
+"""Parity of the CUDA radstep (through the C ABI) against the FP64 oracle.
+
+Tolerances (norm-wise relative per output field): FP64 <= 1e-11; FP32 <= 2e-3
+on fluxes and 5e-3 on heating rates (single-precision pow/exp/log chains).
+"""
+import numpy as np
+import pytest
+import torch
+
+from exoplasim_b200 import radiation as R
+from exoplasim_b200 import synthetic as S
+from tests._util import relerr
+
+pytestmark = pytest.mark.gpu
+
+FLUXES = ("dfu", "dfd", "dftu", "dftd", "dswfl", "dlwfl", "dflux")
+RATES = ("dtdt", "dtdtswr", "dtdtlwr", "dconv")
+
+
+def _run(oracle, nlat, nlev, precision, seed=2, **over):
+    cols, g = S.radiation_columns(nlat, nlev, seed=seed)
+    nhor, nlon = g["nhor"], g["nlon"]
+    params = R.default_params(nlev, nhor, nlon, nsol=0, **over)
+    # identical sigma levels on both sides: the synthetic columns clip T at
+    # 150 K, which makes some of radmod's branch tests exact ties
+    sig = [np.array(getattr(params, k)[:nlev]) for k in ("sigma", "sigmah", "dsigma")]
+    p_ref = oracle.radpar(nlev, nhor, nlon, *sig, nsol=0, **over)
+    ref = oracle.radstep(p_ref, cols["sid"], cols["cola"], cols)
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    dev = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=dt, device="cuda") for k, v in cols.items()}
+    out = R.radstep(params, dev, precision=precision)
+    got = {k: v.cpu().numpy() for k, v in out.items()}
+    for k in ("dqo3", "dalb", "dsalb", "dtdt", "gmu0"):
+        got[k] = dev[k].cpu().numpy()
+    return got, ref
+
+
+@pytest.mark.parametrize("nlat,nlev", [(32, 10), (32, 20), (64, 20)])
+def test_radstep_fp64(oracle, nlat, nlev):
+    got, ref = _run(oracle, nlat, nlev, "fp64")
+    for k in FLUXES + RATES + ("dqo3", "dalb", "dsalb"):
+        assert relerr(got[k], ref[k]) < 1e-11, k
+
+
+def test_radstep_fp32(oracle):
+    got, ref = _run(oracle, 32, 20, "fp32")
+    for k in FLUXES:
+        assert relerr(got[k], ref[k]) < 2e-3, k
+    for k in RATES:
+        assert relerr(got[k], ref[k]) < 5e-3, k
+
+
+def test_radstep_switches(oracle):
+    # prescribed cloud optics, ECHAM-6 ocean albedo, fixed cloud grayness
+    got, ref = _run(oracle, 32, 10, "fp64", seed=5, nswrcl=0, necham=0, necham6=1, clgray=0.5)
+    for k in FLUXES + RATES:
+        assert relerr(got[k], ref[k]) < 1e-11, k
+
+
+def test_night_columns_have_no_shortwave(oracle):
+    got, _ = _run(oracle, 32, 10, "fp64")
+    cols, _ = S.radiation_columns(32, 10, seed=2)
+    dark = cols["gmu0"] <= 0
+    assert dark.any()
+    assert np.all(got["dswfl"][:, dark] == 0.0)
+
+
+def test_energy_closure(oracle):
+    # heating = -g dF/(dsigma ps cp (1+adv q)) (radmod.f90:1100-1103): column
+    # integral of the heating balances the net flux divergence
+    got, _ = _run(oracle, 32, 10, "fp64")
+    cols, g = S.radiation_columns(32, 10, seed=2)
+    p = R.default_params(10, g["nhor"], g["nlon"])
+    ds = np.array(p.dsigma[:10])[:, None]
+    cp = p.acpd * (1 + p.adv * cols["dq"][:10])
+    heat = np.sum(got["dtdt"] * ds * cols["dp"][None, :] * cp / p.ga, axis=0)
+    net = got["dflux"][0] - got["dflux"][10]
+    assert relerr(heat, net) < 1e-12
