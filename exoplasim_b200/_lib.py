@@ -78,6 +78,10 @@ SIGNATURES = {
     "exotx_rad_params_default": [_I, _I, _I, C.POINTER(RadParams)],
     "exotx_solarini": [_D, _D, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)],
     "exotx_radstep": [C.POINTER(RadParams), _I, C.POINTER(RadIO), _S],
+    "exotx_tc_selftest": [_P, _P, _P, _I, _I, _I, _S],
+    "exotx_inverse_set_batch": [_P, _I, _P, _P, _I, _I, _S],
+    "exotx_forward_set_batch": [_P, _I, _P, _P, _I, _I, _S],
+    "exotx_tc_error": [C.POINTER(_I), _S],
 }
 RESTYPES = {"exotx_fft_supported": C.c_int, "exotx_launch_count": C.c_ulonglong,
             "exotx_status_string": C.c_char_p}

@@ -187,6 +187,42 @@ EXOTX_API exotx_status exotx_inverse_set(exotx_plan p, int prec, const void *spi
     return tc_inverse_set(p, (const float *)spin, (float *)gpout, nlev, (cudaStream_t)s);
 }
 
+EXOTX_API exotx_status exotx_inverse_set_batch(exotx_plan p, int prec, const void *spin, void *gpout, int nlev,
+                                               int ninst, exotx_stream s) {
+    PLAN_PREC_CHECK(p, prec);
+    if (ninst == 0) return EXOTX_OK;
+    if (!spin || !gpout || nlev < 1 || ninst < 0) return EXOTX_BAD_ARG;
+    if (prec == EXOTX_MIXED)
+        return tc_inverse_batch(p, (const float *)spin, (float *)gpout, nlev, ninst, (cudaStream_t)s);
+    const size_t esz = prec == EXOTX_FP64 ? 8 : 4;
+    const size_t in_b = (size_t)(4 * nlev + 1) * 2 * p->ncsp * esz;
+    const size_t out_b = (size_t)(6 * nlev + 3) * p->nlat * p->nlon * esz;
+    for (int i = 0; i < ninst; i++)
+        EXOTX_TRY(exotx_inverse_set(p, prec, (const char *)spin + i * in_b, (char *)gpout + i * out_b, nlev, s));
+    return EXOTX_OK;
+}
+
+EXOTX_API exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const void *gpin, void *spout, int nlev,
+                                               int ninst, exotx_stream s) {
+    PLAN_PREC_CHECK(p, prec);
+    if (ninst == 0) return EXOTX_OK;
+    if (!gpin || !spout || nlev < 1 || ninst < 0) return EXOTX_BAD_ARG;
+    if (prec == EXOTX_MIXED)
+        return tc_forward_batch(p, (const float *)gpin, (float *)spout, nlev, ninst, (cudaStream_t)s);
+    const size_t esz = prec == EXOTX_FP64 ? 8 : 4;
+    const size_t in_b = (size_t)(9 * nlev + 1) * p->nlat * p->nlon * esz;
+    const size_t out_b = (size_t)(4 * nlev + 1) * 2 * p->ncsp * esz;
+    for (int i = 0; i < ninst; i++)
+        EXOTX_TRY(exotx_forward_set(p, prec, (const char *)gpin + i * in_b, (char *)spout + i * out_b, nlev, s));
+    return EXOTX_OK;
+}
+
+EXOTX_API exotx_status exotx_tc_error(int *code, exotx_stream s) {
+    if (!code) return EXOTX_BAD_ARG;
+    EXOTX_TRY(tc_error_read(code, (cudaStream_t)s));
+    return tc_error_reset((cudaStream_t)s);
+}
+
 EXOTX_API exotx_status exotx_forward_set(exotx_plan p, int prec, const void *gpin, void *spout, int nlev,
                                          exotx_stream s) {
     PLAN_PREC_CHECK(p, prec);

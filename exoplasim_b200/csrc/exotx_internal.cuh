@@ -115,6 +115,10 @@ exotx_status fft_inverse_l(const T *in, T *out, int n, long long lot, int kin, l
 // tensor-core Legendre (legendre_tc.cu)
 exotx_status tc_inverse_set(exotx_plan p, const float *spin, float *four, int nlev, cudaStream_t s);
 exotx_status tc_forward_set(exotx_plan p, const float *four, float *spout, int nlev, cudaStream_t s);
+exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int L, int ninst, cudaStream_t s);
+exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int L, int ninst, cudaStream_t s);
+exotx_status tc_error_reset(cudaStream_t s);
+exotx_status tc_error_read(int *err, cudaStream_t s);
 exotx_status tc_available();
 void tc_free(exotx_plan p);
 }  // namespace exotx

@@ -208,6 +208,38 @@ class Plan:
         return out
 
 
+    def inverse_set_batch(self, spin, nlev, precision="mixed", out=None):
+        """inverse_set for ninst states stored back to back: (ninst, 4L+1, NRSP) -> (ninst, 6L+3, NLAT, NLON)."""
+        p = _prec(precision)
+        dt = _dtype(p)
+        ninst = spin.shape[0]
+        _check(spin, dt, (ninst, 4 * nlev + 1, self.nrsp), "spin")
+        if out is None:
+            out = torch.zeros((ninst, 6 * nlev + 3, self.nlat, self.nlon), dtype=dt, device=spin.device)
+        _check(out, dt, (ninst, 6 * nlev + 3, self.nlat, self.nlon), "gpout")
+        call("exotx_inverse_set_batch", self._h, p, _ptr(spin), _ptr(out), nlev, ninst, _stream())
+        return out
+
+    def forward_set_batch(self, gpin, nlev, precision="mixed", out=None):
+        """forward_set for ninst states: (ninst, 9L+1, NLAT, NLON) -> (ninst, 4L+1, NRSP)."""
+        p = _prec(precision)
+        dt = _dtype(p)
+        ninst = gpin.shape[0]
+        _check(gpin, dt, (ninst, 9 * nlev + 1, self.nlat, self.nlon), "gpin")
+        if out is None:
+            out = torch.zeros((ninst, 4 * nlev + 1, self.nrsp), dtype=dt, device=gpin.device)
+        _check(out, dt, (ninst, 4 * nlev + 1, self.nrsp), "spout")
+        call("exotx_forward_set_batch", self._h, p, _ptr(gpin), _ptr(out), nlev, ninst, _stream())
+        return out
+
+
+def tc_error():
+    """Read and reset the tensor-core kernels' error word (0 = no bounded wait gave up)."""
+    code = C.c_int(0)
+    call("exotx_tc_error", C.byref(code), _stream())
+    return code.value
+
+
 def _fft_args(a, precision):
     if not isinstance(a, torch.Tensor) or not a.is_cuda or not a.is_contiguous():
         raise TypeError("FFT input must be a contiguous CUDA tensor")

@@ -118,6 +118,17 @@ exotx_status exotx_inverse_set(exotx_plan p, int prec, const void *spin, void *g
                                int nlev, exotx_stream s);
 exotx_status exotx_forward_set(exotx_plan p, int prec, const void *gpin, void *spout,
                                int nlev, exotx_stream s);
+/* The same sets for ninst independent model states of this resolution stored
+ * back to back (spin: ninst x (4L+1) x NRSP, gpout: ninst x (6L+3) x NHOR, ...).
+ * The reference runs one state per process (plasim.f90 gridpointa); batching
+ * makes fields x levels x states the N extent of the tensor-core contractions. */
+exotx_status exotx_inverse_set_batch(exotx_plan p, int prec, const void *spin, void *gpout,
+                                     int nlev, int ninst, exotx_stream s);
+exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const void *gpin, void *spout,
+                                     int nlev, int ninst, exotx_stream s);
+/* Error word of the tensor-core kernels (0 = none; nonzero = a bounded
+ * device-side wait gave up), read after synchronising the stream, then reset. */
+exotx_status exotx_tc_error(int *code, exotx_stream s);
 
 /* ---- radiation column pass (radmod.f90 radstep :927-1110) ---- */
 typedef struct {
@@ -160,6 +171,14 @@ exotx_status exotx_solarini(double starbbtemp, double minwavel_m,
  * EXOTX_FP64 (double arrays) or EXOTX_FP32 (float arrays). */
 exotx_status exotx_radstep(const exotx_rad_params *p, int prec, const exotx_rad_io *io,
                            exotx_stream s);
+
+/* Diagnostic of the tensor-core path (no counterpart in the reference):
+ * C(128 x N) = A(128 x K) * B(N x K)^T on one CTA with tcgen05.mma, FP32
+ * inputs split into three BF16 terms, nprod in {1,3,6} split products,
+ * FP32 accumulation in tensor memory.  Device pointers, row-major, N and K
+ * multiples of 16 (N <= 256, K <= 64).  Synchronises the stream. */
+exotx_status exotx_tc_selftest(const float *A, const float *B, float *C, int N, int K, int nprod,
+                               exotx_stream s);
 
 /* Human-readable text for a status code. */
 const char *exotx_status_string(exotx_status st);
