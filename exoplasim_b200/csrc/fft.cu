@@ -227,6 +227,209 @@ __global__ void __launch_bounds__(256) k_rfft_inverse(const T *fc, T *gp, FftLau
     for (int i = threadIdx.x; i < rows * n; i += blockDim.x) dst[i] = zr[i];
 }
 
+// ------------------------------------------- length-specialised kernels
+// For the model's grid lengths the radix schedule, loop trip counts and
+// index divisions are compile-time constants and the twiddles live in
+// shared memory; one block transforms ROWS rows.
+__host__ __device__ constexpr int radix_count(int h) {
+    int r = h, k = 0;
+    while (r % 8 == 0 && r > 8) { k++; r /= 8; }
+    while (r % 4 == 0) { k++; r /= 4; }
+    while (r % 2 == 0) { k++; r /= 2; }
+    while (r % 3 == 0) { k++; r /= 3; }
+    while (r % 5 == 0) { k++; r /= 5; }
+    if (r == 8) k++;
+    return k;
+}
+__host__ __device__ constexpr int radix_at(int h, int idx) {
+    int r = h, k = 0;
+    while (r % 8 == 0 && r > 8) { if (k++ == idx) return 8; r /= 8; }
+    while (r % 4 == 0) { if (k++ == idx) return 4; r /= 4; }
+    while (r % 2 == 0) { if (k++ == idx) return 2; r /= 2; }
+    while (r % 3 == 0) { if (k++ == idx) return 3; r /= 3; }
+    while (r % 5 == 0) { if (k++ == idx) return 5; r /= 5; }
+    return 8;
+}
+
+template <typename T, int S, int H, int ROWS, int R, int NS>
+__device__ __forceinline__ void pass_ct(const cpx<T> *src, cpx<T> *dst, const cpx<T> *tw) {
+    constexpr int NQ = H / R, STEP = H / (NS * R), NIT = ROWS * NQ;
+    for (int it = threadIdx.x; it < NIT; it += blockDim.x) {
+        const int row = it / NQ, t = it - row * NQ, k = t % NS;
+        const cpx<T> *s = src + row * H;
+        cpx<T> *d = dst + row * H;
+        cpx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = s[t + r * NQ];
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+            cpx<T> w = tw[r * k * STEP];
+            if (S > 0) w.y = -w.y;
+            v[r] = cmul(v[r], w);
+        }
+        dftR<T, S, R>(v);
+        const int base = (t / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) d[base + r * NS] = v[r];
+    }
+}
+
+template <typename T, int S, int H, int ROWS, int IDX, int NS>
+__device__ __forceinline__ const cpx<T> *passes_ct(cpx<T> *src, cpx<T> *dst, const cpx<T> *tw) {
+    if constexpr (IDX >= radix_count(H)) {
+        return src;
+    } else {
+        constexpr int R = radix_at(H, IDX);
+        pass_ct<T, S, H, ROWS, R, NS>(src, dst, tw);
+        __syncthreads();
+        return passes_ct<T, S, H, ROWS, IDX + 1, NS * R>(dst, src, tw);
+    }
+}
+
+template <typename T> struct vec2 { using t = float4; };
+template <> struct vec2<double> { using t = double2; };
+
+template <typename T, int N, int ROWS>
+__global__ void __launch_bounds__(256) k_rfft_fwd_ct(const T *gp, T *fc, long long lot, int kf, long long f_rs,
+                                                      long long f_ms, const cpx<T> *__restrict__ wtab,
+                                                      const cpx<T> *__restrict__ rtab) {
+    constexpr int H = N / 2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
+    cpx<T> *b1 = b0 + ROWS * H;
+    cpx<T> *tw = b1 + ROWS * H;
+    cpx<T> *rt = tw + H;
+    const long long row0 = (long long)blockIdx.x * ROWS;
+    const int rows = (int)min((long long)ROWS, lot - row0);
+    for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
+    for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
+    {
+        // rows are contiguous: two complex (= 4 reals for FP32) per vector load
+        using V = typename vec2<T>::t;
+        constexpr int PER = (int)(sizeof(V) / sizeof(T));
+        const V *src = reinterpret_cast<const V *>(gp + row0 * N);
+        V *dst = reinterpret_cast<V *>(b0);
+        const int nv = rows * N / PER;
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) dst[i] = src[i];
+        if (rows < ROWS) {
+            T *raw = reinterpret_cast<T *>(b0);
+            for (int i = rows * N + threadIdx.x; i < ROWS * N; i += blockDim.x) raw[i] = 0;
+        }
+    }
+    __syncthreads();
+    const cpx<T> *Z = passes_ct<T, -1, H, ROWS, 0, 1>(b0, b1, tw);
+    const T scale = (T)1 / (T)N;
+    for (int it = threadIdx.x; it < ROWS * kf; it += blockDim.x) {
+        const int row = it % ROWS, k = it / ROWS;
+        if (row >= rows) continue;
+        const cpx<T> *z = Z + row * H;
+        T re, im;
+        if (k == 0) {
+            re = (z[0].x + z[0].y) * scale;
+            im = 0;
+        } else {
+            cpx<T> a = z[k], b = z[H - k];
+            cpx<T> E{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
+            cpx<T> O{(T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x)};
+            cpx<T> wo = cmul(rt[k], O);
+            re = (E.x + wo.x) * scale;
+            im = (E.y + wo.y) * scale;
+        }
+        const size_t o = 2 * ((row0 + row) * f_rs + (long long)k * f_ms);
+        fc[o] = re;
+        fc[o + 1] = im;
+    }
+}
+
+template <typename T, int N, int ROWS>
+__global__ void __launch_bounds__(256) k_rfft_inv_ct(const T *fc, T *gp, long long lot, int kf, long long f_rs,
+                                                      long long f_ms, const cpx<T> *__restrict__ wtab,
+                                                      const cpx<T> *__restrict__ rtab) {
+    constexpr int H = N / 2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
+    cpx<T> *b1 = b0 + ROWS * H;
+    cpx<T> *tw = b1 + ROWS * H;
+    cpx<T> *rt = tw + H;
+    const long long row0 = (long long)blockIdx.x * ROWS;
+    const int rows = (int)min((long long)ROWS, lot - row0);
+    for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
+    for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
+    // c_k for k < kf (row fastest: consecutive rows are adjacent on the m-major side)
+    for (int it = threadIdx.x; it < ROWS * H; it += blockDim.x) {
+        const int row = it % ROWS, k = it / ROWS;
+        cpx<T> c{0, 0};
+        if (k < kf && row < rows) {
+            const size_t o = 2 * ((row0 + row) * f_rs + (long long)k * f_ms);
+            c.x = fc[o];
+            c.y = (k == 0) ? (T)0 : fc[o + 1];
+        }
+        b1[row * H + k] = c;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < ROWS * H; it += blockDim.x) {
+        const int row = it / H, k = it - row * H;
+        const cpx<T> *c = b1 + row * H;
+        cpx<T> a = c[k];
+        cpx<T> b = (k == 0) ? cpx<T>{0, 0} : c[H - k];
+        cpx<T> E{a.x + b.x, a.y - b.y};
+        cpx<T> D{a.x - b.x, a.y + b.y};
+        cpx<T> w = rt[k];
+        w.y = -w.y;
+        cpx<T> O = cmul(D, w);
+        b0[row * H + k] = cpx<T>{E.x - O.y, E.y + O.x};
+    }
+    __syncthreads();
+    const cpx<T> *z = passes_ct<T, +1, H, ROWS, 0, 1>(b0, b1, tw);
+    using V = typename vec2<T>::t;
+    constexpr int PER = (int)(sizeof(V) / sizeof(T));
+    const V *src = reinterpret_cast<const V *>(z);
+    V *dst = reinterpret_cast<V *>(gp + row0 * N);
+    const int nv = rows * N / PER;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) dst[i] = src[i];
+}
+
+template <typename T> constexpr int ct_rows(int n) {
+    return (sizeof(T) == 4) ? (n <= 256 ? 16 : 8) : (n <= 256 ? 8 : 4);
+}
+
+template <typename T, int N>
+static exotx_status launch_ct(bool fwd, const T *in, T *out, long long lot, int kf, long long f_rs, long long f_ms,
+                              const cpx<T> *w, const cpx<T> *r, cudaStream_t s) {
+    constexpr int ROWS = ct_rows<T>(N);
+    const size_t smem = (2 * ROWS * (N / 2) + N / 2 + N / 2 + 1) * sizeof(cpx<T>);
+    const long long nb = (lot + ROWS - 1) / ROWS;
+    if (fwd) {
+        if (smem > 48 * 1024)
+            EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_ct<T, N, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+        k_rfft_fwd_ct<T, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, lot, kf, f_rs, f_ms, w, r);
+    } else {
+        if (smem > 48 * 1024)
+            EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_inv_ct<T, N, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+        k_rfft_inv_ct<T, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, lot, kf, f_rs, f_ms, w, r);
+    }
+    EXOTX_CHECK_LAUNCH();
+    return EXOTX_OK;
+}
+
+// returns EXOTX_NOT_BUILT when n has no specialised kernel
+template <typename T>
+static exotx_status dispatch_ct(bool fwd, int n, const T *in, T *out, long long lot, int kf, long long f_rs,
+                                long long f_ms, const cpx<T> *w, const cpx<T> *r, cudaStream_t s) {
+    switch (n) {
+        case 64: return launch_ct<T, 64>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
+        case 128: return launch_ct<T, 128>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
+        case 192: return launch_ct<T, 192>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
+        case 256: return launch_ct<T, 256>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
+        case 320: return launch_ct<T, 320>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
+        case 384: return launch_ct<T, 384>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
+        case 512: return launch_ct<T, 512>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
+    }
+    return EXOTX_NOT_BUILT;
+}
+
 // ----------------------------------------------------------------- tables
 static bool factor_h(int h, int *fac, int *nfac) {
     int k = 0, r = h;
@@ -309,6 +512,8 @@ static FftLaunch make_launch(const FftTables *t, long long lot, int kf, long lon
     return L;
 }
 
+static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 template <typename T>
 static exotx_status set_smem(const void *fn, size_t smem) {
     if (smem > 48 * 1024) {
@@ -326,6 +531,10 @@ exotx_status fft_forward_l(const T *in, T *out, int n, long long lot, int kout, 
     const FftTables *t = fft_tables(n, &st);
     if (!t) return st;
     if (lot <= 0) return EXOTX_OK;
+    if (aligned16(in) && aligned16(out)) {
+        exotx_status sc = dispatch_ct<T>(true, n, in, out, lot, kout, f_rs, f_ms, wt<T>(t), rt<T>(t), s);
+        if (sc != EXOTX_NOT_BUILT) return sc;
+    }
     size_t smem;
     FftLaunch L = make_launch<T>(t, lot, kout, f_rs, f_ms, &smem);
     EXOTX_TRY(set_smem<T>((const void *)k_rfft_forward<T>, smem));
@@ -342,6 +551,10 @@ exotx_status fft_inverse_l(const T *in, T *out, int n, long long lot, int kin, l
     const FftTables *t = fft_tables(n, &st);
     if (!t) return st;
     if (lot <= 0) return EXOTX_OK;
+    if (aligned16(in) && aligned16(out)) {
+        exotx_status sc = dispatch_ct<T>(false, n, in, out, lot, kin, f_rs, f_ms, wt<T>(t), rt<T>(t), s);
+        if (sc != EXOTX_NOT_BUILT) return sc;
+    }
     size_t smem;
     FftLaunch L = make_launch<T>(t, lot, kin, f_rs, f_ms, &smem);
     EXOTX_TRY(set_smem<T>((const void *)k_rfft_inverse<T>, smem));

@@ -1,0 +1,507 @@
+// Tensor-core Legendre kernels (included by legendre_tc.cu).
+//
+// One CTA of 256 threads per job.  Warps w and w+4 share TMEM lane quarter
+// w % 4; in the epilogue the two halves split the work (the inverse by
+// column chunks, the forward by parity).  Thread 0 issues the TMA table
+// copies and the MMAs; everybody stages operands and drains accumulators.
+#pragma once
+
+constexpr int TCT2 = 256;
+
+// ------------------------------------------------------------ inverse
+struct TcInvArgs {
+    const unsigned char *tab;
+    const long long *off;
+    const int *woff;
+    const float *spin;      // [inst][4L+1][NRSP]
+    const float *filt;      // skspgp
+    float2 *W;              // [m][row], row = (inst*(6L+3) + field)*nlat + lat
+    long long nrows;
+    const int4 *jobs;
+    int L, nlat, nlath, nj8, ntp1, nrsp;
+    float plavor;
+};
+
+// complex spectral input of column pair q (columns 2q, 2q+1 = re, im), filtered
+__device__ __forceinline__ float2 inv_input2(const TcInvArgs &A, int group, int gq, int m, int k) {
+    const int L = A.L, nf = 4 * L + 1;
+    int inst, f;
+    bool zvort = false;
+    if (group == 0) { inst = gq / nf; f = gq % nf; }
+    else if (group == 1) { inst = gq; f = 4 * L; }
+    else {
+        // columns per level: Dr, Di, Zr, Zi -> pairs 2l (D), 2l+1 (Z)
+        inst = gq / (2 * L);
+        const int l = (gq % (2 * L)) >> 1;
+        zvort = gq & 1;
+        f = zvort ? 2 * L + l : l;
+    }
+    const int w = A.woff[m] + k;
+    float2 x = *reinterpret_cast<const float2 *>(A.spin + ((size_t)inst * nf + f) * A.nrsp + 2 * w);
+    if (zvort && m == 0 && k == 1) x.x -= A.plavor;  // dv2uv, legmod.f90:332
+    const float fl = A.filt[m + k];
+    return make_float2(x.x * fl, x.y * fl);
+}
+
+__global__ void __launch_bounds__(TCT2) k_tc_inverse(TcInvArgs A) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const int4 jb = A.jobs[blockIdx.x];
+    const int m = jb.x, group = jb.y, c0 = jb.z, nc = jb.w;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, half = warp >> 2;
+    const int K = A.ntp1 - m;
+    const int Kq[2] = {kpar(K, 0), kpar(K, 1)};
+    const int Kp[2] = {pad16(Kq[0]), pad16(Kq[1])};
+    const int ncp = pad16(nc);
+    const int ntab = group == 2 ? 2 : 1;
+    const int nj8 = A.nj8;
+    const size_t ttile[2] = {(size_t)nj8 * Kp[0] * 2, (size_t)nj8 * Kp[1] * 2};
+    const size_t tbytes = 3 * (ttile[0] + ttile[1]);
+    const size_t dtile[2] = {(size_t)ncp * Kp[0] * 2, (size_t)ncp * Kp[1] * 2};
+    unsigned char *tab = sm;
+    unsigned char *dat = sm + tbytes;
+    unsigned char *tail = dat + 3 * (dtile[0] + dtile[1]) + (size_t)(128 - nj8) * 64 * 2 + 128;
+    uint64_t *bar_tma = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
+    uint64_t *bar_mma = bar_tma + 1;
+    uint64_t *bar_done = bar_tma + 2;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar_tma + 3);
+    if (warp == 0) tc::tmem_alloc(slot, 512);
+    if (tid == 0) {
+        tc::mbar_init(bar_tma, 1);
+        tc::mbar_init(bar_mma, 1);
+        tc::mbar_init(bar_done, 1);
+        tc::mbar_fence_init();
+        // first table copy goes out before the staging so the two overlap
+        const int t0 = group == 0 ? 0 : (group == 1 ? 1 : 2);
+        tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
+        tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0], (uint32_t)tbytes, bar_tma);
+    }
+    // stage the spectral columns of both parities (one complex load per column pair)
+    size_t doff = 0;
+    for (int p = 0; p < 2; p++) {
+        if (!Kq[p]) break;
+        const int kp = Kp[p];
+        const int npair = ncp >> 1;
+        for (int idx = tid; idx < npair * kp; idx += TCT2) {
+            const int q = idx / kp, k = idx - q * kp;
+            const int c = 2 * q;
+            float2 x = make_float2(0.f, 0.f);
+            if (c < nc && k < Kq[p]) x = inv_input2(A, group, (c0 + c) >> 1, m, 2 * k + p);
+            __nv_bfloat16 h, mm, l;
+            const uint32_t o0 = tc::kmajor_off(c, k, kp), o1 = tc::kmajor_off(c + 1, k, kp);
+            tc::split3(x.x, h, mm, l);
+            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + o0) = h;
+            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + dtile[p] + o0) = mm;
+            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + 2 * dtile[p] + o0) = l;
+            tc::split3(x.y, h, mm, l);
+            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + o1) = h;
+            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + dtile[p] + o1) = mm;
+            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + 2 * dtile[p] + o1) = l;
+        }
+        doff += 3 * dtile[p];
+    }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    bool ok = true;
+    if (tid == 0) {
+        const uint32_t idesc = tc::idesc_bf16(128, ncp);
+        for (int ti = 0; ti < ntab && ok; ti++) {
+            if (ti > 0) {
+                ok = tc::mbar_wait(bar_mma, (ti - 1) & 1);  // table buffer free again
+                if (!ok) break;
+                const int t = 2 + ti;
+                tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
+                tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t], (uint32_t)tbytes, bar_tma);
+            }
+            ok = tc::mbar_wait(bar_tma, ti & 1);
+            if (!ok) break;
+            tc::fence_after_sync();
+            size_t to = 0, dd = 0;
+            for (int p = 0; p < 2; p++) {
+                if (!Kq[p]) break;
+                // hi*hi products and the five smaller correction products go to
+                // separate accumulators (the tensor-core adder truncates; keeping the
+                // large term's chain short bounds that error), summed in the epilogue
+                const uint32_t dm = tmem + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp);
+                const uint32_t dc = tmem + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp);
+                const uint32_t sbo = (uint32_t)(Kp[p] / 8) * 128;
+                bool accm = false, accc = false;
+                for (int kc = 0; kc < Kp[p] / 16; kc++)
+                    for (int pr = 0; pr < 6; pr++) {
+                        const unsigned char *a = tab + to + c_pair_a[pr] * ttile[p] + kc * 256;
+                        const unsigned char *b = dat + dd + c_pair_b[pr] * dtile[p] + kc * 256;
+                        const bool main = (pr == 0);
+                        tc::mma_bf16(main ? dm : dc, tc::smem_desc(a, 128, sbo), tc::smem_desc(b, 128, sbo), idesc,
+                                     main ? accm : accc);
+                        if (main) accm = true; else accc = true;
+                    }
+                to += 3 * ttile[p];
+                dd += 3 * dtile[p];
+            }
+            // intermediate batches recycle the table buffer; the last one releases the epilogue
+            tc::mma_commit(ti == ntab - 1 ? bar_done : bar_mma);
+        }
+        if (!ok) atomicExch(&g_tc_error, 1);
+    }
+    __syncthreads();
+    ok = tc::mbar_wait(bar_done, 0);  // single-phase barrier, bounded
+    if (!ok && lane == 0) atomicExch(&g_tc_error, 2);
+    tc::fence_after_sync();
+    if (ok) {
+        const int j = quarter * 32 + lane;  // TMEM lane = latitude pair
+        const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+        const int L = A.L, nfo = 6 * L + 3, nf = 4 * L + 1;
+        const bool has1 = Kq[1] > 0;
+        for (int cc = half * 16; cc < ncp; cc += 32) {
+            float d[4][16];
+            uint32_t rm[4][16], rc[4][16];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int ti = r >> 1, p = r & 1;
+                if (ti >= ntab || (p == 1 && !has1)) continue;
+                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp + cc), rm[r]);
+                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp + cc), rc[r]);
+            }
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const bool z = (r >> 1) >= ntab || ((r & 1) && !has1);
+#pragma unroll
+                for (int i = 0; i < 16; i++) d[r][i] = z ? 0.f : __uint_as_float(rm[r][i]) + __uint_as_float(rc[r][i]);
+            }
+            if (j >= A.nlath) continue;
+            const int latN = j, latS = A.nlat - 1 - j;
+            if (group < 2) {
+                // P-type qi: N = D0 + D1, S = D0 - D1; Q-type qj: S = D1 - D0
+                const float ss = group == 0 ? 1.f : -1.f;
+#pragma unroll
+                for (int i = 0; i < 16; i += 2) {
+                    if (cc + i >= nc) break;
+                    const int gq = (c0 + cc + i) >> 1;
+                    int inst, f;
+                    if (group == 0) { inst = gq / nf; f = gq % nf; }
+                    else { inst = gq; f = 4 * L; }
+                    float2 vn = make_float2(d[0][i] + d[1][i], d[0][i + 1] + d[1][i + 1]);
+                    float2 vs = make_float2(ss * (d[0][i] - d[1][i]), ss * (d[0][i + 1] - d[1][i + 1]));
+                    int F;
+                    if (group == 1) F = 6 * L;                    // gpj
+                    else if (f < L) F = 3 * L + f;                // sd -> gd
+                    else if (f < 2 * L) F = f + L;                // st -> gt
+                    else if (f < 4 * L) F = f + 2 * L;            // sz -> gz, sq -> gq
+                    else F = 6 * L + 2;                           // sp -> gp
+                    const size_t rb = (size_t)m * A.nrows + (size_t)(inst * nfo + F) * A.nlat;
+                    A.W[rb + latN] = vn;
+                    A.W[rb + latS] = vs;
+                    if (group == 0 && f == 4 * L) {               // gpmt = i*m*gp
+                        const float fm = (float)m;
+                        const size_t rt = (size_t)m * A.nrows + (size_t)(inst * nfo + 6 * L + 1) * A.nlat;
+                        A.W[rt + latN] = make_float2(-fm * vn.y, fm * vn.x);
+                        A.W[rt + latS] = make_float2(-fm * vs.y, fm * vs.x);
+                    }
+                }
+            } else {
+                // dv2uv: u = qv*Z - i*qu*D, v = -i*qu*Z - qv*D; qu P-type, qv Q-type
+                // d[0]=qu p0, d[1]=qu p1, d[2]=qv p0, d[3]=qv p1; columns Dr,Di,Zr,Zi per level
+#pragma unroll
+                for (int i = 0; i < 16; i += 4) {
+                    if (cc + i >= nc) break;
+                    const int gc = c0 + cc + i;
+                    const int inst = gc / (4 * L), l = (gc % (4 * L)) >> 2;
+                    const int Dr = i, Di = i + 1, Zr = i + 2, Zi = i + 3;
+                    const float urs = d[0][Di] + d[3][Zr], ura = d[1][Di] + d[2][Zr];
+                    const float uis = -d[0][Dr] + d[3][Zi], uia = -d[1][Dr] + d[2][Zi];
+                    const float vrs = d[0][Zi] - d[3][Dr], vra = d[1][Zi] - d[2][Dr];
+                    const float vis = -d[0][Zr] - d[3][Di], via = -d[1][Zr] - d[2][Di];
+                    const size_t ru = (size_t)m * A.nrows + (size_t)(inst * nfo + l) * A.nlat;
+                    const size_t rv = (size_t)m * A.nrows + (size_t)(inst * nfo + L + l) * A.nlat;
+                    A.W[ru + latN] = make_float2(urs + ura, uis + uia);
+                    A.W[ru + latS] = make_float2(urs - ura, uis - uia);
+                    A.W[rv + latN] = make_float2(vrs + vra, vis + via);
+                    A.W[rv + latS] = make_float2(vrs - vra, vis - via);
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 512);
+}
+
+static size_t inv_smem(int nj8, int K, int ncp) {
+    const int Kp0 = pad16(kpar(K, 0)), Kp1 = pad16(kpar(K, 1));
+    return 3 * (size_t)nj8 * (Kp0 + Kp1) * 2 + 3 * (size_t)ncp * (Kp0 + Kp1) * 2 + (size_t)(128 - nj8) * 64 * 2 +
+           128 + 80;
+}
+
+// ------------------------------------------------------------ forward
+struct TcFwdArgs {
+    const unsigned char *tab;
+    const long long *off;
+    const int *woff;
+    const float2 *W;        // [m][row], row = (inst*(9L+1) + field)*nlat + lat
+    long long nrows;
+    const float *filt;      // skgpsp
+    float *spout;           // [inst][4L+1][NRSP]
+    const int4 *jobs;
+    int L, nlat, nlath, njc, ntp1, nrsp;
+};
+
+// Columns of one forward job (levels l0..l0+nl-1 of one instance), per table,
+// laid out as if the slab always had FWD_LEV_TILE levels (fixed positions):
+//   column (fi, li, ri) = (fi*FWD_LEV_TILE + li)*2 + ri
+//   qc: tn, qn [+ gvpp at 2*2*FWD_LEV_TILE]   qe: fv, vt, fu, vq   qm: fu, ut, fv, uq   qq: ke
+// gpin field kinds: gtn 0, gqn 1, gut 2, gvt 3, guz 4, gvz 5, gke 6, gvpp 7, guq 8, gvq 9;
+// mktend call: tn=gtn, fu=gvz, fv=guz, ke=gke, ut=gut, vt=gvt; qtend: qn=gqn, uq=guq, vq=gvq
+constexpr int NLT = FWD_LEV_TILE;
+__device__ __constant__ int c_fwd_nf[4] = {2, 4, 4, 1};
+__device__ __constant__ int c_fwd_fields[4][4] = {{0, 1, -1, -1}, {4, 3, 5, 9}, {5, 2, 4, 8}, {6, -1, -1, -1}};
+__host__ __device__ constexpr int fwd_ncol(int t) { return t == 0 ? 2 * NLT * 2 + 2 : (t == 3 ? NLT * 2 : 4 * NLT * 2); }
+__host__ __device__ constexpr int fwd_ncp(int t) { return (fwd_ncol(t) + 15) & ~15; }
+__host__ __device__ constexpr int fwd_colbase(int t) {
+    return t == 0 ? 0 : fwd_colbase(t - 1) + 4 * fwd_ncp(t - 1);  // 2 parities x (main, correction)
+}
+
+__device__ __forceinline__ long long fwd_row(int L, int inst, int kind, int l) {
+    const int nfi = 9 * L + 1;
+    int F;
+    if (kind == 7) F = 7 * L;
+    else if (kind < 7) F = kind * L + l;
+    else F = 7 * L + 1 + (kind - 8) * L + l;
+    return (long long)inst * nfi + F;
+}
+
+__global__ void __launch_bounds__(TCT2) k_tc_forward(TcFwdArgs A) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const int4 jb = A.jobs[blockIdx.x];
+    const int m = jb.x, inst = jb.y, l0 = jb.z, nl = jb.w;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, half = warp >> 2;
+    const int K = A.ntp1 - m;
+    const int Kq[2] = {kpar(K, 0), kpar(K, 1)};
+    const int R[2] = {pad8(Kq[0]), pad8(Kq[1])};
+    const int njc = A.njc, L = A.L, nlat = A.nlat;
+    const bool with_vpp = (l0 == 0);
+    size_t tblk = 0;
+    for (int p = 0; p < 2; p++) if (Kq[p]) tblk += 3 * (size_t)R[p] * njc * 2;
+    // rows >= R of the M=128 table tiles read past the block: keep a margin
+    // before the data so those reads (whose TMEM lanes are never used) stay in bounds
+    unsigned char *tab = sm;
+    unsigned char *dat = sm + tblk + 128 * 32 * 2;
+    size_t doffs[4], dbytes = 0;
+    for (int t = 0; t < 4; t++) { doffs[t] = dbytes; dbytes += 2 * 3 * (size_t)fwd_ncp(t) * njc * 2; }
+    unsigned char *tail = dat + dbytes;
+    uint64_t *bar_tma = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
+    uint64_t *bar_mma = bar_tma + 1;
+    uint64_t *bar_done = bar_tma + 2;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar_tma + 3);
+    if (warp == 0) tc::tmem_alloc(slot, 512);
+    if (tid == 0) {
+        tc::mbar_init(bar_tma, 1);
+        tc::mbar_init(bar_mma, 1);
+        tc::mbar_init(bar_done, 1);
+        tc::mbar_fence_init();
+        tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tblk);
+        tc::bulk_g2s(tab, A.tab + A.off[m * 4 + 0], (uint32_t)tblk, bar_tma);
+    }
+    // stage folded Fourier columns: for each table, S (= N+S) and D (= N-S)
+    // versions; each complex W value feeds the re and im columns of its pair
+    for (int t = 0; t < 4; t++) {
+        const int nf = c_fwd_nf[t];
+        const int ncp = fwd_ncp(t), npair = ncp >> 1;
+        const int nreal = nf * NLT + ((t == 0) ? 1 : 0);  // column pairs in use (incl. padding levels)
+        const size_t dt = (size_t)ncp * njc * 2;           // one split tile
+        unsigned char *bS = dat + doffs[t], *bD = bS + 3 * dt;
+        for (int idx = tid; idx < npair * njc; idx += TCT2) {
+            const int q = idx / njc, j = idx - q * njc;
+            float2 vn = make_float2(0.f, 0.f), vs = vn;
+            if (q < nreal && j < A.nlath) {
+                long long rb = -1;
+                if (t == 0 && q == nf * NLT) { if (with_vpp) rb = fwd_row(L, inst, 7, 0); }
+                else {
+                    const int fi = q / NLT, li = q - fi * NLT;
+                    if (li < nl) rb = fwd_row(L, inst, c_fwd_fields[t][fi], l0 + li);
+                }
+                if (rb >= 0) {
+                    const size_t base = (size_t)m * A.nrows + (size_t)rb * nlat;
+                    vn = A.W[base + j];
+                    vs = A.W[base + nlat - 1 - j];
+                }
+            }
+            const float S[2] = {vn.x + vs.x, vn.y + vs.y}, D[2] = {vn.x - vs.x, vn.y - vs.y};
+#pragma unroll
+            for (int ri = 0; ri < 2; ri++) {
+                const uint32_t o = tc::kmajor_off(2 * q + ri, j, njc);
+                __nv_bfloat16 h, mm, l;
+                tc::split3(S[ri], h, mm, l);
+                *reinterpret_cast<__nv_bfloat16 *>(bS + o) = h;
+                *reinterpret_cast<__nv_bfloat16 *>(bS + dt + o) = mm;
+                *reinterpret_cast<__nv_bfloat16 *>(bS + 2 * dt + o) = l;
+                tc::split3(D[ri], h, mm, l);
+                *reinterpret_cast<__nv_bfloat16 *>(bD + o) = h;
+                *reinterpret_cast<__nv_bfloat16 *>(bD + dt + o) = mm;
+                *reinterpret_cast<__nv_bfloat16 *>(bD + 2 * dt + o) = l;
+            }
+        }
+    }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    bool ok = true;
+    if (tid == 0) {
+        for (int t = 0; t < 4 && ok; t++) {
+            if (t > 0) {
+                ok = tc::mbar_wait(bar_mma, (t - 1) & 1);
+                if (!ok) break;
+                tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tblk);
+                tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t], (uint32_t)tblk, bar_tma);
+            }
+            ok = tc::mbar_wait(bar_tma, t & 1);
+            if (!ok) break;
+            tc::fence_after_sync();
+            const int ncp = fwd_ncp(t);
+            const uint32_t idesc = tc::idesc_bf16(128, ncp);
+            const size_t dt = (size_t)ncp * njc * 2;
+            size_t to = 0;
+            for (int p = 0; p < 2; p++) {
+                if (!Kq[p]) break;
+                // P-type (qc, qm, qq) use N+S on even n-m and N-S on odd; Q-type (qe) the reverse
+                const bool ptype = (t != 1);
+                const int sel = (ptype ? p : 1 - p);  // 0 -> S, 1 -> D
+                const unsigned char *dsel = dat + doffs[t] + (size_t)sel * 3 * dt;
+                const uint32_t dm = tmem + (uint32_t)(fwd_colbase(t) + (2 * p + 0) * ncp);
+                const uint32_t dc = tmem + (uint32_t)(fwd_colbase(t) + (2 * p + 1) * ncp);
+                bool accm = false, accc = false;
+                size_t jo = 0;
+                for (int j0 = 0; j0 < njc; j0 += 32) {
+                    const int jw = njc - j0 < 32 ? njc - j0 : 32;
+                    const size_t tt = (size_t)R[p] * jw * 2;
+                    for (int kc = 0; kc < jw / 16; kc++)
+                        for (int pr = 0; pr < 6; pr++) {
+                            const unsigned char *a = tab + to + jo + c_pair_a[pr] * tt + kc * 256;
+                            const unsigned char *b = dsel + c_pair_b[pr] * dt + (size_t)(j0 / 8) * 128 + kc * 256;
+                            const bool main = (pr == 0);
+                            tc::mma_bf16(main ? dm : dc, tc::smem_desc(a, 128, (uint32_t)(jw / 8) * 128),
+                                         tc::smem_desc(b, 128, (uint32_t)(njc / 8) * 128), idesc,
+                                         main ? accm : accc);
+                            if (main) accm = true; else accc = true;
+                        }
+                    jo += 3 * tt;
+                }
+                to += jo;
+            }
+            tc::mma_commit(t == 3 ? bar_done : bar_mma);
+        }
+        if (!ok) atomicExch(&g_tc_error, 3);
+    }
+    __syncthreads();
+    ok = tc::mbar_wait(bar_done, 0);
+    if (!ok && lane == 0) atomicExch(&g_tc_error, 4);
+    tc::fence_after_sync();
+    // epilogue: warp half h drains parity h; TMEM lane = mode index k'
+    const int p = half;
+    if (ok && Kq[p]) {
+        const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+        const int kk = quarter * 32 + lane;
+        const bool valid = kk < Kq[p];
+        // outputs per level: d, t, z, q (re, im)
+        float od[NLT][2], ot[NLT][2], oz[NLT][2], oq[NLT][2], ov[2] = {0.f, 0.f};
+#pragma unroll
+        for (int li = 0; li < NLT; li++)
+            for (int ri = 0; ri < 2; ri++) od[li][ri] = ot[li][ri] = oz[li][ri] = oq[li][ri] = 0.f;
+        uint32_t rm[32], rc[32];
+        float v[32];
+        // table qc (t=0): tn -> t, qn -> q, gvpp -> spf
+        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(0) + (2 * p) * fwd_ncp(0)), rm);
+        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(0) + (2 * p + 1) * fwd_ncp(0)), rc);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 32; i++) v[i] = __uint_as_float(rm[i]) + __uint_as_float(rc[i]);
+#pragma unroll
+        for (int li = 0; li < NLT; li++) {
+            ot[li][0] += v[(0 * NLT + li) * 2]; ot[li][1] += v[(0 * NLT + li) * 2 + 1];
+            oq[li][0] += v[(1 * NLT + li) * 2]; oq[li][1] += v[(1 * NLT + li) * 2 + 1];
+        }
+        ov[0] = v[2 * NLT * 2]; ov[1] = v[2 * NLT * 2 + 1];
+        // table qe (t=1): fv -> d (-), vt -> t, fu -> z, vq -> q
+        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(1) + (2 * p) * fwd_ncp(1)), rm);
+        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(1) + (2 * p + 1) * fwd_ncp(1)), rc);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 32; i++) v[i] = __uint_as_float(rm[i]) + __uint_as_float(rc[i]);
+#pragma unroll
+        for (int li = 0; li < NLT; li++)
+#pragma unroll
+            for (int ri = 0; ri < 2; ri++) {
+                od[li][ri] -= v[(0 * NLT + li) * 2 + ri];
+                ot[li][ri] += v[(1 * NLT + li) * 2 + ri];
+                oz[li][ri] += v[(2 * NLT + li) * 2 + ri];
+                oq[li][ri] += v[(3 * NLT + li) * 2 + ri];
+            }
+        // table qm (t=2): i*fu -> d, -i*ut -> t, i*fv -> z, -i*uq -> q  (i*(a+ib) = -b + ia)
+        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(2) + (2 * p) * fwd_ncp(2)), rm);
+        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(2) + (2 * p + 1) * fwd_ncp(2)), rc);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 32; i++) v[i] = __uint_as_float(rm[i]) + __uint_as_float(rc[i]);
+#pragma unroll
+        for (int li = 0; li < NLT; li++) {
+            const float fur = v[(0 * NLT + li) * 2], fui = v[(0 * NLT + li) * 2 + 1];
+            const float utr = v[(1 * NLT + li) * 2], uti = v[(1 * NLT + li) * 2 + 1];
+            const float fvr = v[(2 * NLT + li) * 2], fvi = v[(2 * NLT + li) * 2 + 1];
+            const float uqr = v[(3 * NLT + li) * 2], uqi = v[(3 * NLT + li) * 2 + 1];
+            od[li][0] -= fui; od[li][1] += fur;
+            ot[li][0] += uti; ot[li][1] -= utr;
+            oz[li][0] -= fvi; oz[li][1] += fvr;
+            oq[li][0] += uqi; oq[li][1] -= uqr;
+        }
+        // table qq (t=3): ke -> d
+        tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(3) + (2 * p) * fwd_ncp(3)), rm);
+        tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(3) + (2 * p + 1) * fwd_ncp(3)), rc);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int li = 0; li < NLT; li++) {
+            od[li][0] += __uint_as_float(rm[2 * li]) + __uint_as_float(rc[2 * li]);
+            od[li][1] += __uint_as_float(rm[2 * li + 1]) + __uint_as_float(rc[2 * li + 1]);
+        }
+        if (valid) {
+            const int k = 2 * kk + p;  // n - m
+            const float fl = A.filt[m + k];
+            const size_t wo = 2 * (size_t)(A.woff[m] + k);
+            const int nfo = 4 * L + 1;
+#pragma unroll
+            for (int li = 0; li < NLT; li++) {
+                if (li >= nl) break;
+                const int l = l0 + li;
+                float2 *sd = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + l) * A.nrsp + wo);
+                float2 *st = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + L + l) * A.nrsp + wo);
+                float2 *sz = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + 2 * L + l) * A.nrsp + wo);
+                float2 *sq = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + 3 * L + l) * A.nrsp + wo);
+                *sd = make_float2(od[li][0] * fl, od[li][1] * fl);
+                *st = make_float2(ot[li][0] * fl, ot[li][1] * fl);
+                *sz = make_float2(oz[li][0] * fl, oz[li][1] * fl);
+                *sq = make_float2(oq[li][0] * fl, oq[li][1] * fl);
+            }
+            if (with_vpp) {
+                float2 *sp = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + 4 * L) * A.nrsp + wo);
+                *sp = make_float2(ov[0] * fl, ov[1] * fl);
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 512);
+}
+
+static size_t fwd_smem(int K, int njc) {
+    size_t tblk = 0;
+    for (int p = 0; p < 2; p++) {
+        const int Kq = kpar(K, p);
+        if (Kq) tblk += 3 * (size_t)pad8(Kq) * njc * 2;
+    }
+    size_t d = 0;
+    for (int t = 0; t < 4; t++) d += 2 * 3 * (size_t)fwd_ncp(t) * njc * 2;
+    return tblk + 128 * 32 * 2 + d + 80;
+}
