@@ -81,6 +81,7 @@ SIGNATURES = {
     "exotx_tc_selftest": [_P, _P, _P, _I, _I, _I, _S],
     "exotx_inverse_set_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_forward_set_batch": [_P, _I, _P, _P, _I, _I, _S],
+    "exotx_forward_set_noalloc": [_P, _I, _P, _P, _I, _S],
     "exotx_tc_error": [C.POINTER(_I), _S],
 }
 RESTYPES = {"exotx_fft_supported": C.c_int, "exotx_launch_count": C.c_ulonglong,

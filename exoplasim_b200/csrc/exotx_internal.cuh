@@ -111,6 +111,13 @@ exotx_status fft_forward_l(const T *in, T *out, int n, long long lot, int kout, 
 template <typename T>
 exotx_status fft_inverse_l(const T *in, T *out, int n, long long lot, int kin, long long f_rs, long long f_ms,
                            cudaStream_t s);
+// twiddle tables on the host (w: n/2 complex, r: n/2+1 complex) and a forward
+// FFT reading them from caller-provided device memory (no allocation)
+template <typename T>
+void fft_twiddles_host(int n, T *w, T *r);
+template <typename T>
+exotx_status fft_forward_tw(const T *in, T *out, int n, long long lot, int kout, long long f_rs, long long f_ms,
+                            const T *w, const T *r, cudaStream_t s);
 
 // tensor-core Legendre (legendre_tc.cu)
 exotx_status tc_inverse_set(exotx_plan p, const float *spin, float *four, int nlev, cudaStream_t s);

@@ -573,6 +573,56 @@ template exotx_status fft_inverse_l<double>(const double *, double *, int, long 
 template exotx_status fft_inverse_l<float>(const float *, float *, int, long long, int, long long, long long,
                                            cudaStream_t);
 
+// ----------------------------------------------- caller-supplied twiddle tables
+// The twiddle values the cached tables hold (same long-double evaluation, so
+// the transforms agree bit for bit), written into caller buffers of h and h+1
+// complex values.
+template <typename T>
+void fft_twiddles_host(int n, T *w, T *r) {
+    const int h = n / 2;
+    const long double PI_L = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < h; k++) {
+        long double a = -2.0L * PI_L * (long double)k / (long double)h;
+        w[2 * k] = (T)cosl(a); w[2 * k + 1] = (T)sinl(a);
+    }
+    for (int k = 0; k <= h; k++) {
+        long double a = -2.0L * PI_L * (long double)k / (long double)n;
+        r[2 * k] = (T)cosl(a); r[2 * k + 1] = (T)sinl(a);
+    }
+}
+template void fft_twiddles_host<double>(int, double *, double *);
+template void fft_twiddles_host<float>(int, float *, float *);
+
+// fft_forward_l with the twiddles in caller memory (device pointers laid out
+// as fft_twiddles_host writes them); launches the same kernels and allocates
+// nothing.
+template <typename T>
+exotx_status fft_forward_tw(const T *in, T *out, int n, long long lot, int kout, long long f_rs, long long f_ms,
+                            const T *w, const T *r, cudaStream_t s) {
+    if (!exotx_fft_supported(n)) return EXOTX_UNSUPPORTED_N;
+    if (lot <= 0) return EXOTX_OK;
+    const cpx<T> *wc = reinterpret_cast<const cpx<T> *>(w), *rc = reinterpret_cast<const cpx<T> *>(r);
+    if (aligned16(in) && aligned16(out)) {
+        exotx_status sc = dispatch_ct<T>(true, n, in, out, lot, kout, f_rs, f_ms, wc, rc, s);
+        if (sc != EXOTX_NOT_BUILT) return sc;
+    }
+    FftTables t;  // radix schedule only
+    t.n = n;
+    t.h = n / 2;
+    factor_h(t.h, t.fac, &t.nfac);
+    size_t smem;
+    FftLaunch L = make_launch<T>(&t, lot, kout, f_rs, f_ms, &smem);
+    EXOTX_TRY(set_smem<T>((const void *)k_rfft_forward<T>, smem));
+    long long nb = (lot + L.rows_per_block - 1) / L.rows_per_block;
+    k_rfft_forward<T><<<(unsigned)nb, 256, smem, s>>>(in, out, L, wc, rc);
+    EXOTX_CHECK_LAUNCH();
+    return EXOTX_OK;
+}
+template exotx_status fft_forward_tw<double>(const double *, double *, int, long long, int, long long, long long,
+                                             const double *, const double *, cudaStream_t);
+template exotx_status fft_forward_tw<float>(const float *, float *, int, long long, int, long long, long long,
+                                            const float *, const float *, cudaStream_t);
+
 }  // namespace exotx
 
 EXOTX_API int exotx_fft_supported(int n) {

@@ -207,6 +207,22 @@ class Plan:
         call("exotx_forward_set", self._h, p, _ptr(gpin), _ptr(out), nlev, _stream())
         return out
 
+    # size of the library's fixed scratch array used by forward_set_noalloc
+    STATIC_WORK_BYTES = 16 << 20
+
+    def forward_set_noalloc(self, gpin, nlev, out, precision="fp64"):
+        """forward_set for callers that cannot allocate device memory: the
+        Fourier intermediate and FFT twiddles live in a fixed array of
+        STATIC_WORK_BYTES inside the library (shared by all calls on a device;
+        calls that overlap on the GPU race).  `out` must be given.  Sets that
+        need more scratch than the array holds raise ExotxError (BAD_DIM)."""
+        p = _prec(precision)
+        dt = _dtype(p)
+        _check(gpin, dt, (9 * nlev + 1, self.nlat, self.nlon), "gpin")
+        _check(out, dt, (4 * nlev + 1, self.nrsp), "spout")
+        call("exotx_forward_set_noalloc", self._h, p, _ptr(gpin), _ptr(out), nlev, _stream())
+        return out
+
 
     def inverse_set_batch(self, spin, nlev, precision="mixed", out=None):
         """inverse_set for ninst states stored back to back: (ninst, 4L+1, NRSP) -> (ninst, 6L+3, NLAT, NLON)."""

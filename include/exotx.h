@@ -126,6 +126,26 @@ exotx_status exotx_inverse_set_batch(exotx_plan p, int prec, const void *spin, v
                                      int nlev, int ninst, exotx_stream s);
 exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const void *gpin, void *spout,
                                      int nlev, int ninst, exotx_stream s);
+/* forward_set that allocates no device memory.  No counterpart in the
+ * reference (which has no device memory to allocate); it exists for callers
+ * that cannot call cudaMalloc where they transform -- a host model whose own
+ * pool already holds the device memory, or a timestep loop that must not stall
+ * on an allocation call.  exotx_forward_set may grow the plan's work buffer and
+ * build FFT twiddle tables on first use; this variant keeps both in a fixed
+ * array inside the library of EXOTX_STATIC_WORK_BYTES bytes per GPU, held from
+ * the library's first use on that GPU until process exit.  It needs
+ *   256-rounded (NLON/2 + NLON/2+1) complex twiddles + (9L+1)*NLAT*(NTRU+1) complex
+ * of prec's size (FP64: T42 L20 fits, T63 L20 does not; FP32: T63 L20 fits)
+ * and returns EXOTX_BAD_DIM, before any work, for sets that need more.
+ * prec is EXOTX_FP64 or EXOTX_FP32 (EXOTX_MIXED -> EXOTX_BAD_ARG).  Results
+ * equal exotx_forward_set's.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls on a device share the array: calls
+ * that overlap on the GPU (different streams or threads without
+ * synchronisation between them) race. */
+#define EXOTX_STATIC_WORK_BYTES (16u << 20)
+exotx_status exotx_forward_set_noalloc(exotx_plan p, int prec, const void *gpin, void *spout,
+                                       int nlev, exotx_stream s);
 /* Error word of the tensor-core kernels (0 = none; nonzero = a bounded
  * device-side wait gave up), read after synchronising the stream, then reset. */
 exotx_status exotx_tc_error(int *code, exotx_stream s);
