@@ -42,11 +42,28 @@ def fp32_round_trip_bytes(nlat, nlev):
     return 2 * (4 * nlev + 1) * nrsp * 4 + (15 * nlev + 4) * nhor * 4
 
 
-def legendre_flops(nlat, nlev):
-    """Algorithmic folded Legendre flops of one round trip: (19L+3) * 2 NLAT NCSP."""
+def legendre_flops(nlat, nlev, half="both"):
+    """Algorithmic folded Legendre flops of one instance: F_leg = 2 NLAT NCSP per
+    complex field-level; (8L+2) products in the inverse set, (11L+1) in the forward."""
     ntru = (2 * nlat - 1) // 3
     ncsp = (ntru + 1) * (ntru + 2) // 2
-    return (19 * nlev + 3) * 2 * nlat * ncsp
+    nprod = {"inverse": 8 * nlev + 2, "forward": 11 * nlev + 1, "both": 19 * nlev + 3}[half]
+    return nprod * 2 * nlat * ncsp
+
+
+def fft_bytes(nlat, nlev, half, esz):
+    """Algorithmic bytes of one instance's FFT stage: grid rows of NLON reals on
+    one side, NTRU+1 complex Fourier coefficients per row on the other."""
+    ntru = (2 * nlat - 1) // 3
+    nlon = 2 * nlat
+    rows = ((6 * nlev + 3) if half == "inverse" else (9 * nlev + 1)) * nlat
+    return rows * (nlon * esz + (ntru + 1) * 2 * esz)
+
+
+# DRAM bytes per launch of the dominant kernel from one ncu capture (dram__bytes_read.sum
+# + dram__bytes_write.sum), keyed by (kernel, workload); the summary with its command is
+# in profiles/.
+NCU_TRAFFIC = {}
 
 
 def args_():
@@ -57,6 +74,9 @@ def args_():
     a.add_argument("--impl", default="ours", choices=["ours", "reference"])
     a.add_argument("--batch", type=int, default=8, help="T127 L20 instances per step and rank")
     a.add_argument("--no-cpu-baseline", action="store_true")
+    a.add_argument("--precisions", default="mixed,fp32,fp64",
+                   help="transform paths to time, first = headline (profiling runs pass one)")
+    a.add_argument("--skip-radiation", action="store_true")
     return a.parse_args()
 
 
@@ -174,7 +194,7 @@ def run_ours(a, rank, world, local_rank):
 
     from exoplasim_b200 import radiation as R
     from exoplasim_b200 import synthetic as S
-    from exoplasim_b200.transforms import Plan, launch_count
+    from exoplasim_b200.transforms import Plan, kernel_time, kernel_timing, launch_count
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -246,15 +266,7 @@ def run_ours(a, rank, world, local_rank):
     step_fn("fp64", b64)()
     torch.cuda.synchronize()
     ref_gout, ref_sout = b64[2][0].clone(), b64[3][0].clone()
-    precisions = ["fp32", "fp64"]
-    try:
-        from exoplasim_b200 import _lib
-        bm = make(torch.float32)
-        step_fn("mixed", bm)()
-        torch.cuda.synchronize()
-        precisions = ["mixed"] + precisions
-    except Exception as e:  # the tensor-core path is optional until built
-        results["mixed_unavailable"] = str(e)
+    precisions = [p for p in a.precisions.split(",") if p]
     clocks = Clocks(local_rank)
     for prec in precisions:
         bufs = b64 if prec == "fp64" else make(torch.float32)
@@ -272,22 +284,56 @@ def run_ours(a, rank, world, local_rank):
         del bufs
     primary = precisions[0]
 
-    # per-stage timing of the primary precision (dominant stage for the roofline)
+    # per-stage timing of the primary precision
     bufs = make(torch.float32) if primary != "fp64" else make(torch.float64)
     inv_ms, _ = time_graph(lambda: plan.inverse_set_batch(bufs[0], NLEV, primary, out=bufs[2]), a.steps, a.warmup)
     fwd_ms, _ = time_graph(lambda: plan.forward_set_batch(bufs[1], NLEV, primary, out=bufs[3]), a.steps, a.warmup)
     hbm, tc, peak_kind = peaks()
-    ntru = plan.ntru
-    nrsp = plan.nrsp
-    nhor = plan.nhor
     esz = 4 if primary != "fp64" else 8
-    inv_bytes = ((4 * NLEV + 1) * nrsp + (6 * NLEV + 3) * nhor) * esz
-    fwd_bytes = ((4 * NLEV + 1) * nrsp + (9 * NLEV + 1) * nhor) * esz
-    if fwd_ms >= inv_ms:
-        dom, dom_ms, dom_bytes = "forward_set", fwd_ms / (a.steps * B), fwd_bytes
-    else:
-        dom, dom_ms, dom_bytes = "inverse_set", inv_ms / (a.steps * B), inv_bytes
-    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
+
+    # per-kernel device time: each launch bracketed by CUDA events on its own
+    # stream (the library's kernel timer), over K eager steps of the same work
+    fn = step_fn(primary, bufs)
+    for _ in range(a.warmup):
+        fn()
+    torch.cuda.synchronize()
+    kernel_timing(True)
+    for _ in range(a.steps):
+        fn()
+    torch.cuda.synchronize()
+    leg = "tc" if primary == "mixed" else "leg"
+    units = {f"{leg}_inverse": ("tensor" if leg == "tc" else "fma", legendre_flops(NLAT, NLEV, "inverse")),
+             f"{leg}_forward": ("tensor" if leg == "tc" else "fma", legendre_flops(NLAT, NLEV, "forward")),
+             "fft_inverse": ("hbm", fft_bytes(NLAT, NLEV, "inverse", esz)),
+             "fft_forward": ("hbm", fft_bytes(NLAT, NLEV, "forward", esz))}
+    kernels = {}
+    for name, (bound, per_inst) in units.items():
+        kms, nl = kernel_time(name)
+        if nl == 0:
+            continue
+        work = per_inst * B * a.steps            # algorithmic flops or bytes over the timed steps
+        rate = work / (kms / 1000.0)
+        if bound == "hbm":
+            ach, pk, unit = rate / 1e9, hbm, "GB/s"
+        elif bound == "tensor":
+            ach, pk, unit = rate / 1e12, tc, "TFLOP/s"
+        else:  # SIMT FMA path: no measured peak to divide by
+            ach, pk, unit = rate / 1e12, None, "TFLOP/s"
+        kernels[name] = {"bound": bound, "ms_total": kms, "launches": nl, "ms_per_launch": kms / nl,
+                         "achieved": ach, "peak": pk, "unit": unit, "frac": ach / pk if pk else None,
+                         "share": None, "algorithmic_per_launch": work / nl}
+    kernel_timing(False)
+    tot = sum(k["ms_total"] for k in kernels.values())
+    for k in kernels.values():
+        k["share"] = k["ms_total"] / tot
+    dom = max(kernels, key=lambda k: kernels[k]["ms_total"])
+    D = kernels[dom]
+    roof = {"bound": "tensor" if D["bound"] == "tensor" else "hbm", "kernel": dom, "achieved": D["achieved"],
+            "peak": D["peak"], "unit": D["unit"], "frac": D["frac"],
+            "traffic": NCU_TRAFFIC.get((dom, WORKLOAD)), "peak_kind": peak_kind,
+            "algorithmic_per_launch": D["algorithmic_per_launch"],
+            "algorithmic_unit": "flops" if D["unit"] == "TFLOP/s" else "bytes",
+            "ms_per_launch": D["ms_per_launch"]}
     del bufs
 
     # end to end through the public API with host buffers
@@ -325,7 +371,7 @@ def run_ours(a, rank, world, local_rank):
     # radiation column pass: 8192 columns at L20 (T42 grid), plain kernel
     cols, g = S.radiation_columns(RAD_NLAT, RAD_NLEV, seed=2 + rank)
     rad = {}
-    for rprec, rdt in (("fp64", torch.float64), ("fp32", torch.float32)):
+    for rprec, rdt in (() if a.skip_radiation else (("fp64", torch.float64), ("fp32", torch.float32))):
         dev_cols = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=rdt, device=dev) for k, v in cols.items()}
         params = R.default_params(RAD_NLEV, g["nhor"], g["nlon"], nsol=0)
         outs = R.alloc_outputs(params, rdt)
@@ -358,9 +404,8 @@ def run_ours(a, rank, world, local_rank):
                    "l2": f"inputs larger than L2: {B} instances x {fp32_round_trip_bytes(NLAT, NLEV) / 1e6:.0f} MB",
                    "parallelism": f"replicas x{world} (independent instances)"},
         "precisions": results,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": dom_bytes},
+        "roofline": roof,
+        "kernels": kernels,
         "stages_ms_per_instance": {"inverse_set": inv_ms / (a.steps * B), "forward_set": fwd_ms / (a.steps * B)},
         "e2e": {"value": world * B * a.steps / (e2e_ms / 1000.0), "unit": "round-trips/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -82,6 +82,8 @@ SIGNATURES = {
     "exotx_inverse_set_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_forward_set_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_forward_set_noalloc": [_P, _I, _P, _P, _I, _S],
+    "exotx_kernel_timing": [_I],
+    "exotx_kernel_time": [_I, C.POINTER(_D), C.POINTER(C.c_longlong)],
     "exotx_tc_error": [C.POINTER(_I), _S],
 }
 RESTYPES = {"exotx_fft_supported": C.c_int, "exotx_launch_count": C.c_ulonglong,

@@ -119,6 +119,11 @@ template <typename T>
 exotx_status fft_forward_tw(const T *in, T *out, int n, long long lot, int kout, long long f_rs, long long f_ms,
                             const T *w, const T *r, cudaStream_t s);
 
+// per-kernel event timing (ktimer.cu): start returns nullptr when timing is
+// off or the stream is capturing; stop records the pair
+cudaEvent_t ktimer_start(int kernel, cudaStream_t s);
+void ktimer_stop(int kernel, cudaStream_t s, cudaEvent_t e0);
+
 // tensor-core Legendre (legendre_tc.cu)
 exotx_status tc_inverse_set(exotx_plan p, const float *spin, float *four, int nlev, cudaStream_t s);
 exotx_status tc_forward_set(exotx_plan p, const float *four, float *spout, int nlev, cudaStream_t s);

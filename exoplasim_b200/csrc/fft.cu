@@ -399,18 +399,23 @@ static exotx_status launch_ct(bool fwd, const T *in, T *out, long long lot, int 
     constexpr int ROWS = ct_rows<T>(N);
     const size_t smem = (2 * ROWS * (N / 2) + N / 2 + N / 2 + 1) * sizeof(cpx<T>);
     const long long nb = (lot + ROWS - 1) / ROWS;
+    const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
     if (fwd) {
         if (smem > 48 * 1024)
             EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_ct<T, N, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem));
-        k_rfft_fwd_ct<T, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, lot, kf, f_rs, f_ms, w, r);
     } else {
         if (smem > 48 * 1024)
             EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_inv_ct<T, N, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem));
-        k_rfft_inv_ct<T, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, lot, kf, f_rs, f_ms, w, r);
     }
+    cudaEvent_t ev = ktimer_start(kid, s);
+    if (fwd)
+        k_rfft_fwd_ct<T, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, lot, kf, f_rs, f_ms, w, r);
+    else
+        k_rfft_inv_ct<T, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, lot, kf, f_rs, f_ms, w, r);
     EXOTX_CHECK_LAUNCH();
+    ktimer_stop(kid, s, ev);
     return EXOTX_OK;
 }
 
@@ -539,8 +544,10 @@ exotx_status fft_forward_l(const T *in, T *out, int n, long long lot, int kout, 
     FftLaunch L = make_launch<T>(t, lot, kout, f_rs, f_ms, &smem);
     EXOTX_TRY(set_smem<T>((const void *)k_rfft_forward<T>, smem));
     long long nb = (lot + L.rows_per_block - 1) / L.rows_per_block;
+    cudaEvent_t ev = ktimer_start(EXOTX_K_FFT_FORWARD, s);
     k_rfft_forward<T><<<(unsigned)nb, 256, smem, s>>>(in, out, L, wt<T>(t), rt<T>(t));
     EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_FFT_FORWARD, s, ev);
     return EXOTX_OK;
 }
 
@@ -559,8 +566,10 @@ exotx_status fft_inverse_l(const T *in, T *out, int n, long long lot, int kin, l
     FftLaunch L = make_launch<T>(t, lot, kin, f_rs, f_ms, &smem);
     EXOTX_TRY(set_smem<T>((const void *)k_rfft_inverse<T>, smem));
     long long nb = (lot + L.rows_per_block - 1) / L.rows_per_block;
+    cudaEvent_t ev = ktimer_start(EXOTX_K_FFT_INVERSE, s);
     k_rfft_inverse<T><<<(unsigned)nb, 256, smem, s>>>(in, out, L, wt<T>(t), rt<T>(t));
     EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_FFT_INVERSE, s, ev);
     return EXOTX_OK;
 }
 
@@ -614,8 +623,10 @@ exotx_status fft_forward_tw(const T *in, T *out, int n, long long lot, int kout,
     FftLaunch L = make_launch<T>(&t, lot, kout, f_rs, f_ms, &smem);
     EXOTX_TRY(set_smem<T>((const void *)k_rfft_forward<T>, smem));
     long long nb = (lot + L.rows_per_block - 1) / L.rows_per_block;
+    cudaEvent_t ev = ktimer_start(EXOTX_K_FFT_FORWARD, s);
     k_rfft_forward<T><<<(unsigned)nb, 256, smem, s>>>(in, out, L, wc, rc);
     EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_FFT_FORWARD, s, ev);
     return EXOTX_OK;
 }
 template exotx_status fft_forward_tw<double>(const double *, double *, int, long long, int, long long, long long,

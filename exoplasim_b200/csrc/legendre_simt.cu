@@ -278,6 +278,7 @@ exotx_status leg_inverse_l(exotx_plan p, int op, const T *a, const T *b, T *oa, 
     size_t smem = per_level * lv;
     dim3 grid(L.mz, (nlev + lv - 1) / lv);
     constexpr int LT = 4;
+    cudaEvent_t ev = ktimer_start(EXOTX_K_LEG_INVERSE, s);
     switch (op) {
         case OP_SP2FC: k_leg_inv<T, OP_SP2FC, LT><<<grid, 128, smem, s>>>(A, lv); break;
         case OP_SP2FCDMU: k_leg_inv<T, OP_SP2FCDMU, LT><<<grid, 128, smem, s>>>(A, lv); break;
@@ -286,6 +287,7 @@ exotx_status leg_inverse_l(exotx_plan p, int op, const T *a, const T *b, T *oa, 
         default: return EXOTX_BAD_ARG;
     }
     EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_LEG_INVERSE, s, ev);
     return EXOTX_OK;
 }
 
@@ -306,6 +308,7 @@ exotx_status leg_forward_l(exotx_plan p, int op, const T *const *in, T *const *o
     size_t smem = per_level * lv;
     if (smem > 48 * 1024) return EXOTX_BAD_DIM;
     dim3 grid(p->ntp1, (nlev + lv - 1) / lv);
+    cudaEvent_t ev = ktimer_start(EXOTX_K_LEG_FORWARD, s);
     switch (op) {
         case OP_FC2SP: k_leg_fwd<T, OP_FC2SP><<<grid, 128, smem, s>>>(A, lv); break;
         case OP_UV2DV: k_leg_fwd<T, OP_UV2DV><<<grid, 128, smem, s>>>(A, lv); break;
@@ -314,6 +317,7 @@ exotx_status leg_forward_l(exotx_plan p, int op, const T *const *in, T *const *o
         default: return EXOTX_BAD_ARG;
     }
     EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_LEG_FORWARD, s, ev);
     return EXOTX_OK;
 }
 

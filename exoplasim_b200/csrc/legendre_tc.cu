@@ -332,8 +332,10 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
         A.jobs = jl;
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.nj8 = T->nj8; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
         A.plavor = (float)p->desc.plavor;
+        cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
         k_tc_inverse<<<nj, TCT2, smem, s>>>(A);
         EXOTX_CHECK_LAUNCH();
+        ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
         EXOTX_TRY(fft_inverse_l<float>((const float *)p->d_work, gpout + (size_t)i0 * nfo * nhor, p->nlon, A.nrows,
                                        p->ntp1, 1, A.nrows, s));
     }
@@ -371,8 +373,10 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
         A.spout = spout + (size_t)i0 * (4 * L + 1) * nrsp;
         A.jobs = jl;
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.njc = T->njc; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
+        cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
         k_tc_forward<<<nj, TCT2, smem, s>>>(A);
         EXOTX_CHECK_LAUNCH();
+        ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
     }
     return EXOTX_OK;
 }

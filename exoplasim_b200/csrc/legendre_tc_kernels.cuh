@@ -8,6 +8,8 @@
 
 constexpr int TCT2 = 256;
 
+__device__ __forceinline__ void st_shared16(unsigned char *p, uint4 v) { *reinterpret_cast<uint4 *>(p) = v; }
+
 // ------------------------------------------------------------ inverse
 struct TcInvArgs {
     const unsigned char *tab;
@@ -22,25 +24,22 @@ struct TcInvArgs {
     float plavor;
 };
 
-// complex spectral input of column pair q (columns 2q, 2q+1 = re, im), filtered
-__device__ __forceinline__ float2 inv_input2(const TcInvArgs &A, int group, int gq, int m, int k) {
+// spectral row (complex, filter not applied) feeding column pair gq, and
+// whether it is the vorticity of a dv2uv pair (planetary vorticity removed)
+__device__ __forceinline__ const float2 *inv_row(const TcInvArgs &A, int group, int gq, bool *zvort) {
     const int L = A.L, nf = 4 * L + 1;
     int inst, f;
-    bool zvort = false;
+    *zvort = false;
     if (group == 0) { inst = gq / nf; f = gq % nf; }
     else if (group == 1) { inst = gq; f = 4 * L; }
     else {
         // columns per level: Dr, Di, Zr, Zi -> pairs 2l (D), 2l+1 (Z)
         inst = gq / (2 * L);
         const int l = (gq % (2 * L)) >> 1;
-        zvort = gq & 1;
-        f = zvort ? 2 * L + l : l;
+        *zvort = gq & 1;
+        f = *zvort ? 2 * L + l : l;
     }
-    const int w = A.woff[m] + k;
-    float2 x = *reinterpret_cast<const float2 *>(A.spin + ((size_t)inst * nf + f) * A.nrsp + 2 * w);
-    if (zvort && m == 0 && k == 1) x.x -= A.plavor;  // dv2uv, legmod.f90:332
-    const float fl = A.filt[m + k];
-    return make_float2(x.x * fl, x.y * fl);
+    return reinterpret_cast<const float2 *>(A.spin + ((size_t)inst * nf + f) * A.nrsp);
 }
 
 __global__ void __launch_bounds__(TCT2) k_tc_inverse(TcInvArgs A) {
@@ -75,27 +74,45 @@ __global__ void __launch_bounds__(TCT2) k_tc_inverse(TcInvArgs A) {
         tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
         tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0], (uint32_t)tbytes, bar_tma);
     }
-    // stage the spectral columns of both parities (one complex load per column pair)
+    // stage the spectral columns of both parities.  A unit is one column pair
+    // (re, im) and 8 modes of one parity: one 16-byte core-matrix row per
+    // column and split term.
     size_t doff = 0;
     for (int p = 0; p < 2; p++) {
         if (!Kq[p]) break;
         const int kp = Kp[p];
-        const int npair = ncp >> 1;
-        for (int idx = tid; idx < npair * kp; idx += TCT2) {
-            const int q = idx / kp, k = idx - q * kp;
+        const int npair = ncp >> 1, ngk = kp >> 3;
+        for (int u = tid; u < npair * ngk; u += TCT2) {
+            const int q = u % npair, g = u / npair;
             const int c = 2 * q;
-            float2 x = make_float2(0.f, 0.f);
-            if (c < nc && k < Kq[p]) x = inv_input2(A, group, (c0 + c) >> 1, m, 2 * k + p);
-            __nv_bfloat16 h, mm, l;
-            const uint32_t o0 = tc::kmajor_off(c, k, kp), o1 = tc::kmajor_off(c + 1, k, kp);
-            tc::split3(x.x, h, mm, l);
-            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + o0) = h;
-            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + dtile[p] + o0) = mm;
-            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + 2 * dtile[p] + o0) = l;
-            tc::split3(x.y, h, mm, l);
-            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + o1) = h;
-            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + dtile[p] + o1) = mm;
-            *reinterpret_cast<__nv_bfloat16 *>(dat + doff + 2 * dtile[p] + o1) = l;
+            float xr[8], xi[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) xr[e] = xi[e] = 0.f;
+            if (c < nc) {
+                bool zv;
+                const float2 *row = inv_row(A, group, (c0 + c) >> 1, &zv);
+                const int w0 = A.woff[m];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int k = 8 * g + e;
+                    if (k < Kq[p]) {
+                        const int nm = 2 * k + p;  // n - m
+                        float2 x = __ldg(row + w0 + nm);
+                        if (zv && m == 0 && nm == 1) x.x -= A.plavor;  // dv2uv, legmod.f90:332
+                        const float fl = __ldg(A.filt + m + nm);
+                        xr[e] = x.x * fl;
+                        xi[e] = x.y * fl;
+                    }
+                }
+            }
+            const uint32_t o = tc::kmajor_off(c, 8 * g, kp);  // re row; the im row follows at +16
+            unsigned char *d0 = dat + doff;
+            uint4 h, mm, l;
+            tc::split3x8(xr, h, mm, l);
+            st_shared16(d0 + o, h); st_shared16(d0 + dtile[p] + o, mm); st_shared16(d0 + 2 * dtile[p] + o, l);
+            tc::split3x8(xi, h, mm, l);
+            st_shared16(d0 + o + 16, h); st_shared16(d0 + dtile[p] + o + 16, mm);
+            st_shared16(d0 + 2 * dtile[p] + o + 16, l);
         }
         doff += 3 * dtile[p];
     }
@@ -127,16 +144,15 @@ __global__ void __launch_bounds__(TCT2) k_tc_inverse(TcInvArgs A) {
                 const uint32_t dm = tmem + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp);
                 const uint32_t dc = tmem + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp);
                 const uint32_t sbo = (uint32_t)(Kp[p] / 8) * 128;
-                bool accm = false, accc = false;
-                for (int kc = 0; kc < Kp[p] / 16; kc++)
-                    for (int pr = 0; pr < 6; pr++) {
-                        const unsigned char *a = tab + to + c_pair_a[pr] * ttile[p] + kc * 256;
-                        const unsigned char *b = dat + dd + c_pair_b[pr] * dtile[p] + kc * 256;
-                        const bool main = (pr == 0);
-                        tc::mma_bf16(main ? dm : dc, tc::smem_desc(a, 128, sbo), tc::smem_desc(b, 128, sbo), idesc,
-                                     main ? accm : accc);
-                        if (main) accm = true; else accc = true;
-                    }
+                const uint64_t da0 = tc::smem_desc(tab + to, 128, sbo), db0 = tc::smem_desc(dat + dd, 128, sbo);
+                const uint32_t tt = (uint32_t)ttile[p], dt = (uint32_t)dtile[p];
+                for (int kc = 0; kc < Kp[p] / 16; kc++) {
+#pragma unroll
+                    for (int pr = 0; pr < 6; pr++)
+                        tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
+                                     tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 256), idesc,
+                                     kc > 0 || pr > 1);
+                }
                 to += 3 * ttile[p];
                 dd += 3 * dtile[p];
             }
@@ -291,57 +307,92 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(TcFwdArgs A) {
     size_t doffs[4], dbytes = 0;
     for (int t = 0; t < 4; t++) { doffs[t] = dbytes; dbytes += 2 * 3 * (size_t)fwd_ncp(t) * njc * 2; }
     unsigned char *tail = dat + dbytes;
-    uint64_t *bar_tma = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
-    uint64_t *bar_mma = bar_tma + 1;
-    uint64_t *bar_done = bar_tma + 2;
-    uint32_t *slot = reinterpret_cast<uint32_t *>(bar_tma + 3);
+    uint64_t *bars = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
+    uint64_t *bar_tma = bars;       // [2] table half of parity p landed
+    uint64_t *bar_mma = bars + 2;   // [2] MMAs reading table half p completed
+    uint64_t *bar_done = bars + 4;  // every MMA completed
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 5);
+    // a table block is [parity 0: 3 splits x R0 rows][parity 1: 3 splits x R1 rows];
+    // the halves travel separately so the next table's half 0 lands while half 1 computes
+    const uint32_t hbytes[2] = {(uint32_t)(3 * R[0] * njc * 2), (uint32_t)(3 * R[1] * njc * 2)};
+    const uint32_t hoff[2] = {0u, hbytes[0]};
     if (warp == 0) tc::tmem_alloc(slot, 512);
     if (tid == 0) {
-        tc::mbar_init(bar_tma, 1);
-        tc::mbar_init(bar_mma, 1);
-        tc::mbar_init(bar_done, 1);
+        for (int i = 0; i < 5; i++) tc::mbar_init(bars + i, 1);
         tc::mbar_fence_init();
-        tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tblk);
-        tc::bulk_g2s(tab, A.tab + A.off[m * 4 + 0], (uint32_t)tblk, bar_tma);
+        for (int p = 0; p < 2; p++)
+            if (Kq[p]) {
+                tc::mbar_arrive_expect_tx(bar_tma + p, hbytes[p]);
+                tc::bulk_g2s(tab + hoff[p], A.tab + A.off[m * 4 + 0] + hoff[p], hbytes[p], bar_tma + p);
+            }
     }
     // stage folded Fourier columns: for each table, S (= N+S) and D (= N-S)
-    // versions; each complex W value feeds the re and im columns of its pair
+    // versions.  A unit is one column pair (re, im of one field-level) and 8
+    // latitude pairs: 16-byte loads of the north and south rows, and one
+    // 16-byte core-matrix row per column, split term and version.
+    const int ng = njc >> 3;
     for (int t = 0; t < 4; t++) {
         const int nf = c_fwd_nf[t];
         const int ncp = fwd_ncp(t), npair = ncp >> 1;
         const int nreal = nf * NLT + ((t == 0) ? 1 : 0);  // column pairs in use (incl. padding levels)
-        const size_t dt = (size_t)ncp * njc * 2;           // one split tile
+        const uint32_t dt = (uint32_t)ncp * njc * 2;       // one split tile
         unsigned char *bS = dat + doffs[t], *bD = bS + 3 * dt;
-        for (int idx = tid; idx < npair * njc; idx += TCT2) {
-            const int q = idx / njc, j = idx - q * njc;
-            float2 vn = make_float2(0.f, 0.f), vs = vn;
-            if (q < nreal && j < A.nlath) {
-                long long rb = -1;
+        const int nunit = npair * ng;
+        for (int u = tid; u < nunit; u += TCT2) {
+            const int q = u % npair, g = u / npair;
+            long long rb = -1;
+            if (q < nreal) {
                 if (t == 0 && q == nf * NLT) { if (with_vpp) rb = fwd_row(L, inst, 7, 0); }
                 else {
                     const int fi = q / NLT, li = q - fi * NLT;
                     if (li < nl) rb = fwd_row(L, inst, c_fwd_fields[t][fi], l0 + li);
                 }
-                if (rb >= 0) {
-                    const size_t base = (size_t)m * A.nrows + (size_t)rb * nlat;
-                    vn = A.W[base + j];
-                    vs = A.W[base + nlat - 1 - j];
+            }
+            const int j0 = 8 * g;
+            float sr[8], si[8], dr[8], di[8];
+            float2 vn[8], vs[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) vn[e] = vs[e] = make_float2(0.f, 0.f);
+            if (rb >= 0) {
+                const float2 *wr = A.W + (size_t)m * A.nrows + (size_t)rb * nlat;
+                if (j0 + 8 <= A.nlath) {
+                    // rows j0..j0+7 north, and nlat-8-j0..nlat-1-j0 south (reversed)
+                    const float4 *pn = reinterpret_cast<const float4 *>(wr + j0);
+                    const float4 *ps = reinterpret_cast<const float4 *>(wr + nlat - 8 - j0);
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float4 x = __ldg(pn + i), y = __ldg(ps + i);
+                        vn[2 * i] = make_float2(x.x, x.y);
+                        vn[2 * i + 1] = make_float2(x.z, x.w);
+                        vs[7 - 2 * i] = make_float2(y.x, y.y);
+                        vs[6 - 2 * i] = make_float2(y.z, y.w);
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 8; e++)
+                        if (j0 + e < A.nlath) {
+                            vn[e] = __ldg(wr + j0 + e);
+                            vs[e] = __ldg(wr + nlat - 1 - j0 - e);
+                        }
                 }
             }
-            const float S[2] = {vn.x + vs.x, vn.y + vs.y}, D[2] = {vn.x - vs.x, vn.y - vs.y};
 #pragma unroll
-            for (int ri = 0; ri < 2; ri++) {
-                const uint32_t o = tc::kmajor_off(2 * q + ri, j, njc);
-                __nv_bfloat16 h, mm, l;
-                tc::split3(S[ri], h, mm, l);
-                *reinterpret_cast<__nv_bfloat16 *>(bS + o) = h;
-                *reinterpret_cast<__nv_bfloat16 *>(bS + dt + o) = mm;
-                *reinterpret_cast<__nv_bfloat16 *>(bS + 2 * dt + o) = l;
-                tc::split3(D[ri], h, mm, l);
-                *reinterpret_cast<__nv_bfloat16 *>(bD + o) = h;
-                *reinterpret_cast<__nv_bfloat16 *>(bD + dt + o) = mm;
-                *reinterpret_cast<__nv_bfloat16 *>(bD + 2 * dt + o) = l;
+            for (int e = 0; e < 8; e++) {
+                sr[e] = vn[e].x + vs[e].x;
+                si[e] = vn[e].y + vs[e].y;
+                dr[e] = vn[e].x - vs[e].x;
+                di[e] = vn[e].y - vs[e].y;
             }
+            const uint32_t o = tc::kmajor_off(2 * q, j0, njc);  // re row; the im row follows at +16
+            uint4 h, mm, l;
+            tc::split3x8(sr, h, mm, l);
+            st_shared16(bS + o, h); st_shared16(bS + dt + o, mm); st_shared16(bS + 2 * dt + o, l);
+            tc::split3x8(si, h, mm, l);
+            st_shared16(bS + o + 16, h); st_shared16(bS + dt + o + 16, mm); st_shared16(bS + 2 * dt + o + 16, l);
+            tc::split3x8(dr, h, mm, l);
+            st_shared16(bD + o, h); st_shared16(bD + dt + o, mm); st_shared16(bD + 2 * dt + o, l);
+            tc::split3x8(di, h, mm, l);
+            st_shared16(bD + o + 16, h); st_shared16(bD + dt + o + 16, mm); st_shared16(bD + 2 * dt + o + 16, l);
         }
     }
     tc::fence_proxy_async();
@@ -351,49 +402,48 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(TcFwdArgs A) {
     const uint32_t tmem = *slot;
     bool ok = true;
     if (tid == 0) {
+        const uint32_t sbo_b = (uint32_t)(njc / 8) * 128;
         for (int t = 0; t < 4 && ok; t++) {
-            if (t > 0) {
-                ok = tc::mbar_wait(bar_mma, (t - 1) & 1);
-                if (!ok) break;
-                tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tblk);
-                tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t], (uint32_t)tblk, bar_tma);
-            }
-            ok = tc::mbar_wait(bar_tma, t & 1);
-            if (!ok) break;
-            tc::fence_after_sync();
             const int ncp = fwd_ncp(t);
             const uint32_t idesc = tc::idesc_bf16(128, ncp);
-            const size_t dt = (size_t)ncp * njc * 2;
-            size_t to = 0;
-            for (int p = 0; p < 2; p++) {
+            const uint32_t dt = (uint32_t)ncp * njc * 2;
+            // P-type (qc, qm, qq) use N+S on even n-m and N-S on odd; Q-type (qe) the reverse
+            const bool ptype = (t != 1);
+            for (int p = 0; p < 2 && ok; p++) {
                 if (!Kq[p]) break;
-                // P-type (qc, qm, qq) use N+S on even n-m and N-S on odd; Q-type (qe) the reverse
-                const bool ptype = (t != 1);
-                const int sel = (ptype ? p : 1 - p);  // 0 -> S, 1 -> D
-                const unsigned char *dsel = dat + doffs[t] + (size_t)sel * 3 * dt;
+                ok = tc::mbar_wait(bar_tma + p, t & 1);
+                if (!ok) break;
+                tc::fence_after_sync();
+                const int sel = ptype ? p : 1 - p;  // 0 -> S, 1 -> D
+                const uint64_t db0 = tc::smem_desc(dat + doffs[t] + (size_t)sel * 3 * dt, 128, sbo_b);
                 const uint32_t dm = tmem + (uint32_t)(fwd_colbase(t) + (2 * p + 0) * ncp);
                 const uint32_t dc = tmem + (uint32_t)(fwd_colbase(t) + (2 * p + 1) * ncp);
-                bool accm = false, accc = false;
-                size_t jo = 0;
+                uint32_t jo = 0;
                 for (int j0 = 0; j0 < njc; j0 += 32) {
                     const int jw = njc - j0 < 32 ? njc - j0 : 32;
-                    const size_t tt = (size_t)R[p] * jw * 2;
-                    for (int kc = 0; kc < jw / 16; kc++)
-                        for (int pr = 0; pr < 6; pr++) {
-                            const unsigned char *a = tab + to + jo + c_pair_a[pr] * tt + kc * 256;
-                            const unsigned char *b = dsel + c_pair_b[pr] * dt + (size_t)(j0 / 8) * 128 + kc * 256;
-                            const bool main = (pr == 0);
-                            tc::mma_bf16(main ? dm : dc, tc::smem_desc(a, 128, (uint32_t)(jw / 8) * 128),
-                                         tc::smem_desc(b, 128, (uint32_t)(njc / 8) * 128), idesc,
-                                         main ? accm : accc);
-                            if (main) accm = true; else accc = true;
-                        }
+                    const uint32_t tt = (uint32_t)R[p] * jw * 2;
+                    const uint64_t da0 = tc::smem_desc(tab + hoff[p] + jo, 128, (uint32_t)(jw / 8) * 128);
+                    for (int kc = 0; kc < jw / 16; kc++) {
+#pragma unroll
+                        for (int pr = 0; pr < 6; pr++)
+                            tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
+                                         tc::desc_add(db0, tc::pair_b(pr) * dt + (j0 / 8) * 128 + kc * 256), idesc,
+                                         j0 > 0 || kc > 0 || pr > 1);
+                    }
                     jo += 3 * tt;
                 }
-                to += jo;
+                if (t < 3) tc::mma_commit(bar_mma + p);
             }
-            tc::mma_commit(t == 3 ? bar_done : bar_mma);
+            // refill each half with the next table once its MMAs have drained
+            for (int p = 0; p < 2 && ok && t < 3; p++) {
+                if (!Kq[p]) break;
+                ok = tc::mbar_wait(bar_mma + p, t & 1);
+                if (!ok) break;
+                tc::mbar_arrive_expect_tx(bar_tma + p, hbytes[p]);
+                tc::bulk_g2s(tab + hoff[p], A.tab + A.off[m * 4 + t + 1] + hoff[p], hbytes[p], bar_tma + p);
+            }
         }
+        if (ok) tc::mma_commit(bar_done);  // arrives once every MMA issued above has completed
         if (!ok) atomicExch(&g_tc_error, 3);
     }
     __syncthreads();

@@ -12,8 +12,10 @@ exotx_status launch_radstep_fp64(const RadDev &D, int blocks, int warps, size_t 
 static exotx_status launch_radstep_fp32(const RadDev &D, int blocks, int warps, size_t smem, cudaStream_t st) {
     if (smem > 48 * 1024)
         EXOTX_CUDA(cudaFuncSetAttribute(k_radstep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cudaEvent_t ev = ktimer_start(EXOTX_K_RADSTEP, st);
     k_radstep<float><<<blocks, warps * 32, smem, st>>>(D);
     EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_RADSTEP, st, ev);
     return EXOTX_OK;
 }
 }  // namespace exotx

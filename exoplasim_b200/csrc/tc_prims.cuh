@@ -120,6 +120,12 @@ __device__ __forceinline__ uint64_t smem_desc(const void *p, uint32_t lbo_bytes,
     d |= (uint64_t)1 << 46;  // descriptor version for sm_100
     return d;                // base offset 0, layout type 0 (no swizzle)
 }
+// descriptor of (p + bytes) from the descriptor of p (16-byte aligned offsets;
+// the 14-bit start-address field cannot carry below 256 KB of shared memory)
+__device__ __forceinline__ uint64_t desc_add(uint64_t d, uint32_t bytes) { return d + (uint64_t)(bytes >> 4); }
+// split-product schedule: term pairs (a, b) with a + b <= 2; product 0 is hi*hi
+__host__ __device__ constexpr int pair_a(int pr) { return pr == 2 || pr == 4 ? 1 : (pr == 5 ? 2 : 0); }
+__host__ __device__ constexpr int pair_b(int pr) { return pr == 1 || pr == 4 ? 1 : (pr == 3 ? 2 : 0); }
 // instruction descriptor: D=F32, A=B=BF16, both K-major, shape M x N
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
@@ -152,6 +158,26 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16 &h, __nv_bfloat16 
     m = __float2bfloat16_rn(r1);
     float r2 = r1 - __bfloat162float(m);
     l = __float2bfloat16_rn(r2);
+}
+
+// split3 of 8 values into three rows of 8 packed BF16 (one 16-byte core-matrix row each)
+__device__ __forceinline__ void split3x8(const float *x, uint4 &h, uint4 &m, uint4 &l) {
+    uint32_t hw[4], mw[4], lw[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+        const float2 hf = __bfloat1622float2(h2);
+        const float r0 = x[2 * i] - hf.x, r1 = x[2 * i + 1] - hf.y;
+        const __nv_bfloat162 m2 = __floats2bfloat162_rn(r0, r1);
+        const float2 mf = __bfloat1622float2(m2);
+        const __nv_bfloat162 l2 = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+        hw[i] = *reinterpret_cast<const uint32_t *>(&h2);
+        mw[i] = *reinterpret_cast<const uint32_t *>(&m2);
+        lw[i] = *reinterpret_cast<const uint32_t *>(&l2);
+    }
+    h = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    m = make_uint4(mw[0], mw[1], mw[2], mw[3]);
+    l = make_uint4(lw[0], lw[1], lw[2], lw[3]);
 }
 
 }  // namespace tc

@@ -296,3 +296,22 @@ def inigau(nlat, device="cuda"):
 def launch_count():
     """Kernel launches issued by libexotx in this process so far."""
     return int(_lib.load().exotx_launch_count())
+
+
+KERNELS = {"tc_forward": 0, "tc_inverse": 1, "fft_forward": 2, "fft_inverse": 3, "leg_forward": 4,
+           "leg_inverse": 5, "radstep": 6}
+
+
+def kernel_timing(enable):
+    """Bracket the library's main kernel launches (outside stream capture)
+    with CUDA events on their launching stream while enabled."""
+    call("exotx_kernel_timing", 1 if enable else 0)
+
+
+def kernel_time(name):
+    """(summed milliseconds, launches) recorded for one kernel since the last
+    read; clears that kernel's record."""
+    ms = C.c_double()
+    n = C.c_longlong()
+    call("exotx_kernel_time", KERNELS[name], C.byref(ms), C.byref(n))
+    return ms.value, n.value

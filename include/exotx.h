@@ -146,6 +146,24 @@ exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const void *gpin, v
 #define EXOTX_STATIC_WORK_BYTES (16u << 20)
 exotx_status exotx_forward_set_noalloc(exotx_plan p, int prec, const void *gpin, void *spout,
                                        int nlev, exotx_stream s);
+/* Per-kernel device time (diagnostics; no counterpart in the reference).
+ * While enabled, launches of these kernels outside stream capture are
+ * bracketed by CUDA events on the launching stream.  exotx_kernel_time
+ * waits for the recorded events, returns the summed milliseconds and the
+ * launch count of one kernel, and clears that kernel's record. */
+typedef enum {
+    EXOTX_K_TC_FORWARD = 0,   /* tensor-core forward Legendre (fc2sp + mktend + qtend) */
+    EXOTX_K_TC_INVERSE = 1,   /* tensor-core inverse Legendre (dv2uv + sp2fc + sp2fcdmu) */
+    EXOTX_K_FFT_FORWARD = 2,  /* gp2fc rows */
+    EXOTX_K_FFT_INVERSE = 3,  /* fc2gp rows */
+    EXOTX_K_LEG_FORWARD = 4,  /* FP64/FP32 forward Legendre */
+    EXOTX_K_LEG_INVERSE = 5,  /* FP64/FP32 inverse Legendre */
+    EXOTX_K_RADSTEP = 6,      /* radiation column pass */
+    EXOTX_K_COUNT = 7
+} exotx_kernel_id;
+exotx_status exotx_kernel_timing(int enable);
+exotx_status exotx_kernel_time(int kernel, double *ms, long long *launches);
+
 /* Error word of the tensor-core kernels (0 = none; nonzero = a bounded
  * device-side wait gave up), read after synchronising the stream, then reset. */
 exotx_status exotx_tc_error(int *code, exotx_stream s);
