@@ -379,6 +379,47 @@ def run_ours(a, rank, world, local_rank):
         ms = max_over_ranks(ms)
         rad[rprec] = {"cols_per_s": world * g["nhor"] * a.steps / (ms / 1000.0), "ms_per_pass": ms / a.steps}
 
+    # learned surrogate (BF16 tensor-core MLP with out-of-range fallback) on the same
+    # columns, and on 16 such grids side by side (64 tiles of 128 columns cannot fill 148 SMs)
+    from exoplasim_b200 import surrogate as SG
+    if not a.skip_radiation and os.path.exists(SG.DEFAULT_NET):
+        net = SG.Mlp.load(SG.DEFAULT_NET)
+        net.prepare()
+        rad["surrogate"] = {"net": os.path.basename(SG.DEFAULT_NET)}
+        for ncopy in (1, 16):
+            rep = {k: (np.tile(v, ncopy) if k in ("sid", "cola") else
+                       np.ascontiguousarray(np.tile(v, (1, ncopy)) if np.ndim(v) == 2 and k != "dsalb"
+                                            else np.tile(v, (ncopy, 1)) if k == "dsalb" else np.tile(v, ncopy)))
+                   for k, v in cols.items()}
+            nh = g["nhor"] * ncopy
+            params = R.default_params(RAD_NLEV, nh, g["nlon"], nsol=0)
+            dev_cols = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=torch.float64, device=dev)
+                        for k, v in rep.items()}
+            outs = R.alloc_outputs(params, torch.float64)
+            ms_p, _ = time_graph(lambda: R.radstep(params, dev_cols, outs, precision="fp64"), a.steps, a.warmup)
+            scols = {k: v.clone() for k, v in dev_cols.items()}
+            souts = R.alloc_outputs(params, torch.float64)
+            ms_s, nlaunch = time_graph(lambda: SG.surrogate_step(net, params, scols, souts), a.steps, a.warmup)
+            ms_p, ms_s = max_over_ranks(ms_p), max_over_ranks(ms_s)
+            key = f"{nh}_columns"
+            rad["surrogate"][key] = {"cols_per_s": world * nh * a.steps / (ms_s / 1000.0),
+                                     "plain_fp64_cols_per_s": world * nh * a.steps / (ms_p / 1000.0),
+                                     "speedup_vs_plain_fp64": ms_p / ms_s, "launches_per_pass": nlaunch}
+            if ncopy == 1:
+                # accuracy against plain FP64 radstep on fresh outputs
+                pc = {k: v.clone() for k, v in dev_cols.items()}
+                pc["dtdt"].zero_()
+                po = R.radstep(params, pc, precision="fp64")
+                sc = {k: v.clone() for k, v in dev_cols.items()}
+                sc["dtdt"].zero_()
+                so = R.alloc_outputs(params, torch.float64)
+                nfb = SG.surrogate_step(net, params, sc, so, count=True)
+                L = RAD_NLEV
+                fl = lambda o: torch.stack([o["dfd"][L], o["dfu"][L], o["dftd"][L], o["dftu"][L]])
+                rad["surrogate"]["heating_rms_K_per_day"] = SG.heating_rms(sc["dtdt"], pc["dtdt"])
+                rad["surrogate"]["surface_flux_rms_W_m2"] = float(torch.sqrt(((fl(so) - fl(po)) ** 2).mean()))
+                rad["surrogate"]["fallback_fraction"] = nfb / nh
+        del net
     if world > 1:
         dist.barrier()
     if rank != 0:

@@ -46,7 +46,7 @@ class RadParams(C.Structure):
 
 RAD_IO_FIELDS = ("sid", "cola", "dt", "dq", "dcc", "dql", "dqco2", "dp", "dls", "dicec", "dqo3", "gmu0",
                  "dalb", "dsalb", "dfu", "dfd", "dftu", "dftd", "dswfl", "dlwfl", "dflux", "dtdt", "dtdtswr",
-                 "dtdtlwr", "dconv")
+                 "dtdtlwr", "dconv", "zsol")
 
 
 class RadIO(C.Structure):
@@ -83,6 +83,18 @@ SIGNATURES = {
     "exotx_forward_set_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_forward_set_noalloc": [_P, _I, _P, _P, _I, _S],
     "exotx_kernel_timing": [_I],
+    "exotx_mlp_create": [_I, _I, _I, _I, _I, C.POINTER(C.c_void_p)],
+    "exotx_mlp_destroy": [_P],
+    "exotx_mlp_params": [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)],
+    "exotx_mlp_layer": [_P, _I, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(_I), C.POINTER(_I)],
+    "exotx_mlp_set_norm": [_P, _P],
+    "exotx_mlp_forward": [_P, _P, _P, _I, _S],
+    "exotx_mlp_backward": [_P, _P, _P, _I, _P, _S],
+    "exotx_mlp_adam": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _I, _S],
+    "exotx_mlp_prepare": [_P, _S],
+    "exotx_surr_features": [C.POINTER(RadParams), _I, C.POINTER(RadIO), _P, _S],
+    "exotx_surr_targets": [C.POINTER(RadParams), _I, C.POINTER(RadIO), _P, _S],
+    "exotx_rad_surrogate": [_P, C.POINTER(RadParams), _I, C.POINTER(RadIO), C.POINTER(_I), _S],
     "exotx_kernel_time": [_I, C.POINTER(_D), C.POINTER(C.c_longlong)],
     "exotx_tc_error": [C.POINTER(_I), _S],
 }

@@ -119,6 +119,10 @@ template <typename T>
 exotx_status fft_forward_tw(const T *in, T *out, int n, long long lot, int kout, long long f_rs, long long f_ms,
                             const T *w, const T *r, cudaStream_t s);
 
+// radstep over all columns or a device-side column list (radiation.cu)
+exotx_status radstep_columns(const exotx_rad_params *p, int prec, const exotx_rad_io *io, const int *cols,
+                             const int *ncols, int maxcols, cudaStream_t st);
+
 // per-kernel event timing (ktimer.cu): start returns nullptr when timing is
 // off or the stream is capturing; stop records the pair
 cudaEvent_t ktimer_start(int kernel, cudaStream_t s);

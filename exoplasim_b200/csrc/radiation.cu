@@ -4,6 +4,7 @@
 // differences of nearly equal quantities) sees the same rounding.
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include "radiation_kernel.cuh"
 
 namespace exotx {
@@ -98,8 +99,11 @@ EXOTX_API exotx_status exotx_solarini(double starbbtemp, double minwavel, double
     return EXOTX_OK;
 }
 
-EXOTX_API exotx_status exotx_radstep(const exotx_rad_params *p, int prec, const exotx_rad_io *io,
-                                     exotx_stream s) {
+namespace exotx {
+// radstep over all columns, or over the device-side list cols[0 .. *ncols)
+// (at most maxcols entries); the list's length is read by the kernel
+exotx_status radstep_columns(const exotx_rad_params *p, int prec, const exotx_rad_io *io, const int *cols,
+                             const int *ncols, int maxcols, cudaStream_t st) {
     if (!p || !io) return EXOTX_BAD_ARG;
     if (p->nlev < 2 || p->nlev > RAD_MAXLEV || p->nhor < 1 || p->nlon < 1) return EXOTX_BAD_DIM;
     if (prec != EXOTX_FP64 && prec != EXOTX_FP32) return EXOTX_BAD_ARG;
@@ -111,6 +115,8 @@ EXOTX_API exotx_status exotx_radstep(const exotx_rad_params *p, int prec, const 
     if ((p->nsol == 1 || p->no3 == 1) && (!io->sid || !io->cola)) return EXOTX_BAD_ARG;
     // sid/cola are indexed by latitude row col/nlon: columns must fill whole rows
     if ((p->nsol == 1 || p->no3 == 1) && (p->nhor % p->nlon) != 0) return EXOTX_BAD_DIM;
+    if ((cols == nullptr) != (ncols == nullptr)) return EXOTX_BAD_ARG;
+    if (maxcols <= 0) return EXOTX_OK;
     RadDev D;
     D.p = *p;
     D.sid = io->sid; D.cola = io->cola; D.dt = io->dt; D.dq = io->dq; D.dcc = io->dcc; D.dql = io->dql;
@@ -119,6 +125,7 @@ EXOTX_API exotx_status exotx_radstep(const exotx_rad_params *p, int prec, const 
     D.dfu = io->dfu; D.dfd = io->dfd; D.dftu = io->dftu; D.dftd = io->dftd; D.dswfl = io->dswfl;
     D.dlwfl = io->dlwfl; D.dflux = io->dflux; D.dtdt = io->dtdt; D.dtdtswr = io->dtdtswr;
     D.dtdtlwr = io->dtdtlwr; D.dconv = io->dconv;
+    D.zsol = io->zsol; D.cols = cols; D.ncols = ncols;
     int L = p->nlev, E = L + 1;
     size_t elems = (size_t)6 * E + 7 * L + 11 * L + 8 * L + 8 * E + 2 * E + 4 * L + 2 * (E + 1) + (size_t)L * L + L +
                    6 * E + 32;
@@ -127,8 +134,17 @@ EXOTX_API exotx_status exotx_radstep(const exotx_rad_params *p, int prec, const 
     int warps = (int)((200 * 1024) / (elems * esz));
     warps = warps < 1 ? 1 : (warps > RAD_WARPS ? RAD_WARPS : warps);
     size_t smem = elems * esz * warps;
-    int blocks = (p->nhor + warps - 1) / warps;
-    cudaStream_t st = (cudaStream_t)s;
+    int blocks = (maxcols + warps - 1) / warps;
+    // a column list is usually short (often empty): a few resident blocks per SM
+    // stride over it instead of one block per possible entry
+    if (cols) blocks = std::min(blocks, 148 * 8);
     if (prec == EXOTX_FP64) return launch_radstep_fp64(D, blocks, warps, smem, st);
     return launch_radstep_fp32(D, blocks, warps, smem, st);
+}
+}  // namespace exotx
+
+EXOTX_API exotx_status exotx_radstep(const exotx_rad_params *p, int prec, const exotx_rad_io *io,
+                                     exotx_stream s) {
+    if (!p || !io) return EXOTX_BAD_ARG;
+    return radstep_columns(p, prec, io, nullptr, nullptr, p->nhor, (cudaStream_t)s);
 }

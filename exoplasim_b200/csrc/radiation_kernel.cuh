@@ -22,6 +22,9 @@ struct RadDev {
     const void *sid, *cola, *dt, *dq, *dcc, *dql, *dqco2, *dp, *dls, *dicec;
     void *dqo3, *gmu0, *dalb, *dsalb;
     void *dfu, *dfd, *dftu, *dftd, *dswfl, *dlwfl, *dflux, *dtdt, *dtdtswr, *dtdtlwr, *dconv;
+    const void *zsol;       // optional (NHOR,3): per-column zsolar1, zsolar2, rcoeff
+    const int *cols;        // optional list of the columns to compute ...
+    const int *ncols;       // ... and its length (device memory)
 };
 
 template <typename T> __device__ __forceinline__ T P_(T x, T y);
@@ -79,15 +82,15 @@ template <typename T> __device__ ColScratch<T> carve(T *b, int L) {
 
 template <typename T>
 __device__ void swr_warp(const exotx_rad_params &P, ColScratch<T> &s, int L, T zmu0, T zmu1, T dp, T &dalb,
-                         T *dsalb, T dls, T dicec, int lane) {
+                         T *dsalb, T dls, T dicec, T csol1, T csol2, T crco, int lane) {
     const T zero = (T)1e-6, zbetta = (T)1.66, zmbar = (T)1.9, zro3 = (T)2.14, zfo3 = (T)100. / zro3;
     const T aa = (T)0.2542857142857143, bb = (T)0.8229693877551021, c0 = (T)0.14997959183673468;
     const T ga = (T)P.ga;
     const int E = L + 1;
     const int nclouds = P.nclouds;
     for (int k = lane; k < E; k += 32) { s.fu[k] = 0; s.fd[k] = 0; s.sw[k] = 0; }
-    T zftop1 = (T)P.zsolar1 * (T)P.gsol0 * (T)P.gdist2 * zmu1;
-    T zftop2 = (T)P.zsolar2 * (T)P.gsol0 * (T)P.gdist2 * zmu1;
+    T zftop1 = csol1 * (T)P.gsol0 * (T)P.gdist2 * zmu1;
+    T zftop2 = csol2 * (T)P.gsol0 * (T)P.gdist2 * zmu1;
     bool losun = (zftop1 + zftop2 > zero);
     const T zmu00 = (T)0.5;
     if (!losun) { __syncwarp(); return; }
@@ -183,7 +186,7 @@ __device__ void swr_warp(const exotx_rad_params &P, ColScratch<T> &s, int L, T z
     __syncwarp();
     if (lane == 0) {
         const int newrsc = P.newrsc, nrscat = P.nrscat;
-        const T zs1 = (T)P.zsolar1, zs2 = (T)P.zsolar2;
+        const T zs1 = csol1, zs2 = csol2;
         const T dccL = s.dcc[L - 1];
         T zta1 = 1, zta1s = 1, zra1 = 0, zra1s = 0, zta2 = 1, zta2s = 1, zra2 = 0, zra2s = 0;
         T zto3t = 1;
@@ -192,7 +195,7 @@ __device__ void swr_warp(const exotx_rad_params &P, ColScratch<T> &s, int L, T z
         T ztwvtu = (T)1. - awv_<T>(zywvt + zbetta * zwvt) / zs2;
         // Rayleigh scattering in the lowest layer only (newrsc = 0 default, :1928-1939)
         T zcs_run = 1;
-        T zscf = (T)P.rcoeff * dp / (T)101100.0 * (T)9.80665 / ga;
+        T zscf = crco * dp / (T)101100.0 * (T)9.80665 / ga;
         for (int jl = 0; jl < L; jl++) {
             zcs_run = zcs_run * ((T)1. - s.dcc[jl] * nclouds);
             T zrcs = (aa / ((T)1. + bb * zmu0) * zcs_run + c0 * ((T)1. - zcs_run - dccL * nclouds)) *
@@ -254,7 +257,7 @@ __device__ void swr_warp(const exotx_rad_params &P, ColScratch<T> &s, int L, T z
                        ((T)1. - dls) * ((T)1. - dicec) * (1 - ne) * ne6 * ocean6 +
                        ((T)1. - dls) * ((T)1. - dicec) * ((T)1. - ne) * (1 - ne6) * dsalb[b];
         }
-        dalb = ((T)P.zsolar1 * dsalb[0] + (T)P.zsolar2 * dsalb[1]) * nst +
+        dalb = (csol1 * dsalb[0] + csol2 * dsalb[1]) * nst +
                (dls * dalb + ((T)1. - dls) * dicec * dalb + ((T)1. - dls) * ((T)1. - dicec) * ocean3 * ne * (1 - ne6) +
                 ((T)1. - dls) * ((T)1. - dicec) * (1 - ne) * ne6 * ocean6 +
                 ((T)1. - dls) * ((T)1. - dicec) * ((T)1. - ne) * (1 - ne6) * dalb) *
@@ -439,8 +442,17 @@ __global__ void __launch_bounds__(RAD_WARPS * 32) k_radstep(RadDev D) {
     const T PI = (T)3.14159265359, TWOPI = PI + PI;
     const T ga = (T)P.ga, gascon = (T)P.gascon;
     const int nwarps = blockDim.x >> 5;
-    for (int col = blockIdx.x * nwarps + warp; col < nhor; col += gridDim.x * nwarps) {
+    const int count = D.cols ? *D.ncols : nhor;
+    for (int w = blockIdx.x * nwarps + warp; w < count; w += gridDim.x * nwarps) {
+        const int col = D.cols ? D.cols[w] : w;
         const int jlat = col / nlon, jlon = col - jlat * nlon;
+        T csol1 = (T)P.zsolar1, csol2 = (T)P.zsolar2, crco = (T)P.rcoeff;
+        if (D.zsol) {
+            const T *z = (const T *)D.zsol;
+            csol1 = z[col];
+            csol2 = z[(size_t)nhor + col];
+            crco = z[2 * (size_t)nhor + col];
+        }
         for (int k = lane; k < E; k += 32) {
             s.dt[k] = dt[(size_t)k * nhor + col];
             s.dq[k] = dq[(size_t)k * nhor + col];
@@ -500,7 +512,7 @@ __global__ void __launch_bounds__(RAD_WARPS * 32) k_radstep(RadDev D) {
         T dalb = dalbv[col];
         T dsalb[2] = {dsalbv[2 * col], dsalbv[2 * col + 1]};
         if (P.nswr == 1) {
-            swr_warp<T>(P, s, L, mu0, mu0, dp, dalb, dsalb, dls, dicec, lane);
+            swr_warp<T>(P, s, L, mu0, mu0, dp, dalb, dsalb, dls, dicec, csol1, csol2, crco, lane);
         } else {
             for (int k = lane; k < E; k += 32) { s.fu[k] = 0; s.fd[k] = 0; s.sw[k] = 0; }
         }

@@ -60,16 +60,25 @@ def radstep(params, cols, out=None, precision="fp64"):
     dtype = torch.float64 if prec == FP64 else torch.float32
     if out is None:
         out = alloc_outputs(params, dtype)
+    io = make_io(cols, out, prec)
+    call("exotx_radstep", C.byref(params), prec, C.byref(io),
+         C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return out
+
+
+def make_io(cols, out, prec):
+    """exotx_rad_io over the column and output tensors (zsol optional)."""
+    dtype = torch.float64 if prec == FP64 else torch.float32
     io = _lib.RadIO()
     allv = dict(cols)
     allv.update(out)
     for name in RAD_IO_FIELDS:
         t = allv.get(name)
         if t is None:
+            if name == "zsol":
+                continue
             raise KeyError(f"radstep needs '{name}'")
         if not t.is_cuda or t.dtype != dtype or not t.is_contiguous():
             raise TypeError(f"{name} must be a contiguous CUDA {dtype} tensor")
         setattr(io, name, t.data_ptr())
-    call("exotx_radstep", C.byref(params), prec, C.byref(io),
-         C.c_void_p(torch.cuda.current_stream().cuda_stream))
-    return out
+    return io

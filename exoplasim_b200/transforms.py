@@ -299,7 +299,7 @@ def launch_count():
 
 
 KERNELS = {"tc_forward": 0, "tc_inverse": 1, "fft_forward": 2, "fft_inverse": 3, "leg_forward": 4,
-           "leg_inverse": 5, "radstep": 6}
+           "leg_inverse": 5, "radstep": 6, "surrogate": 7}
 
 
 def kernel_timing(enable):

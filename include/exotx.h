@@ -159,7 +159,8 @@ typedef enum {
     EXOTX_K_LEG_FORWARD = 4,  /* FP64/FP32 forward Legendre */
     EXOTX_K_LEG_INVERSE = 5,  /* FP64/FP32 inverse Legendre */
     EXOTX_K_RADSTEP = 6,      /* radiation column pass */
-    EXOTX_K_COUNT = 7
+    EXOTX_K_SURROGATE = 7,    /* radiation surrogate inference */
+    EXOTX_K_COUNT = 8
 } exotx_kernel_id;
 exotx_status exotx_kernel_timing(int enable);
 exotx_status exotx_kernel_time(int kernel, double *ms, long long *launches);
@@ -197,7 +198,52 @@ typedef struct {
     void *dfu, *dfd, *dftu, *dftd, *dswfl, *dlwfl, *dflux;   /* (NHOR,NLEP) */
     void *dtdt;                           /* (NHOR,NLEV) in/out (tendency is added) */
     void *dtdtswr, *dtdtlwr, *dconv;      /* (NHOR,NLEV) */
+    /* optional (NHOR,3): zsolar1, zsolar2, rcoeff per column (a star per
+     * column, each from exotx_solarini); NULL = the params' scalars */
+    const void *zsol;
 } exotx_rad_io;
+
+/* ---- learned radiation surrogate (no counterpart in the reference) ----
+ * An MLP (nin -> width x nhidden -> nout, SiLU) trained on columns that
+ * exotx_radstep computes; it predicts a column's heating-rate profile and
+ * its four surface fluxes.  Training runs in FP32 on the library's kernels
+ * (exotx_mlp_backward + exotx_mlp_adam); exotx_rad_surrogate runs the
+ * network in BF16 on the tensor cores and sends every column with an input
+ * outside the training ranges to the plain radstep kernel. */
+typedef struct exotx_mlp_s *exotx_mlp;
+/* parameters: per layer l, W_l (dout x din, row-major) then b_l (dout) in one
+ * flat FP32 device array; max_batch bounds the rows of forward/backward */
+exotx_status exotx_mlp_create(int nin, int width, int nhidden, int nout, int max_batch, exotx_mlp *out);
+exotx_status exotx_mlp_destroy(exotx_mlp net);
+exotx_status exotx_mlp_params(exotx_mlp net, float **params, float **grads, long long *nparams);
+exotx_status exotx_mlp_layer(exotx_mlp net, int layer, long long *w_off, long long *b_off, int *din, int *dout);
+/* HOST array of 4*nin + 2*nout floats: feature mean, std, min, max; target mean, std */
+exotx_status exotx_mlp_set_norm(exotx_mlp net, const float *host_norm);
+/* FP32 forward of n normalised rows X (n x nin) -> Y (n x nout, normalised) */
+exotx_status exotx_mlp_forward(exotx_mlp net, const float *X, float *Y, int n, exotx_stream s);
+/* forward + backward of the mean squared error against T (n x nout): the
+ * gradients land in the net's gradient array; *loss (device) += the loss */
+exotx_status exotx_mlp_backward(exotx_mlp net, const float *X, const float *T, int n, float *loss,
+                                exotx_stream s);
+exotx_status exotx_mlp_adam(exotx_mlp net, float lr, float beta1, float beta2, float eps, int step,
+                            exotx_stream s);
+/* BF16 tensor-core copy of the current weights (width 256, nin <= 80, nout <= 32) */
+exotx_status exotx_mlp_prepare(exotx_mlp net, exotx_stream s);
+/* raw features X (nhor x (3L+9)) and targets Y (nhor x (L+4)) of radstep columns:
+ * features T(k), T surface, ln q(k<=L), cloud cover(k), ln ps, albedo, gmu0,
+ * ln CO2, zsolar1, rcoeff, sin(lat); targets per level the heating rate
+ * (K/day) times (ps / 1e5 Pa)(1 + ADV q), then dfd, dfu, dftd, dftu at the surface */
+exotx_status exotx_surr_features(const exotx_rad_params *p, int prec, const exotx_rad_io *io, float *X,
+                                 exotx_stream s);
+exotx_status exotx_surr_targets(const exotx_rad_params *p, int prec, const exotx_rad_io *io, float *Y,
+                                exotx_stream s);
+/* Surrogate radiation pass (needs nsol = 0: gmu0 is an input).  In-range
+ * columns get dtdt += predicted heating and the surface entries of dfd, dfu,
+ * dftd, dftu, dswfl, dlwfl; out-of-range columns go through radstep (every
+ * output).  *nfallback (HOST, may be NULL; non-NULL synchronises s) receives
+ * the number of fallback columns. */
+exotx_status exotx_rad_surrogate(exotx_mlp net, const exotx_rad_params *p, int prec,
+                                 const exotx_rad_io *io, int *nfallback, exotx_stream s);
 
 /* Reference defaults (radmod.f90:27-100, p_earth.f90, default sigma levels
  * plasim.f90:1554-1564) for nlev levels and nhor columns in rows of nlon. */
