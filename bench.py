@@ -77,6 +77,7 @@ def args_():
     a.add_argument("--precisions", default="mixed,fp32,fp64",
                    help="transform paths to time, first = headline (profiling runs pass one)")
     a.add_argument("--skip-radiation", action="store_true")
+    a.add_argument("--skip-ensemble", action="store_true")
     return a.parse_args()
 
 
@@ -420,6 +421,40 @@ def run_ours(a, rank, world, local_rank):
                 rad["surrogate"]["surface_flux_rms_W_m2"] = float(torch.sqrt(((fl(so) - fl(po)) ** 2).mean()))
                 rad["surrogate"]["fallback_fraction"] = nfb / nh
         del net
+    # uneven ensemble: 96 instances of T21/T42/T63 x 10/15/20 levels, one tensor-core
+    # and one FFT launch per half of the round trip, tuned, against running the same
+    # instances one at a time through the single-resolution API
+    ens = None
+    if not a.skip_ensemble:
+        from exoplasim_b200.ensemble import Ensemble, draw
+        nl_e, lv_e = draw(96, seed=0)
+        E = Ensemble(nl_e, lv_e)
+        sp_i, gi_i = [], []
+        for i, (nlat, L) in enumerate(zip(nl_e, lv_e)):
+            ntru = (2 * nlat - 1) // 3
+            sp_i.append(torch.as_tensor(S.transform_state(ntru, L, seed=7 + i, kind="nn1"), device=dev).float())
+            gi_i.append(torch.as_tensor(S.grid_tendencies(nlat, L, seed=500 + i), device=dev).float())
+        spin_e, gin_e = E.pack("spec", sp_i), E.pack("gin", gi_i)
+        _, gout_e, _, spout_e = E.buffers()
+        choice = E.tune(spin_e, gout_e, gin_e, spout_e, reps=3)
+        ms_e, nlch_e = time_graph(lambda: (E.inverse(spin_e, gout_e), E.forward(gin_e, spout_e)), a.steps, a.warmup)
+        eplans = {n: Plan(n) for n in sorted(set(nl_e))}
+        sp_b = [t.unsqueeze(0).contiguous() for t in sp_i]
+        gi_b = [t.unsqueeze(0).contiguous() for t in gi_i]
+        go_b = [torch.zeros((1, 6 * L + 3, n, 2 * n), device=dev) for n, L in zip(nl_e, lv_e)]
+        so_b = [torch.zeros_like(t) for t in sp_b]
+
+        def one_by_one():
+            for i, (n, L) in enumerate(zip(nl_e, lv_e)):
+                eplans[n].inverse_set_batch(sp_b[i], L, "mixed", out=go_b[i])
+                eplans[n].forward_set_batch(gi_b[i], L, "mixed", out=so_b[i])
+        ms_1, nlch_1 = time_graph(one_by_one, a.steps, a.warmup)
+        ms_e, ms_1 = max_over_ranks(ms_e), max_over_ranks(ms_1)
+        ens = {"instances": 96, "resolutions": {f"T{(2 * n - 1) // 3}": nl_e.count(n) for n in sorted(set(nl_e))},
+               "round_trips_per_s": world * 96 * a.steps / (ms_e / 1000.0), "launches_per_step": nlch_e,
+               "one_by_one_round_trips_per_s": world * 96 * a.steps / (ms_1 / 1000.0),
+               "one_by_one_launches_per_step": nlch_1, "tuned": choice}
+        del E, eplans
     if world > 1:
         dist.barrier()
     if rank != 0:
@@ -451,6 +486,7 @@ def run_ours(a, rank, world, local_rank):
         "e2e": {"value": world * B * a.steps / (e2e_ms / 1000.0), "unit": "round-trips/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "radiation": {"metric": "radiation cols/s (T42 grid, 8192 columns, L20, plain radmod kernel)", **rad},
+        "ensemble": ens,
         "clocks": clk,
         "gpu_launches": prim["launches_per_step"] * a.steps,
         "cpu_baseline": cpu,

@@ -83,6 +83,13 @@ SIGNATURES = {
     "exotx_forward_set_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_forward_set_noalloc": [_P, _I, _P, _P, _I, _S],
     "exotx_kernel_timing": [_I],
+    "exotx_ensemble_create": [_I, _P, _P, C.POINTER(C.c_void_p)],
+    "exotx_ensemble_destroy": [_P],
+    "exotx_ensemble_layout": [_P, _P, _P, _P, _P],
+    "exotx_ensemble_inverse": [_P, _P, _P, _S],
+    "exotx_ensemble_forward": [_P, _P, _P, _S],
+    "exotx_ensemble_configure": [_P, _I, _I, _I, _I],
+    "exotx_ensemble_tune": [_P, _P, _P, _P, _P, _I, _S, _P, _P],
     "exotx_mlp_create": [_I, _I, _I, _I, _I, C.POINTER(C.c_void_p)],
     "exotx_mlp_destroy": [_P],
     "exotx_mlp_params": [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)],

@@ -119,6 +119,17 @@ template <typename T>
 exotx_status fft_forward_tw(const T *in, T *out, int n, long long lot, int kout, long long f_rs, long long f_ms,
                             const T *w, const T *r, cudaStream_t s);
 
+// FFTs of several segments of FP32 rows (lengths 64..512 with specialised
+// kernels) in one launch, for uneven ensembles (fft.cu)
+constexpr int FFT_ENS_MAXSEG = 12;
+struct FftEnsSeg {
+    const float *in;
+    float *out;
+    long long lot, f_rs, f_ms;
+    int n, kf;
+};
+exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s);
+
 // radstep over all columns or a device-side column list (radiation.cu)
 exotx_status radstep_columns(const exotx_rad_params *p, int prec, const exotx_rad_io *io, const int *cols,
                              const int *ncols, int maxcols, cudaStream_t st);
@@ -133,6 +144,19 @@ exotx_status tc_inverse_set(exotx_plan p, const float *spin, float *four, int nl
 exotx_status tc_forward_set(exotx_plan p, const float *four, float *spout, int nlev, cudaStream_t s);
 exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int L, int ninst, cudaStream_t s);
 exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int L, int ninst, cudaStream_t s);
+// uneven ensembles: a segment is a run of instances of one resolution and level count
+constexpr int TC_MAXSEG = 12;  // segments per tensor-core launch
+struct EnsSeg {
+    exotx_plan p;
+    int L, ninst;
+    const float *spin;  // inverse input, (4L+1) x NRSP per instance
+    float *spout;       // forward output, (4L+1) x NRSP per instance
+    float *W;           // m-major Fourier intermediate of the segment
+};
+exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, int nc_uv_cap, bool sort,
+                         int4 **d_jobs, int *njobs, size_t *smem);
+exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_jobs, int njobs, size_t smem,
+                        int nprod, cudaStream_t s);
 exotx_status tc_error_reset(cudaStream_t s);
 exotx_status tc_error_read(int *err, cudaStream_t s);
 exotx_status tc_available();

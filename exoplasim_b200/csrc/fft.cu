@@ -9,6 +9,7 @@
 // One block transforms R rows; loads and stores of the grid side are
 // row-contiguous and coalesced.  The Fourier side may be row-major (the
 // reference layout) or m-major (the transform sets' intermediate).
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -289,17 +290,18 @@ __device__ __forceinline__ const cpx<T> *passes_ct(cpx<T> *src, cpx<T> *dst, con
 template <typename T> struct vec2 { using t = float4; };
 template <> struct vec2<double> { using t = double2; };
 
+// block blk of a forward transform of lot rows (the kernels below pass blockIdx.x)
 template <typename T, int N, int ROWS>
-__global__ void __launch_bounds__(256) k_rfft_fwd_ct(const T *gp, T *fc, long long lot, int kf, long long f_rs,
-                                                      long long f_ms, const cpx<T> *__restrict__ wtab,
-                                                      const cpx<T> *__restrict__ rtab) {
+__device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long lot, int kf, long long f_rs,
+                                                 long long f_ms, const cpx<T> *__restrict__ wtab,
+                                                 const cpx<T> *__restrict__ rtab, long long blk) {
     constexpr int H = N / 2;
     extern __shared__ __align__(16) unsigned char smraw[];
     cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
     cpx<T> *b1 = b0 + ROWS * H;
     cpx<T> *tw = b1 + ROWS * H;
     cpx<T> *rt = tw + H;
-    const long long row0 = (long long)blockIdx.x * ROWS;
+    const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
     for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
     for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
@@ -342,16 +344,16 @@ __global__ void __launch_bounds__(256) k_rfft_fwd_ct(const T *gp, T *fc, long lo
 }
 
 template <typename T, int N, int ROWS>
-__global__ void __launch_bounds__(256) k_rfft_inv_ct(const T *fc, T *gp, long long lot, int kf, long long f_rs,
-                                                      long long f_ms, const cpx<T> *__restrict__ wtab,
-                                                      const cpx<T> *__restrict__ rtab) {
+__device__ __forceinline__ void rfft_inv_ct_body(const T *fc, T *gp, long long lot, int kf, long long f_rs,
+                                                 long long f_ms, const cpx<T> *__restrict__ wtab,
+                                                 const cpx<T> *__restrict__ rtab, long long blk) {
     constexpr int H = N / 2;
     extern __shared__ __align__(16) unsigned char smraw[];
     cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
     cpx<T> *b1 = b0 + ROWS * H;
     cpx<T> *tw = b1 + ROWS * H;
     cpx<T> *rt = tw + H;
-    const long long row0 = (long long)blockIdx.x * ROWS;
+    const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
     for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
     for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
@@ -389,8 +391,104 @@ __global__ void __launch_bounds__(256) k_rfft_inv_ct(const T *fc, T *gp, long lo
     for (int i = threadIdx.x; i < nv; i += blockDim.x) dst[i] = src[i];
 }
 
+template <typename T, int N, int ROWS>
+__global__ void __launch_bounds__(256) k_rfft_fwd_ct(const T *gp, T *fc, long long lot, int kf, long long f_rs,
+                                                      long long f_ms, const cpx<T> *__restrict__ wtab,
+                                                      const cpx<T> *__restrict__ rtab) {
+    rfft_fwd_ct_body<T, N, ROWS>(gp, fc, lot, kf, f_rs, f_ms, wtab, rtab, blockIdx.x);
+}
+template <typename T, int N, int ROWS>
+__global__ void __launch_bounds__(256) k_rfft_inv_ct(const T *fc, T *gp, long long lot, int kf, long long f_rs,
+                                                      long long f_ms, const cpx<T> *__restrict__ wtab,
+                                                      const cpx<T> *__restrict__ rtab) {
+    rfft_inv_ct_body<T, N, ROWS>(fc, gp, lot, kf, f_rs, f_ms, wtab, rtab, blockIdx.x);
+}
+
 template <typename T> constexpr int ct_rows(int n) {
     return (sizeof(T) == 4) ? (n <= 256 ? 16 : 8) : (n <= 256 ? 8 : 4);
+}
+
+// ---------------------------------------------------------------- ensembles
+// One launch transforms the rows of up to FFT_ENS_MAXSEG segments of different
+// lengths (an uneven ensemble); block b belongs to the last segment whose
+// first block is <= b.
+struct FftEnsArgs {
+    const float *in;
+    float *out;
+    long long lot, f_rs, f_ms;
+    int n, kf, block0;
+    const cpx<float> *w, *r;
+};
+struct FftEnsLaunch {
+    FftEnsArgs seg[FFT_ENS_MAXSEG];
+    int nseg;
+};
+
+template <bool FWD>
+__global__ void __launch_bounds__(256) k_rfft_ens(const __grid_constant__ FftEnsLaunch P) {
+    int s = 0;
+    while (s + 1 < P.nseg && P.seg[s + 1].block0 <= (int)blockIdx.x) s++;
+    const FftEnsArgs &S = P.seg[s];
+    const long long blk = (long long)blockIdx.x - S.block0;
+    switch (S.n) {
+#define EXOTX_FFT_ENS_CASE(NN)                                                                                 \
+    case NN:                                                                                                   \
+        if (FWD) rfft_fwd_ct_body<float, NN, ct_rows<float>(NN)>(S.in, S.out, S.lot, S.kf, S.f_rs, S.f_ms, S.w, S.r, blk); \
+        else rfft_inv_ct_body<float, NN, ct_rows<float>(NN)>(S.in, S.out, S.lot, S.kf, S.f_rs, S.f_ms, S.w, S.r, blk);    \
+        break;
+        EXOTX_FFT_ENS_CASE(64)
+        EXOTX_FFT_ENS_CASE(128)
+        EXOTX_FFT_ENS_CASE(192)
+        EXOTX_FFT_ENS_CASE(256)
+        EXOTX_FFT_ENS_CASE(320)
+        EXOTX_FFT_ENS_CASE(384)
+        EXOTX_FFT_ENS_CASE(512)
+#undef EXOTX_FFT_ENS_CASE
+        default: break;
+    }
+}
+
+static bool ens_len(int n) {
+    return n == 64 || n == 128 || n == 192 || n == 256 || n == 320 || n == 384 || n == 512;
+}
+static bool aligned16_(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s) {
+    if (nseg < 1 || nseg > FFT_ENS_MAXSEG) return EXOTX_BAD_ARG;
+    FftEnsLaunch P;
+    P.nseg = nseg;
+    int blocks = 0;
+    size_t smem = 0;
+    for (int i = 0; i < nseg; i++) {
+        const FftEnsSeg &g = segs[i];
+        if (!ens_len(g.n)) return EXOTX_NOT_BUILT;
+        if (!aligned16_(g.in) || !aligned16_(g.out)) return EXOTX_BAD_ARG;
+        exotx_status st;
+        const FftTables *t = fft_tables(g.n, &st);
+        if (!t) return st;
+        const int rows = ct_rows<float>(g.n);
+        FftEnsArgs &a = P.seg[i];
+        a.in = g.in; a.out = g.out; a.lot = g.lot; a.f_rs = g.f_rs; a.f_ms = g.f_ms; a.n = g.n; a.kf = g.kf;
+        a.w = reinterpret_cast<const cpx<float> *>(t->w32);
+        a.r = reinterpret_cast<const cpx<float> *>(t->r32);
+        a.block0 = blocks;
+        blocks += (int)((g.lot + rows - 1) / rows);
+        smem = std::max(smem, (2 * (size_t)rows * (g.n / 2) + g.n / 2 + g.n / 2 + 1) * sizeof(cpx<float>));
+    }
+    if (blocks == 0) return EXOTX_OK;
+    const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
+    if (fwd) {
+        if (smem > 48 * 1024)
+            EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_ens<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    } else if (smem > 48 * 1024) {
+        EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_ens<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    cudaEvent_t ev = ktimer_start(kid, s);
+    if (fwd) k_rfft_ens<true><<<blocks, 256, smem, s>>>(P);
+    else k_rfft_ens<false><<<blocks, 256, smem, s>>>(P);
+    EXOTX_CHECK_LAUNCH();
+    ktimer_stop(kid, s, ev);
+    return EXOTX_OK;
 }
 
 template <typename T, int N>

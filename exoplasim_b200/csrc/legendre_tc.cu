@@ -323,17 +323,19 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
         const int4 *jl = jobs;
         int nj = njobs;
         if (ni != chunk) EXOTX_TRY(tc_jobs(p, T, 0, L, ni, &jl, &nj));
-        TcInvArgs A;
+        TcInvLaunch P;
+        P.jobs = jl;
+        P.nprod = 6;
+        TcInvArgs &A = P.seg[0];
         A.tab = T->inv; A.off = T->d_inv_off; A.woff = p->d_woff;
         A.spin = spin + (size_t)i0 * (4 * L + 1) * nrsp;
         A.filt = p->d_fs32;
         A.W = (float2 *)p->d_work;
         A.nrows = (long long)ni * nfo * p->nlat;
-        A.jobs = jl;
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.nj8 = T->nj8; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
         A.plavor = (float)p->desc.plavor;
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
-        k_tc_inverse<<<nj, TCT2, smem, s>>>(A);
+        k_tc_inverse<<<nj, TCT2, smem, s>>>(P);
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
         EXOTX_TRY(fft_inverse_l<float>((const float *)p->d_work, gpout + (size_t)i0 * nfo * nhor, p->nlon, A.nrows,
@@ -365,16 +367,131 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
         const long long nrows = (long long)ni * nfi * p->nlat;
         EXOTX_TRY(fft_forward_l<float>(gpin + (size_t)i0 * nfi * nhor, (float *)p->d_work, p->nlon, nrows, p->ntp1,
                                        1, nrows, s));
-        TcFwdArgs A;
+        TcFwdLaunch P;
+        P.jobs = jl;
+        P.nprod = 6;
+        TcFwdArgs &A = P.seg[0];
         A.tab = T->fwd; A.off = T->d_fwd_off; A.woff = p->d_woff;
         A.W = (const float2 *)p->d_work;
         A.nrows = nrows;
         A.filt = p->d_fg32;
         A.spout = spout + (size_t)i0 * (4 * L + 1) * nrsp;
-        A.jobs = jl;
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.njc = T->njc; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
-        k_tc_forward<<<nj, TCT2, smem, s>>>(A);
+        k_tc_forward<<<nj, TCT2, smem, s>>>(P);
+        EXOTX_CHECK_LAUNCH();
+        ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
+    }
+    return EXOTX_OK;
+}
+
+// ---------------------------------------------------------- ensembles
+// Merged job list of an uneven ensemble: every segment's jobs, with the
+// inverse column tiles capped at nc_qi_cap / nc_uv_cap, optionally ordered by
+// decreasing work so the longest jobs start first.
+exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, int nc_uv_cap, bool sort,
+                         int4 **d_jobs, int *njobs, size_t *smem) {
+    if (nseg < 1 || nseg > TC_MAXSEG) return EXOTX_BAD_ARG;
+    std::vector<std::pair<long long, int4>> v;
+    size_t smax = 0;
+    for (int sgi = 0; sgi < nseg; sgi++) {
+        const EnsSeg &g = segs[sgi];
+        exotx_plan p = g.p;
+        TcTables *T;
+        EXOTX_TRY(tc_tables(p, &T));
+        const int L = g.L, ni = g.ninst;
+        if (dir == 0) {
+            int a, b;
+            inv_tiles(T->nj8, p->ntp1, &a, &b);
+            a = std::max(16, std::min(a, nc_qi_cap) & ~15);
+            b = std::max(16, std::min(b, nc_uv_cap) & ~15);
+            smax = std::max(smax, std::max(inv_smem(T->nj8, p->ntp1, a), inv_smem(T->nj8, p->ntp1, b)));
+            for (int m = 0; m < p->ntp1; m++) {
+                const int K = p->ntp1 - m;
+                const long long kw = pad16(kpar(K, 0)) + pad16(kpar(K, 1));
+                const int n0 = ni * (4 * L + 1) * 2, n1 = ni * 2, n2 = ni * L * 4;
+                for (int c = 0; c < n0; c += a)
+                    v.push_back({kw * a, make_int4(m, 0 | (sgi << 2), c, std::min(a, n0 - c))});
+                for (int c = 0; c < n1; c += a)
+                    v.push_back({kw * a, make_int4(m, 1 | (sgi << 2), c, std::min(a, n1 - c))});
+                for (int c = 0; c < n2; c += b)
+                    v.push_back({2 * kw * b, make_int4(m, 2 | (sgi << 2), c, std::min(b, n2 - c))});
+            }
+        } else {
+            smax = std::max(smax, fwd_smem(p->ntp1, T->njc));
+            for (int m = 0; m < p->ntp1; m++) {
+                const int K = p->ntp1 - m;
+                const long long kw = (long long)(pad8(kpar(K, 0)) + pad8(kpar(K, 1))) * T->njc;
+                for (int i = 0; i < ni; i++)
+                    for (int l0 = 0; l0 < L; l0 += FWD_LEV_TILE)
+                        v.push_back({kw, make_int4(m, i | (sgi << 16), l0, std::min(FWD_LEV_TILE, L - l0))});
+            }
+        }
+    }
+    if (smax > TC_SMEM_MAX) return EXOTX_BAD_DIM;
+    if (sort)
+        std::stable_sort(v.begin(), v.end(), [](const std::pair<long long, int4> &x,
+                                               const std::pair<long long, int4> &y) { return x.first > y.first; });
+    std::vector<int4> jobs(v.size());
+    for (size_t i = 0; i < v.size(); i++) jobs[i] = v[i].second;
+    int4 *d = nullptr;
+    EXOTX_CUDA(cudaMalloc(&d, sizeof(int4) * jobs.size()));
+    if (cudaMemcpy(d, jobs.data(), sizeof(int4) * jobs.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d);
+        return EXOTX_CUDA_ERR;
+    }
+    *d_jobs = d;
+    *njobs = (int)jobs.size();
+    *smem = smax;
+    return EXOTX_OK;
+}
+
+// one tensor-core launch over every segment: inverse (spin -> W) or forward (W -> spout)
+exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_jobs, int njobs, size_t smem,
+                        int nprod, cudaStream_t s) {
+    if (nseg < 1 || nseg > TC_MAXSEG || (nprod != 3 && nprod != 6)) return EXOTX_BAD_ARG;
+    if (njobs == 0) return EXOTX_OK;
+    if (dir == 0) {
+        TcInvLaunch P;
+        P.jobs = d_jobs;
+        P.nprod = nprod;
+        for (int i = 0; i < nseg; i++) {
+            const EnsSeg &g = segs[i];
+            exotx_plan p = g.p;
+            TcTables *T;
+            EXOTX_TRY(tc_tables(p, &T));
+            TcInvArgs &A = P.seg[i];
+            A.tab = T->inv; A.off = T->d_inv_off; A.woff = p->d_woff;
+            A.spin = g.spin; A.filt = p->d_fs32; A.W = (float2 *)g.W;
+            A.nrows = (long long)g.ninst * (6 * g.L + 3) * p->nlat;
+            A.L = g.L; A.nlat = p->nlat; A.nlath = p->nlath; A.nj8 = T->nj8; A.ntp1 = p->ntp1;
+            A.nrsp = 2 * p->ncsp; A.plavor = (float)p->desc.plavor;
+        }
+        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+        cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
+        k_tc_inverse<<<njobs, TCT2, smem, s>>>(P);
+        EXOTX_CHECK_LAUNCH();
+        ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
+    } else {
+        TcFwdLaunch P;
+        P.jobs = d_jobs;
+        P.nprod = nprod;
+        for (int i = 0; i < nseg; i++) {
+            const EnsSeg &g = segs[i];
+            exotx_plan p = g.p;
+            TcTables *T;
+            EXOTX_TRY(tc_tables(p, &T));
+            TcFwdArgs &A = P.seg[i];
+            A.tab = T->fwd; A.off = T->d_fwd_off; A.woff = p->d_woff;
+            A.W = (const float2 *)g.W;
+            A.nrows = (long long)g.ninst * (9 * g.L + 1) * p->nlat;
+            A.filt = p->d_fg32; A.spout = g.spout;
+            A.L = g.L; A.nlat = p->nlat; A.nlath = p->nlath; A.njc = T->njc; A.ntp1 = p->ntp1;
+            A.nrsp = 2 * p->ncsp;
+        }
+        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+        cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
+        k_tc_forward<<<njobs, TCT2, smem, s>>>(P);
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
     }

@@ -19,9 +19,17 @@ struct TcInvArgs {
     const float *filt;      // skspgp
     float2 *W;              // [m][row], row = (inst*(6L+3) + field)*nlat + lat
     long long nrows;
-    const int4 *jobs;
     int L, nlat, nlath, nj8, ntp1, nrsp;
     float plavor;
+};
+
+// One launch covers up to TC_MAXSEG segments (a resolution, a level count and
+// a run of instances each); a job names its segment.  nprod = 6 keeps every
+// split product of order <= 2 (3-term split); nprod = 3 keeps a0b0, a0b1, a1b0.
+struct TcInvLaunch {
+    TcInvArgs seg[TC_MAXSEG];
+    const int4 *jobs;       // (m, group | seg << 2, first column, columns)
+    int nprod;
 };
 
 // spectral row (complex, filter not applied) feeding column pair gq, and
@@ -42,10 +50,12 @@ __device__ __forceinline__ const float2 *inv_row(const TcInvArgs &A, int group, 
     return reinterpret_cast<const float2 *>(A.spin + ((size_t)inst * nf + f) * A.nrsp);
 }
 
-__global__ void __launch_bounds__(TCT2) k_tc_inverse(TcInvArgs A) {
+__global__ void __launch_bounds__(TCT2) k_tc_inverse(const __grid_constant__ TcInvLaunch P) {
     extern __shared__ __align__(128) unsigned char sm[];
-    const int4 jb = A.jobs[blockIdx.x];
-    const int m = jb.x, group = jb.y, c0 = jb.z, nc = jb.w;
+    const int4 jb = P.jobs[blockIdx.x];
+    const TcInvArgs &A = P.seg[jb.y >> 2];
+    const int nprod = P.nprod;
+    const int m = jb.x, group = jb.y & 3, c0 = jb.z, nc = jb.w;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, half = warp >> 2;
     const int K = A.ntp1 - m;
     const int Kq[2] = {kpar(K, 0), kpar(K, 1)};
@@ -149,9 +159,10 @@ __global__ void __launch_bounds__(TCT2) k_tc_inverse(TcInvArgs A) {
                 for (int kc = 0; kc < Kp[p] / 16; kc++) {
 #pragma unroll
                     for (int pr = 0; pr < 6; pr++)
-                        tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
-                                     tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 256), idesc,
-                                     kc > 0 || pr > 1);
+                        if (pr < nprod)
+                            tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
+                                         tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 256), idesc,
+                                         kc > 0 || pr > 1);
                 }
                 to += 3 * ttile[p];
                 dd += 3 * dtile[p];
@@ -260,8 +271,13 @@ struct TcFwdArgs {
     long long nrows;
     const float *filt;      // skgpsp
     float *spout;           // [inst][4L+1][NRSP]
-    const int4 *jobs;
     int L, nlat, nlath, njc, ntp1, nrsp;
+};
+
+struct TcFwdLaunch {
+    TcFwdArgs seg[TC_MAXSEG];
+    const int4 *jobs;       // (m, inst | seg << 16, first level, levels)
+    int nprod;
 };
 
 // Columns of one forward job (levels l0..l0+nl-1 of one instance), per table,
@@ -288,10 +304,12 @@ __device__ __forceinline__ long long fwd_row(int L, int inst, int kind, int l) {
     return (long long)inst * nfi + F;
 }
 
-__global__ void __launch_bounds__(TCT2) k_tc_forward(TcFwdArgs A) {
+__global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcFwdLaunch P) {
     extern __shared__ __align__(128) unsigned char sm[];
-    const int4 jb = A.jobs[blockIdx.x];
-    const int m = jb.x, inst = jb.y, l0 = jb.z, nl = jb.w;
+    const int4 jb = P.jobs[blockIdx.x];
+    const TcFwdArgs &A = P.seg[jb.y >> 16];
+    const int nprod = P.nprod;
+    const int m = jb.x, inst = jb.y & 0xffff, l0 = jb.z, nl = jb.w;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, half = warp >> 2;
     const int K = A.ntp1 - m;
     const int Kq[2] = {kpar(K, 0), kpar(K, 1)};
@@ -426,9 +444,10 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(TcFwdArgs A) {
                     for (int kc = 0; kc < jw / 16; kc++) {
 #pragma unroll
                         for (int pr = 0; pr < 6; pr++)
-                            tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
-                                         tc::desc_add(db0, tc::pair_b(pr) * dt + (j0 / 8) * 128 + kc * 256), idesc,
-                                         j0 > 0 || kc > 0 || pr > 1);
+                            if (pr < nprod)
+                                tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
+                                             tc::desc_add(db0, tc::pair_b(pr) * dt + (j0 / 8) * 128 + kc * 256),
+                                             idesc, j0 > 0 || kc > 0 || pr > 1);
                     }
                     jo += 3 * tt;
                 }

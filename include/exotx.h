@@ -126,6 +126,34 @@ exotx_status exotx_inverse_set_batch(exotx_plan p, int prec, const void *spin, v
                                      int nlev, int ninst, exotx_stream s);
 exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const void *gpin, void *spout,
                                      int nlev, int ninst, exotx_stream s);
+/* Uneven ensembles (no counterpart in the reference, which runs one model
+ * state per process): ninst instances with their own nlat (NLON = 2 NLAT) and
+ * level count, MIXED precision (float arrays).  Instances of one resolution
+ * and level count form a segment (at most 12 segments); each half of the
+ * round trip (plasim.f90 gridpointa :2396-2486, as inverse_set/forward_set)
+ * is one tensor-core Legendre launch and one FFT launch over every segment.
+ * Arrays are packed: instance i's spectral data (4L+1 x NRSP, input of the
+ * inverse half and output of the forward half) start at spec_off[i] floats,
+ * its forward-half grid input (9L+1 fields) at gin_off[i], its inverse-half
+ * grid output (6L+3 fields) at gout_off[i]; totals[3] are the three lengths. */
+typedef struct exotx_ensemble_s *exotx_ensemble;
+exotx_status exotx_ensemble_create(int ninst, const int *nlat, const int *nlev, exotx_ensemble *out);
+exotx_status exotx_ensemble_destroy(exotx_ensemble e);
+/* HOST arrays of ninst offsets (each may be NULL) and totals[3] */
+exotx_status exotx_ensemble_layout(exotx_ensemble e, long long *spec_off, long long *gin_off,
+                                   long long *gout_off, long long *totals);
+exotx_status exotx_ensemble_inverse(exotx_ensemble e, const float *spin, float *gpout, exotx_stream s);
+exotx_status exotx_ensemble_forward(exotx_ensemble e, const float *gpin, float *spout, exotx_stream s);
+/* tile caps of the inverse column tiles (qi/qj and qu/qv jobs), job order
+ * (1 = longest first), split products (6 = 3-term BF16 split, 3 = 2-term) */
+exotx_status exotx_ensemble_configure(exotx_ensemble e, int nc_qi, int nc_uv, int sorted, int nprod);
+/* Autotuner: times every combination of tile caps {64,128} x {32,64}, job
+ * order and split products on these inputs (reps round trips each), keeps
+ * only those within 1e-6 relative L2 of the 3-term split, and configures the
+ * fastest.  choice (HOST, 4 ints, may be NULL) = nc_qi, nc_uv, sorted, nprod;
+ * *best_ms (HOST, may be NULL) = its round-trip time.  Synchronises s. */
+exotx_status exotx_ensemble_tune(exotx_ensemble e, const float *spin, float *gpout, const float *gpin,
+                                 float *spout, int reps, exotx_stream s, int *choice, float *best_ms);
 /* forward_set that allocates no device memory.  No counterpart in the
  * reference (which has no device memory to allocate); it exists for callers
  * that cannot call cudaMalloc where they transform -- a host model whose own
