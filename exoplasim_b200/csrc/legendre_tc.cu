@@ -253,10 +253,9 @@ exotx_status tc_available() { return EXOTX_OK; }
 // inverse groups: 0 = qi on sd,st,sz,sq,sp; 1 = qj on sp; 2 = qu,qv on (D,Z)
 // forward groups: 0 = qc,qe,qm,qq on the mktend/qtend/fc2sp inputs (one level slab)
 // job = (m, group, first column, number of columns)
-static constexpr int FWD_LEV_TILE = 4;  // levels per forward job (shared-memory bound)
 static constexpr size_t TC_SMEM_MAX = 227 * 1024;
 
-static size_t inv_smem(int nj8, int K, int ncp);
+#include "legendre_tc_kernels.cuh"
 
 // inverse column tiles: as wide as shared memory (both parities of one table
 // plus the staged columns) and TMEM (tables x parities x columns <= 256) allow
@@ -266,6 +265,32 @@ static void inv_tiles(int nj8, int ntp1, int *nc_qi, int *nc_uv) {
     while (b > 16 && inv_smem(nj8, ntp1, b) > TC_SMEM_MAX) b -= 16;
     *nc_qi = a;
     *nc_uv = b;
+}
+
+// forward kernel variants, tried in order until the widest job fits shared memory:
+// 4 levels per job with both table halves resident, 4 levels with one half
+// buffer, 2 levels with one half buffer
+static const int kFwdNlt[3] = {4, 4, 2};
+static const bool kFwdOne[3] = {false, true, true};
+static int fwd_level(exotx_plan p, const TcTables *T) {
+    for (int v = 0; v < 3; v++)
+        if (fwd_smem(p->ntp1, T->njc, kFwdNlt[v], kFwdOne[v]) <= TC_SMEM_MAX) return v;
+    return -1;
+}
+static exotx_status launch_fwd(const TcFwdLaunch &P, int level, int njobs, size_t smem, cudaStream_t s) {
+    cudaEvent_t ev = nullptr;
+    if (kFwdNlt[level] == 4) {
+        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+        ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
+        k_tc_forward<4><<<njobs, TCT2, smem, s>>>(P);
+    } else {
+        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+        ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
+        k_tc_forward<2><<<njobs, TCT2, smem, s>>>(P);
+    }
+    EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
+    return EXOTX_OK;
 }
 
 static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst, const int4 **d, int *njobs) {
@@ -281,10 +306,11 @@ static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst
             for (int c = 0; c < n1; c += INV_NC_QI) v.push_back(make_int4(m, 1, c, std::min(INV_NC_QI, n1 - c)));
             for (int c = 0; c < n2; c += INV_NC_UV) v.push_back(make_int4(m, 2, c, std::min(INV_NC_UV, n2 - c)));
         } else {
-            // slabs of FWD_LEV_TILE levels of one instance; the level-independent gvpp rides with slab 0
+            // slabs of nlt levels of one instance; the level-independent gvpp rides with slab 0
+            const int lv = fwd_level(p, T), nlt = lv < 0 ? 2 : kFwdNlt[lv];
             for (int i = 0; i < ninst; i++)
-                for (int l0 = 0; l0 < L; l0 += FWD_LEV_TILE)
-                    v.push_back(make_int4(m, i, l0, std::min(FWD_LEV_TILE, L - l0)));
+                for (int l0 = 0; l0 < L; l0 += nlt)
+                    v.push_back(make_int4(m, i, l0, std::min(nlt, L - l0)));
         }
     }
     TcTables::Jobs J;
@@ -296,8 +322,6 @@ static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst
     *njobs = J.njobs;
     return EXOTX_OK;
 }
-
-#include "legendre_tc_kernels.cuh"
 
 // ---------------------------------------------------------- set drivers
 exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int L, int ninst, cudaStream_t s) {
@@ -356,9 +380,9 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
     const int4 *jobs;
     int njobs;
     EXOTX_TRY(tc_jobs(p, T, 1, L, chunk, &jobs, &njobs));
-    size_t smem = fwd_smem(p->ntp1, T->njc);
-    if (smem > TC_SMEM_MAX) return EXOTX_BAD_DIM;
-    EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+    const int lv = fwd_level(p, T);
+    if (lv < 0) return EXOTX_BAD_DIM;
+    const size_t smem = fwd_smem(p->ntp1, T->njc, kFwdNlt[lv], kFwdOne[lv]);
     for (int i0 = 0; i0 < ninst; i0 += chunk) {
         const int ni = std::min(chunk, ninst - i0);
         const int4 *jl = jobs;
@@ -370,6 +394,7 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
         TcFwdLaunch P;
         P.jobs = jl;
         P.nprod = 6;
+        P.onebuf = kFwdOne[lv];
         TcFwdArgs &A = P.seg[0];
         A.tab = T->fwd; A.off = T->d_fwd_off; A.woff = p->d_woff;
         A.W = (const float2 *)p->d_work;
@@ -377,10 +402,7 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
         A.filt = p->d_fg32;
         A.spout = spout + (size_t)i0 * (4 * L + 1) * nrsp;
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.njc = T->njc; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
-        cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
-        k_tc_forward<<<nj, TCT2, smem, s>>>(P);
-        EXOTX_CHECK_LAUNCH();
-        ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
+        EXOTX_TRY(launch_fwd(P, lv, nj, smem, s));
     }
     return EXOTX_OK;
 }
@@ -394,6 +416,14 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
     if (nseg < 1 || nseg > TC_MAXSEG) return EXOTX_BAD_ARG;
     std::vector<std::pair<long long, int4>> v;
     size_t smax = 0;
+    int lv = 0;  // forward variant shared by every segment of the launch
+    for (int sgi = 0; sgi < nseg && dir == 1; sgi++) {
+        TcTables *T;
+        EXOTX_TRY(tc_tables(segs[sgi].p, &T));
+        const int l = fwd_level(segs[sgi].p, T);
+        if (l < 0) return EXOTX_BAD_DIM;
+        lv = std::max(lv, l);
+    }
     for (int sgi = 0; sgi < nseg; sgi++) {
         const EnsSeg &g = segs[sgi];
         exotx_plan p = g.p;
@@ -418,13 +448,14 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
                     v.push_back({2 * kw * b, make_int4(m, 2 | (sgi << 2), c, std::min(b, n2 - c))});
             }
         } else {
-            smax = std::max(smax, fwd_smem(p->ntp1, T->njc));
+            const int nlt = kFwdNlt[lv];
+            smax = std::max(smax, fwd_smem(p->ntp1, T->njc, nlt, kFwdOne[lv]));
             for (int m = 0; m < p->ntp1; m++) {
                 const int K = p->ntp1 - m;
                 const long long kw = (long long)(pad8(kpar(K, 0)) + pad8(kpar(K, 1))) * T->njc;
                 for (int i = 0; i < ni; i++)
-                    for (int l0 = 0; l0 < L; l0 += FWD_LEV_TILE)
-                        v.push_back({kw, make_int4(m, i | (sgi << 16), l0, std::min(FWD_LEV_TILE, L - l0))});
+                    for (int l0 = 0; l0 < L; l0 += nlt)
+                        v.push_back({kw, make_int4(m, i | (sgi << 16), l0, std::min(nlt, L - l0))});
             }
         }
     }
@@ -476,6 +507,15 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
         TcFwdLaunch P;
         P.jobs = d_jobs;
         P.nprod = nprod;
+        int lv = 0;
+        for (int i = 0; i < nseg; i++) {
+            TcTables *T;
+            EXOTX_TRY(tc_tables(segs[i].p, &T));
+            const int l = fwd_level(segs[i].p, T);
+            if (l < 0) return EXOTX_BAD_DIM;
+            lv = std::max(lv, l);
+        }
+        P.onebuf = kFwdOne[lv];
         for (int i = 0; i < nseg; i++) {
             const EnsSeg &g = segs[i];
             exotx_plan p = g.p;
@@ -489,11 +529,7 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
             A.L = g.L; A.nlat = p->nlat; A.nlath = p->nlath; A.njc = T->njc; A.ntp1 = p->ntp1;
             A.nrsp = 2 * p->ncsp;
         }
-        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
-        cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
-        k_tc_forward<<<njobs, TCT2, smem, s>>>(P);
-        EXOTX_CHECK_LAUNCH();
-        ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
+        EXOTX_TRY(launch_fwd(P, lv, njobs, smem, s));
     }
     return EXOTX_OK;
 }

@@ -278,21 +278,28 @@ struct TcFwdLaunch {
     TcFwdArgs seg[TC_MAXSEG];
     const int4 *jobs;       // (m, inst | seg << 16, first level, levels)
     int nprod;
+    int onebuf;             // 1: both parity halves of a table share one buffer (large grids)
 };
 
 // Columns of one forward job (levels l0..l0+nl-1 of one instance), per table,
-// laid out as if the slab always had FWD_LEV_TILE levels (fixed positions):
-//   column (fi, li, ri) = (fi*FWD_LEV_TILE + li)*2 + ri
-//   qc: tn, qn [+ gvpp at 2*2*FWD_LEV_TILE]   qe: fv, vt, fu, vq   qm: fu, ut, fv, uq   qq: ke
+// laid out as if the slab always had NLT levels (fixed positions):
+//   column (fi, li, ri) = (fi*NLT + li)*2 + ri
+//   qc: tn, qn [+ gvpp at 2*2*NLT]   qe: fv, vt, fu, vq   qm: fu, ut, fv, uq   qq: ke
 // gpin field kinds: gtn 0, gqn 1, gut 2, gvt 3, guz 4, gvz 5, gke 6, gvpp 7, guq 8, gvq 9;
 // mktend call: tn=gtn, fu=gvz, fv=guz, ke=gke, ut=gut, vt=gvt; qtend: qn=gqn, uq=guq, vq=gvq
-constexpr int NLT = FWD_LEV_TILE;
 __device__ __constant__ int c_fwd_nf[4] = {2, 4, 4, 1};
 __device__ __constant__ int c_fwd_fields[4][4] = {{0, 1, -1, -1}, {4, 3, 5, 9}, {5, 2, 4, 8}, {6, -1, -1, -1}};
-__host__ __device__ constexpr int fwd_ncol(int t) { return t == 0 ? 2 * NLT * 2 + 2 : (t == 3 ? NLT * 2 : 4 * NLT * 2); }
-__host__ __device__ constexpr int fwd_ncp(int t) { return (fwd_ncol(t) + 15) & ~15; }
-__host__ __device__ constexpr int fwd_colbase(int t) {
-    return t == 0 ? 0 : fwd_colbase(t - 1) + 4 * fwd_ncp(t - 1);  // 2 parities x (main, correction)
+template <int NLT> __host__ __device__ constexpr int fwd_ncol(int t) {
+    return t == 0 ? 2 * NLT * 2 + 2 : (t == 3 ? NLT * 2 : 4 * NLT * 2);
+}
+template <int NLT> __host__ __device__ constexpr int fwd_ncp(int t) { return (fwd_ncol<NLT>(t) + 15) & ~15; }
+template <int NLT> __host__ __device__ constexpr int fwd_colbase(int t) {
+    return t == 0 ? 0 : fwd_colbase<NLT>(t - 1) + 4 * fwd_ncp<NLT>(t - 1);  // 2 parities x (main, correction)
+}
+// TMEM loads of 16 or 32 columns without the wait
+template <int NC> __device__ __forceinline__ void tmem_ld_nw(uint32_t taddr, uint32_t *r) {
+    if constexpr (NC >= 32) tc::tmem_ld32_nw(taddr, r);
+    else tc::tmem_ld16_nw(taddr, r);
 }
 
 __device__ __forceinline__ long long fwd_row(int L, int inst, int kind, int l) {
@@ -304,6 +311,7 @@ __device__ __forceinline__ long long fwd_row(int L, int inst, int kind, int l) {
     return (long long)inst * nfi + F;
 }
 
+template <int NLT>
 __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcFwdLaunch P) {
     extern __shared__ __align__(128) unsigned char sm[];
     const int4 jb = P.jobs[blockIdx.x];
@@ -316,32 +324,34 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
     const int R[2] = {pad8(Kq[0]), pad8(Kq[1])};
     const int njc = A.njc, L = A.L, nlat = A.nlat;
     const bool with_vpp = (l0 == 0);
-    size_t tblk = 0;
-    for (int p = 0; p < 2; p++) if (Kq[p]) tblk += 3 * (size_t)R[p] * njc * 2;
+    const bool onebuf = P.onebuf != 0;
+    // a table block is [parity 0: 3 splits x R0 rows][parity 1: 3 splits x R1 rows];
+    // the halves travel separately, into two buffers so the next table's half 0
+    // lands while half 1 computes, or (large grids) one after the other into one
+    const uint32_t hbytes[2] = {(uint32_t)(3 * R[0] * njc * 2), (uint32_t)(3 * R[1] * njc * 2)};
+    const uint32_t hoff[2] = {0u, hbytes[0]};                 // in the global block
+    const uint32_t soff[2] = {0u, onebuf ? 0u : hbytes[0]};   // in shared memory
+    const size_t tregion = onebuf ? hbytes[0] : (size_t)hbytes[0] + hbytes[1];
     // rows >= R of the M=128 table tiles read past the block: keep a margin
     // before the data so those reads (whose TMEM lanes are never used) stay in bounds
     unsigned char *tab = sm;
-    unsigned char *dat = sm + tblk + 128 * 32 * 2;
+    unsigned char *dat = sm + tregion + 128 * 32 * 2;
     size_t doffs[4], dbytes = 0;
-    for (int t = 0; t < 4; t++) { doffs[t] = dbytes; dbytes += 2 * 3 * (size_t)fwd_ncp(t) * njc * 2; }
+    for (int t = 0; t < 4; t++) { doffs[t] = dbytes; dbytes += 2 * 3 * (size_t)fwd_ncp<NLT>(t) * njc * 2; }
     unsigned char *tail = dat + dbytes;
     uint64_t *bars = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
     uint64_t *bar_tma = bars;       // [2] table half of parity p landed
     uint64_t *bar_mma = bars + 2;   // [2] MMAs reading table half p completed
     uint64_t *bar_done = bars + 4;  // every MMA completed
     uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 5);
-    // a table block is [parity 0: 3 splits x R0 rows][parity 1: 3 splits x R1 rows];
-    // the halves travel separately so the next table's half 0 lands while half 1 computes
-    const uint32_t hbytes[2] = {(uint32_t)(3 * R[0] * njc * 2), (uint32_t)(3 * R[1] * njc * 2)};
-    const uint32_t hoff[2] = {0u, hbytes[0]};
     if (warp == 0) tc::tmem_alloc(slot, 512);
     if (tid == 0) {
         for (int i = 0; i < 5; i++) tc::mbar_init(bars + i, 1);
         tc::mbar_fence_init();
         for (int p = 0; p < 2; p++)
-            if (Kq[p]) {
+            if (Kq[p] && (p == 0 || !onebuf)) {
                 tc::mbar_arrive_expect_tx(bar_tma + p, hbytes[p]);
-                tc::bulk_g2s(tab + hoff[p], A.tab + A.off[m * 4 + 0] + hoff[p], hbytes[p], bar_tma + p);
+                tc::bulk_g2s(tab + soff[p], A.tab + A.off[m * 4 + 0] + hoff[p], hbytes[p], bar_tma + p);
             }
     }
     // stage folded Fourier columns: for each table, S (= N+S) and D (= N-S)
@@ -351,7 +361,7 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
     const int ng = njc >> 3;
     for (int t = 0; t < 4; t++) {
         const int nf = c_fwd_nf[t];
-        const int ncp = fwd_ncp(t), npair = ncp >> 1;
+        const int ncp = fwd_ncp<NLT>(t), npair = ncp >> 1;
         const int nreal = nf * NLT + ((t == 0) ? 1 : 0);  // column pairs in use (incl. padding levels)
         const uint32_t dt = (uint32_t)ncp * njc * 2;       // one split tile
         unsigned char *bS = dat + doffs[t], *bD = bS + 3 * dt;
@@ -421,26 +431,27 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
     bool ok = true;
     if (tid == 0) {
         const uint32_t sbo_b = (uint32_t)(njc / 8) * 128;
+        int u = 0;  // table-half units issued (one-buffer mode)
         for (int t = 0; t < 4 && ok; t++) {
-            const int ncp = fwd_ncp(t);
+            const int ncp = fwd_ncp<NLT>(t);
             const uint32_t idesc = tc::idesc_bf16(128, ncp);
             const uint32_t dt = (uint32_t)ncp * njc * 2;
             // P-type (qc, qm, qq) use N+S on even n-m and N-S on odd; Q-type (qe) the reverse
             const bool ptype = (t != 1);
             for (int p = 0; p < 2 && ok; p++) {
                 if (!Kq[p]) break;
-                ok = tc::mbar_wait(bar_tma + p, t & 1);
+                ok = onebuf ? tc::mbar_wait(bar_tma, u & 1) : tc::mbar_wait(bar_tma + p, t & 1);
                 if (!ok) break;
                 tc::fence_after_sync();
                 const int sel = ptype ? p : 1 - p;  // 0 -> S, 1 -> D
                 const uint64_t db0 = tc::smem_desc(dat + doffs[t] + (size_t)sel * 3 * dt, 128, sbo_b);
-                const uint32_t dm = tmem + (uint32_t)(fwd_colbase(t) + (2 * p + 0) * ncp);
-                const uint32_t dc = tmem + (uint32_t)(fwd_colbase(t) + (2 * p + 1) * ncp);
+                const uint32_t dm = tmem + (uint32_t)(fwd_colbase<NLT>(t) + (2 * p + 0) * ncp);
+                const uint32_t dc = tmem + (uint32_t)(fwd_colbase<NLT>(t) + (2 * p + 1) * ncp);
                 uint32_t jo = 0;
                 for (int j0 = 0; j0 < njc; j0 += 32) {
                     const int jw = njc - j0 < 32 ? njc - j0 : 32;
                     const uint32_t tt = (uint32_t)R[p] * jw * 2;
-                    const uint64_t da0 = tc::smem_desc(tab + hoff[p] + jo, 128, (uint32_t)(jw / 8) * 128);
+                    const uint64_t da0 = tc::smem_desc(tab + soff[p] + jo, 128, (uint32_t)(jw / 8) * 128);
                     for (int kc = 0; kc < jw / 16; kc++) {
 #pragma unroll
                         for (int pr = 0; pr < 6; pr++)
@@ -451,10 +462,25 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
                     }
                     jo += 3 * tt;
                 }
-                if (t < 3) tc::mma_commit(bar_mma + p);
+                if (onebuf) {
+                    // the next half may overwrite the buffer once these MMAs have read it
+                    const bool last = t == 3 && (p == 1 || !Kq[1]);
+                    if (!last) {
+                        tc::mma_commit(bar_mma);
+                        ok = tc::mbar_wait(bar_mma, u & 1);
+                        if (ok) {
+                            const int tn = (p == 0 && Kq[1]) ? t : t + 1, pn = (p == 0 && Kq[1]) ? 1 : 0;
+                            tc::mbar_arrive_expect_tx(bar_tma, hbytes[pn]);
+                            tc::bulk_g2s(tab, A.tab + A.off[m * 4 + tn] + hoff[pn], hbytes[pn], bar_tma);
+                        }
+                    }
+                    u++;
+                } else if (t < 3) {
+                    tc::mma_commit(bar_mma + p);
+                }
             }
             // refill each half with the next table once its MMAs have drained
-            for (int p = 0; p < 2 && ok && t < 3; p++) {
+            for (int p = 0; p < 2 && ok && t < 3 && !onebuf; p++) {
                 if (!Kq[p]) break;
                 ok = tc::mbar_wait(bar_mma + p, t & 1);
                 if (!ok) break;
@@ -483,11 +509,11 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
         uint32_t rm[32], rc[32];
         float v[32];
         // table qc (t=0): tn -> t, qn -> q, gvpp -> spf
-        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(0) + (2 * p) * fwd_ncp(0)), rm);
-        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(0) + (2 * p + 1) * fwd_ncp(0)), rc);
+        tmem_ld_nw<fwd_ncp<NLT>(0)>(tmem + lane_addr + (uint32_t)(fwd_colbase<NLT>(0) + (2 * p) * fwd_ncp<NLT>(0)), rm);
+        tmem_ld_nw<fwd_ncp<NLT>(0)>(tmem + lane_addr + (uint32_t)(fwd_colbase<NLT>(0) + (2 * p + 1) * fwd_ncp<NLT>(0)), rc);
         tc::tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 32; i++) v[i] = __uint_as_float(rm[i]) + __uint_as_float(rc[i]);
+        for (int i = 0; i < 32; i++) v[i] = i < fwd_ncp<NLT>(0) ? __uint_as_float(rm[i]) + __uint_as_float(rc[i]) : 0.f;
 #pragma unroll
         for (int li = 0; li < NLT; li++) {
             ot[li][0] += v[(0 * NLT + li) * 2]; ot[li][1] += v[(0 * NLT + li) * 2 + 1];
@@ -495,11 +521,11 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
         }
         ov[0] = v[2 * NLT * 2]; ov[1] = v[2 * NLT * 2 + 1];
         // table qe (t=1): fv -> d (-), vt -> t, fu -> z, vq -> q
-        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(1) + (2 * p) * fwd_ncp(1)), rm);
-        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(1) + (2 * p + 1) * fwd_ncp(1)), rc);
+        tmem_ld_nw<fwd_ncp<NLT>(1)>(tmem + lane_addr + (uint32_t)(fwd_colbase<NLT>(1) + (2 * p) * fwd_ncp<NLT>(1)), rm);
+        tmem_ld_nw<fwd_ncp<NLT>(1)>(tmem + lane_addr + (uint32_t)(fwd_colbase<NLT>(1) + (2 * p + 1) * fwd_ncp<NLT>(1)), rc);
         tc::tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 32; i++) v[i] = __uint_as_float(rm[i]) + __uint_as_float(rc[i]);
+        for (int i = 0; i < 32; i++) v[i] = i < fwd_ncp<NLT>(1) ? __uint_as_float(rm[i]) + __uint_as_float(rc[i]) : 0.f;
 #pragma unroll
         for (int li = 0; li < NLT; li++)
 #pragma unroll
@@ -510,11 +536,11 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
                 oq[li][ri] += v[(3 * NLT + li) * 2 + ri];
             }
         // table qm (t=2): i*fu -> d, -i*ut -> t, i*fv -> z, -i*uq -> q  (i*(a+ib) = -b + ia)
-        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(2) + (2 * p) * fwd_ncp(2)), rm);
-        tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(2) + (2 * p + 1) * fwd_ncp(2)), rc);
+        tmem_ld_nw<fwd_ncp<NLT>(2)>(tmem + lane_addr + (uint32_t)(fwd_colbase<NLT>(2) + (2 * p) * fwd_ncp<NLT>(2)), rm);
+        tmem_ld_nw<fwd_ncp<NLT>(2)>(tmem + lane_addr + (uint32_t)(fwd_colbase<NLT>(2) + (2 * p + 1) * fwd_ncp<NLT>(2)), rc);
         tc::tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 32; i++) v[i] = __uint_as_float(rm[i]) + __uint_as_float(rc[i]);
+        for (int i = 0; i < 32; i++) v[i] = i < fwd_ncp<NLT>(2) ? __uint_as_float(rm[i]) + __uint_as_float(rc[i]) : 0.f;
 #pragma unroll
         for (int li = 0; li < NLT; li++) {
             const float fur = v[(0 * NLT + li) * 2], fui = v[(0 * NLT + li) * 2 + 1];
@@ -527,8 +553,8 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
             oq[li][0] += uqi; oq[li][1] -= uqr;
         }
         // table qq (t=3): ke -> d
-        tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(3) + (2 * p) * fwd_ncp(3)), rm);
-        tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(fwd_colbase(3) + (2 * p + 1) * fwd_ncp(3)), rc);
+        tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(fwd_colbase<NLT>(3) + (2 * p) * fwd_ncp<NLT>(3)), rm);
+        tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(fwd_colbase<NLT>(3) + (2 * p + 1) * fwd_ncp<NLT>(3)), rc);
         tc::tmem_wait_ld();
 #pragma unroll
         for (int li = 0; li < NLT; li++) {
@@ -564,13 +590,19 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
     if (warp == 0) tc::tmem_dealloc(tmem, 512);
 }
 
-static size_t fwd_smem(int K, int njc) {
-    size_t tblk = 0;
+static int fwd_ncp_rt(int nlt, int t) {
+    const int c = t == 0 ? 4 * nlt + 2 : (t == 3 ? 2 * nlt : 8 * nlt);
+    return (c + 15) & ~15;
+}
+// shared memory of a forward job at the widest m (K = NTP1 modes)
+static size_t fwd_smem(int K, int njc, int nlt, bool onebuf) {
+    size_t h[2] = {0, 0};
     for (int p = 0; p < 2; p++) {
         const int Kq = kpar(K, p);
-        if (Kq) tblk += 3 * (size_t)pad8(Kq) * njc * 2;
+        if (Kq) h[p] = 3 * (size_t)pad8(Kq) * njc * 2;
     }
+    const size_t tblk = onebuf ? std::max(h[0], h[1]) : h[0] + h[1];
     size_t d = 0;
-    for (int t = 0; t < 4; t++) d += 2 * 3 * (size_t)fwd_ncp(t) * njc * 2;
+    for (int t = 0; t < 4; t++) d += 2 * 3 * (size_t)fwd_ncp_rt(nlt, t) * njc * 2;
     return tblk + 128 * 32 * 2 + d + 80;
 }

@@ -35,7 +35,7 @@ def _plan(plans, nlat):
     return plans[nlat]
 
 
-@pytest.mark.parametrize("nlat,nlev", [(32, 10), (64, 20), (96, 10), (192, 20)])
+@pytest.mark.parametrize("nlat,nlev", [(32, 10), (64, 20), (96, 10), (192, 20), (256, 25)])
 def test_mixed_sets_vs_oracle(plans, oracle, nlat, nlev):
     P = _plan(plans, nlat)
     L = oracle.Leg(nlat)

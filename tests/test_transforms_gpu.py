@@ -226,7 +226,7 @@ def test_smallest_resolution(plans, oracle):
     assert relerr(out[0], L.sp2fc(sp[0])) < FP64_TOL
 
 
-@pytest.mark.parametrize("nlat,nlev", [(32, 10), (64, 20), (96, 10)])
+@pytest.mark.parametrize("nlat,nlev", [(32, 10), (64, 20), (96, 10), (256, 25)])
 def test_transform_sets_fp64(plans, oracle, nlat, nlev):
     P = plans[nlat]
     L = oracle.Leg(nlat)
@@ -246,7 +246,7 @@ def test_transform_sets_fp64(plans, oracle, nlat, nlev):
     assert np.array_equal(gin_t.cpu().numpy(), gin)
 
 
-@pytest.mark.parametrize("nlat,nlev", [(64, 20), (192, 20)])
+@pytest.mark.parametrize("nlat,nlev", [(64, 20), (192, 20), (256, 25)])
 def test_transform_sets_fp32(plans, oracle, nlat, nlev):
     P = plans[nlat]
     L = oracle.Leg(nlat)
