@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const float *A, const float
         }
         tc::mma_commit(bar);
     }
-    bool ok = tc::mbar_wait(bar, 0);
+    bool ok = __all_sync(0xffffffffu, tc::mbar_wait(bar, 0));
     if (!ok && lane == 0) atomicExch(&g_tc_error, 1);
     tc::fence_after_sync();
     if (ok) {
@@ -113,11 +113,17 @@ struct TcTables {
     std::vector<int> fwd_bytes;
     unsigned char *inv = nullptr, *fwd = nullptr;
     long long *d_inv_off = nullptr, *d_fwd_off = nullptr;
+    // stacked-split forward tables (NTRU+1 <= 128): block (m, t, p) at [(m*4+t)*2+p]
+    bool has3 = false;
+    std::vector<long long> fwd3_off;
+    unsigned char *fwd3 = nullptr;
+    long long *d_fwd3_off = nullptr;
     // cached job lists, keyed by (direction, nlev, ninst)
     struct Jobs { int dir, nlev, ninst, njobs; int4 *d = nullptr; };
     std::vector<Jobs> jobs;
     ~TcTables() {
         cudaFree(inv); cudaFree(fwd); cudaFree(d_inv_off); cudaFree(d_fwd_off);
+        cudaFree(fwd3); cudaFree(d_fwd3_off);
         for (auto &j : jobs) cudaFree(j.d);
     }
 };
@@ -192,6 +198,34 @@ __global__ void k_build_tc_fwd(const double *qref, const int *woff, const long l
     }
 }
 
+// stacked-split forward block (m, t, p) = per latitude chunk of 32:
+// [S01: 2R rows (a0 of modes 0..R-1, then a1)][S2: 2R rows (zeros, then a2)] x chunk width
+__global__ void k_build_tc_fwd3(const double *qref, const int *woff, const long long *off3, int nlat, int nlath,
+                                int ncsp, int ntp1, int njc, int t, int tref, unsigned char *base) {
+    const int m = blockIdx.x, p = blockIdx.y;
+    const int K = ntp1 - m, Kq = kpar(K, p), R = pad8(Kq);
+    if (Kq == 0) return;
+    unsigned char *blk = base + off3[(m * 4 + t) * 2 + p];
+    const double *q = qref + (size_t)tref * ncsp * nlat;
+    size_t co = 0;
+    for (int j0 = 0; j0 < njc; j0 += 32) {
+        const int jw = min(32, njc - j0);
+        const size_t tt = (size_t)2 * R * jw * 2;
+        for (int idx = threadIdx.x; idx < 2 * R * jw; idx += blockDim.x) {
+            const int row = idx / jw, jj = idx % jw, j = j0 + jj;
+            const int mode = row < R ? row : row - R;
+            double v = 0.0;
+            if (mode < Kq && j < nlath) v = q[(size_t)j * ncsp + woff[m] + 2 * mode + p];
+            __nv_bfloat16 h, mm, l;
+            split3d(v, h, mm, l);
+            const uint32_t o = tc::kmajor_off(row, jj, jw);
+            *reinterpret_cast<__nv_bfloat16 *>(blk + co + o) = row < R ? h : mm;
+            *reinterpret_cast<__nv_bfloat16 *>(blk + co + tt + o) = row < R ? __float2bfloat16_rn(0.f) : l;
+        }
+        co += 2 * tt;
+    }
+}
+
 static exotx_status tc_tables(exotx_plan p, TcTables **out) {
     if (p->tc) { *out = p->tc; return EXOTX_OK; }
     if (p->nlath > 128) return EXOTX_BAD_DIM;  // inverse M tile = 128 latitude pairs
@@ -226,6 +260,27 @@ static exotx_status tc_tables(exotx_plan p, TcTables **out) {
          cudaMemcpy(T->d_fwd_off, T->fwd_off.data(), sizeof(long long) * ntp1 * 4, cudaMemcpyHostToDevice) ==
              cudaSuccess;
     if (!ok) { delete T; return EXOTX_NO_MEM; }
+    if (ntp1 <= 128) {
+        // every parity has at most 64 modes: the stacked-split forward tables
+        T->fwd3_off.assign(ntp1 * 8, 0);
+        long long o3 = 0;
+        for (int m = 0; m < ntp1; m++)
+            for (int t = 0; t < 4; t++)
+                for (int q = 0; q < 2; q++) {
+                    T->fwd3_off[(m * 4 + t) * 2 + q] = o3;
+                    o3 += 8LL * pad8(kpar(ntp1 - m, q)) * T->njc;
+                }
+        T->has3 = cudaMalloc(&T->fwd3, o3) == cudaSuccess &&
+                  cudaMalloc(&T->d_fwd3_off, sizeof(long long) * ntp1 * 8) == cudaSuccess &&
+                  cudaMemcpy(T->d_fwd3_off, T->fwd3_off.data(), sizeof(long long) * ntp1 * 8,
+                             cudaMemcpyHostToDevice) == cudaSuccess;
+        if (!T->has3) { delete T; return EXOTX_NO_MEM; }
+        for (int t = 0; t < 4; t++) {
+            k_build_tc_fwd3<<<dim3(ntp1, 2), 256>>>(p->d_qref, p->d_woff, T->d_fwd3_off, p->nlat, p->nlath, p->ncsp,
+                                                    ntp1, T->njc, t, kFwdRef[t], T->fwd3);
+            note_launch();
+        }
+    }
     for (int t = 0; t < 4; t++) {
         k_build_tc_inv<<<ntp1, 256>>>(p->d_qref, p->d_woff, T->d_inv_off, p->nlat, p->nlath, p->ncsp, ntp1, T->nj8,
                                       t, kInvRef[t], T->inv);
@@ -277,6 +332,38 @@ static int fwd_level(exotx_plan p, const TcTables *T) {
         if (fwd_smem(p->ntp1, T->njc, kFwdNlt[v], kFwdOne[v]) <= TC_SMEM_MAX) return v;
     return -1;
 }
+// the stacked-split forward kernel runs wherever its tables exist and fit
+static bool use_fwd3(const TcTables *T) { return T->has3 && fwd3_smem(T->njc, F3_NLT) <= TC_SMEM_MAX; }
+static exotx_status launch_fwd3(const TcFwd3Launch &P, int njobs, size_t smem, cudaStream_t s) {
+    EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward3<F3_NLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TC_SMEM_MAX));
+    cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
+    k_tc_forward3<F3_NLT><<<njobs, TCT3, smem, s>>>(P);
+    EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
+    return EXOTX_OK;
+}
+static void fwd3_args(TcFwd3Args &A, exotx_plan p, const TcTables *T, int L, const float2 *W, long long nrows,
+                      float *spout) {
+    A.tab = T->fwd3; A.off = T->d_fwd3_off; A.woff = p->d_woff; A.W = W; A.nrows = nrows;
+    A.filt = p->d_fg32; A.spout = spout;
+    A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.njc = T->njc; A.ntp1 = p->ntp1; A.nrsp = 2 * p->ncsp;
+}
+// stacked-split forward jobs of one instance range: (m, inst | seg << 16, l0, nl | parity << 8),
+// with a cost estimate (modes x latitude pairs) for ordering
+static void fwd3_jobs(exotx_plan p, const TcTables *T, int L, int ninst, int seg,
+                      std::vector<std::pair<long long, int4>> &v) {
+    for (int m = 0; m < p->ntp1; m++)
+        for (int q = 0; q < 2; q++) {
+            const int Kq = kpar(p->ntp1 - m, q);
+            if (!Kq) continue;
+            const long long cost = (long long)pad8(Kq) * T->njc;
+            for (int i = 0; i < ninst; i++)
+                for (int l0 = 0; l0 < L; l0 += F3_NLT)
+                    v.push_back({cost, make_int4(m, i | (seg << 16), l0, std::min(F3_NLT, L - l0) | (q << 8))});
+        }
+}
+
 static exotx_status launch_fwd(const TcFwdLaunch &P, int level, int njobs, size_t smem, cudaStream_t s) {
     cudaEvent_t ev = nullptr;
     if (kFwdNlt[level] == 4) {
@@ -307,6 +394,18 @@ static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst
             for (int c = 0; c < n2; c += INV_NC_UV) v.push_back(make_int4(m, 2, c, std::min(INV_NC_UV, n2 - c)));
         } else {
             // slabs of nlt levels of one instance; the level-independent gvpp rides with slab 0
+            if (use_fwd3(T)) {
+                if (m == 0) {
+                    std::vector<std::pair<long long, int4>> w;
+                    fwd3_jobs(p, T, L, ninst, 0, w);
+                    std::stable_sort(w.begin(), w.end(), [](const std::pair<long long, int4> &x,
+                                                            const std::pair<long long, int4> &y) {
+                        return x.first > y.first;
+                    });
+                    for (auto &e : w) v.push_back(e.second);
+                }
+                continue;
+            }
             const int lv = fwd_level(p, T), nlt = lv < 0 ? 2 : kFwdNlt[lv];
             for (int i = 0; i < ninst; i++)
                 for (int l0 = 0; l0 < L; l0 += nlt)
@@ -380,9 +479,10 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
     const int4 *jobs;
     int njobs;
     EXOTX_TRY(tc_jobs(p, T, 1, L, chunk, &jobs, &njobs));
+    const bool v3 = use_fwd3(T);
     const int lv = fwd_level(p, T);
-    if (lv < 0) return EXOTX_BAD_DIM;
-    const size_t smem = fwd_smem(p->ntp1, T->njc, kFwdNlt[lv], kFwdOne[lv]);
+    if (!v3 && lv < 0) return EXOTX_BAD_DIM;
+    const size_t smem = v3 ? fwd3_smem(T->njc, F3_NLT) : fwd_smem(p->ntp1, T->njc, kFwdNlt[lv], kFwdOne[lv]);
     for (int i0 = 0; i0 < ninst; i0 += chunk) {
         const int ni = std::min(chunk, ninst - i0);
         const int4 *jl = jobs;
@@ -391,6 +491,14 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
         const long long nrows = (long long)ni * nfi * p->nlat;
         EXOTX_TRY(fft_forward_l<float>(gpin + (size_t)i0 * nfi * nhor, (float *)p->d_work, p->nlon, nrows, p->ntp1,
                                        1, nrows, s));
+        if (v3) {
+            TcFwd3Launch P3;
+            P3.jobs = jl;
+            P3.nprod = 6;
+            fwd3_args(P3.seg[0], p, T, L, (const float2 *)p->d_work, nrows, spout + (size_t)i0 * (4 * L + 1) * nrsp);
+            EXOTX_TRY(launch_fwd3(P3, nj, smem, s));
+            continue;
+        }
         TcFwdLaunch P;
         P.jobs = jl;
         P.nprod = 6;
@@ -416,10 +524,12 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
     if (nseg < 1 || nseg > TC_MAXSEG) return EXOTX_BAD_ARG;
     std::vector<std::pair<long long, int4>> v;
     size_t smax = 0;
-    int lv = 0;  // forward variant shared by every segment of the launch
+    int lv = 0;       // forward variant shared by every segment of the launch
+    bool v3 = true;   // stacked-split forward kernel when every segment has its tables
     for (int sgi = 0; sgi < nseg && dir == 1; sgi++) {
         TcTables *T;
         EXOTX_TRY(tc_tables(segs[sgi].p, &T));
+        v3 = v3 && use_fwd3(T);
         const int l = fwd_level(segs[sgi].p, T);
         if (l < 0) return EXOTX_BAD_DIM;
         lv = std::max(lv, l);
@@ -447,6 +557,9 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
                 for (int c = 0; c < n2; c += b)
                     v.push_back({2 * kw * b, make_int4(m, 2 | (sgi << 2), c, std::min(b, n2 - c))});
             }
+        } else if (v3) {
+            smax = std::max(smax, fwd3_smem(T->njc, F3_NLT));
+            fwd3_jobs(p, T, L, ni, sgi, v);
         } else {
             const int nlt = kFwdNlt[lv];
             smax = std::max(smax, fwd_smem(p->ntp1, T->njc, nlt, kFwdOne[lv]));
@@ -508,12 +621,27 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
         P.jobs = d_jobs;
         P.nprod = nprod;
         int lv = 0;
+        bool v3 = true;
         for (int i = 0; i < nseg; i++) {
             TcTables *T;
             EXOTX_TRY(tc_tables(segs[i].p, &T));
+            v3 = v3 && use_fwd3(T);
             const int l = fwd_level(segs[i].p, T);
             if (l < 0) return EXOTX_BAD_DIM;
             lv = std::max(lv, l);
+        }
+        if (v3) {
+            TcFwd3Launch P3;
+            P3.jobs = d_jobs;
+            P3.nprod = nprod;
+            for (int i = 0; i < nseg; i++) {
+                const EnsSeg &g = segs[i];
+                TcTables *T;
+                EXOTX_TRY(tc_tables(g.p, &T));
+                fwd3_args(P3.seg[i], g.p, T, g.L, (const float2 *)g.W,
+                          (long long)g.ninst * (9 * g.L + 1) * g.p->nlat, g.spout);
+            }
+            return launch_fwd3(P3, njobs, smem, s);
         }
         P.onebuf = kFwdOne[lv];
         for (int i = 0; i < nseg; i++) {

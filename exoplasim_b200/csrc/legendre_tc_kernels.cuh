@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(TCT2) k_tc_inverse(const __grid_constant__ TcI
         if (!ok) atomicExch(&g_tc_error, 1);
     }
     __syncthreads();
-    ok = tc::mbar_wait(bar_done, 0);  // single-phase barrier, bounded
+    ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, 0));  // warp-uniform for the .sync.aligned TMEM loads  // single-phase barrier, bounded
     if (!ok && lane == 0) atomicExch(&g_tc_error, 2);
     tc::fence_after_sync();
     if (ok) {
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
         if (!ok) atomicExch(&g_tc_error, 3);
     }
     __syncthreads();
-    ok = tc::mbar_wait(bar_done, 0);
+    ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, 0));  // warp-uniform for the .sync.aligned TMEM loads
     if (!ok && lane == 0) atomicExch(&g_tc_error, 4);
     tc::fence_after_sync();
     // epilogue: warp half h drains parity h; TMEM lane = mode index k'
@@ -605,4 +605,302 @@ static size_t fwd_smem(int K, int njc, int nlt, bool onebuf) {
     size_t d = 0;
     for (int t = 0; t < 4; t++) d += 2 * 3 * (size_t)fwd_ncp_rt(nlt, t) * njc * 2;
     return tblk + 128 * 32 * 2 + d + 80;
+}
+
+// ------------------------------------------------------------ forward, stacked splits
+// Variant for NTRU+1 <= 128 (every parity has at most 64 modes): one parity per
+// job, and the table's split terms stacked in the M=128 tile so that two MMAs
+// per K-chunk cover all six split products.  Per (m, table, parity) and
+// latitude chunk the table holds two 2R-row K-major tiles:
+//   S01 = [a0 of modes 0..R-1 ; a1 of modes 0..R-1],   S2 = [0 ; a2]
+// and the data of the table's columns is staged as [b0 | b1 | b2] (N-adjacent):
+//   MMA1  [X0|X1|X2] (+)= S01 x [b0|b1|b2]   (N = 3 ncp)
+//   MMA2   X0        +=  S2  x  b0           (N = ncp)
+// Row k' < R of X0 is the hi*hi chain alone; every other entry of rows k' and
+// R+k' is a correction product.  The mode's value is the sum of both rows'
+// three blocks; the rows meet in shared memory in the epilogue.
+struct TcFwd3Args {
+    const unsigned char *tab;
+    const long long *off;   // [(m*4 + t)*2 + p]
+    const int *woff;
+    const float2 *W;
+    long long nrows;
+    const float *filt;
+    float *spout;
+    int L, nlat, nlath, njc, ntp1, nrsp;
+};
+struct TcFwd3Launch {
+    TcFwd3Args seg[TC_MAXSEG];
+    const int4 *jobs;       // (m, inst | seg << 16, first level, levels | parity << 8)
+    int nprod;              // 6: all six products; 3: a0b0, a0b1, a1b0 (and a1b1)
+};
+template <int NLT> __host__ __device__ constexpr int f3_colbase(int t) {
+    return t == 0 ? 0 : f3_colbase<NLT>(t - 1) + 3 * fwd_ncp<NLT>(t - 1);
+}
+constexpr int F3_NLT = 5;   // levels per job: 3 x (32 + 48 + 48 + 16) = 432 TMEM columns
+
+// partial outputs of one table's columns: d, t, z, q per level (re, im) and spf
+template <int NLT>
+__device__ __forceinline__ void f3_combine(int t, int c, float v, float (*o)[4][2], float *ov) {
+    const int q = c >> 1, ri = c & 1;
+    if (t == 0) {
+        if (q == 2 * NLT) { ov[ri] += v; return; }
+        if (q >= 2 * NLT) return;
+        const int fi = q / NLT, li = q - fi * NLT;
+        o[li][fi == 0 ? 1 : 3][ri] += v;             // tn -> t, qn -> q
+    } else if (t == 1) {
+        if (q >= 4 * NLT) return;
+        const int fi = q / NLT, li = q - fi * NLT;
+        if (fi == 0) o[li][0][ri] -= v;              // fv -> d (-)
+        else if (fi == 1) o[li][1][ri] += v;         // vt -> t
+        else if (fi == 2) o[li][2][ri] += v;         // fu -> z
+        else o[li][3][ri] += v;                      // vq -> q
+    } else if (t == 2) {
+        if (q >= 4 * NLT) return;
+        const int fi = q / NLT, li = q - fi * NLT;
+        // i*(a + ib) = -b + ia: the real column feeds im, the imaginary feeds re
+        const float sgn = (fi == 0 || fi == 2) ? 1.f : -1.f;   // +i for fu, fv; -i for ut, uq
+        const int out = fi == 0 ? 0 : fi == 1 ? 1 : fi == 2 ? 2 : 3;
+        if (ri == 0) o[li][out][1] += sgn * v;
+        else o[li][out][0] -= sgn * v;
+    } else {
+        if (q >= NLT) return;
+        o[q][0][ri] += v;                            // ke -> d
+    }
+}
+
+// 16 warps: warp 0 issues copies and MMAs, warps 1-15 stage operands (the
+// staging loads are latency-bound, so more warps keep more of them in flight),
+// warps 0-3 drain TMEM
+constexpr int TCT3 = 512;
+
+template <int NLT>
+__global__ void __launch_bounds__(TCT3) k_tc_forward3(const __grid_constant__ TcFwd3Launch P) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const int4 jb = P.jobs[blockIdx.x];
+    const TcFwd3Args &A = P.seg[jb.y >> 16];
+    const int nprod = P.nprod;
+    const int m = jb.x, inst = jb.y & 0xffff, l0 = jb.z, nl = jb.w & 0xff, p = jb.w >> 8;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3;
+    const int K = A.ntp1 - m;
+    const int Kq = kpar(K, p), R = pad8(Kq);
+    const int njc = A.njc, L = A.L, nlat = A.nlat;
+    const bool with_vpp = (l0 == 0);
+    const uint32_t tbytes = (uint32_t)8 * R * njc;   // one (m, table, parity) block
+    const uint32_t tbuf = (uint32_t)8 * 64 * njc;    // buffer for the widest block
+    unsigned char *tabb[2] = {sm, sm + tbuf};
+    // rows >= 2R of the M=128 tiles read past a block (their TMEM lanes are unused)
+    unsigned char *dat = sm + 2 * tbuf + 128 * 32 * 2;
+    size_t doffs[4], dbytes = 0;
+    for (int t = 0; t < 4; t++) { doffs[t] = dbytes; dbytes += 3 * (size_t)fwd_ncp<NLT>(t) * njc * 2; }
+    unsigned char *tail = dat + dbytes;
+    uint64_t *bars = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
+    uint64_t *bar_tma = bars;       // [2] table buffer b landed
+    uint64_t *bar_mma = bars + 2;   // [2] MMAs reading table buffer b completed
+    uint64_t *bar_done = bars + 4;
+    uint64_t *bar_stage = bars + 5; // [4] operands of table t staged (warps 1-15 arrive)
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 9);
+    if (warp == 0) tc::tmem_alloc(slot, 512);
+    if (tid == 0) {
+        for (int i = 0; i < 5; i++) tc::mbar_init(bars + i, 1);
+        for (int t = 0; t < 4; t++) tc::mbar_init(bar_stage + t, TCT3 - 32);
+        tc::mbar_fence_init();
+        for (int t = 0; t < 2; t++) {
+            tc::mbar_arrive_expect_tx(bar_tma + t, tbytes);
+            tc::bulk_g2s(tabb[t], A.tab + A.off[(m * 4 + t) * 2 + p], tbytes, bar_tma + t);
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();  // barriers initialised, TMEM address published
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    bool ok = true;
+    // warps 1-15 stage the folded columns each table needs for this parity,
+    // table by table, while warp 0 issues the MMAs of every table already
+    // staged.  P-type tables (qc, qm, qq) take N+S on even n-m and N-S on odd,
+    // Q-type (qe) the reverse.
+    const int ng = njc >> 3;
+    for (int t = 0; t < 4 && warp != 0; t++) {
+        const int nf = c_fwd_nf[t];
+        const int ncp = fwd_ncp<NLT>(t), npair = ncp >> 1;
+        const int nreal = nf * NLT + ((t == 0) ? 1 : 0);
+        const bool diff = (t != 1) ? (p == 1) : (p == 0);
+        const uint32_t dt = (uint32_t)ncp * njc * 2;
+        unsigned char *bt = dat + doffs[t];
+        const int nunit = npair * ng;
+        for (int u = tid - 32; u < nunit; u += TCT3 - 32) {
+            const int q = u % npair, g = u / npair;
+            long long rb = -1;
+            if (q < nreal) {
+                if (t == 0 && q == nf * NLT) { if (with_vpp) rb = fwd_row(L, inst, 7, 0); }
+                else {
+                    const int fi = q / NLT, li = q - fi * NLT;
+                    if (li < nl) rb = fwd_row(L, inst, c_fwd_fields[t][fi], l0 + li);
+                }
+            }
+            const int j0 = 8 * g;
+            float xr[8], xi[8];
+            float2 vn[8], vs[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) vn[e] = vs[e] = make_float2(0.f, 0.f);
+            if (rb >= 0) {
+                const float2 *wr = A.W + (size_t)m * A.nrows + (size_t)rb * nlat;
+                if (j0 + 8 <= A.nlath) {
+                    // rows j0..j0+7 north, and nlat-8-j0..nlat-1-j0 south (reversed)
+                    const float4 *pn = reinterpret_cast<const float4 *>(wr + j0);
+                    const float4 *ps = reinterpret_cast<const float4 *>(wr + nlat - 8 - j0);
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float4 x = __ldg(pn + i), y = __ldg(ps + i);
+                        vn[2 * i] = make_float2(x.x, x.y);
+                        vn[2 * i + 1] = make_float2(x.z, x.w);
+                        vs[7 - 2 * i] = make_float2(y.x, y.y);
+                        vs[6 - 2 * i] = make_float2(y.z, y.w);
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 8; e++)
+                        if (j0 + e < A.nlath) {
+                            vn[e] = __ldg(wr + j0 + e);
+                            vs[e] = __ldg(wr + nlat - 1 - j0 - e);
+                        }
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+                xr[e] = diff ? vn[e].x - vs[e].x : vn[e].x + vs[e].x;
+                xi[e] = diff ? vn[e].y - vs[e].y : vn[e].y + vs[e].y;
+            }
+            const uint32_t o = tc::kmajor_off(2 * q, j0, njc);
+            uint4 h, mm, l;
+            tc::split3x8(xr, h, mm, l);
+            st_shared16(bt + o, h); st_shared16(bt + dt + o, mm); st_shared16(bt + 2 * dt + o, l);
+            tc::split3x8(xi, h, mm, l);
+            st_shared16(bt + o + 16, h); st_shared16(bt + dt + o + 16, mm); st_shared16(bt + 2 * dt + o + 16, l);
+        }
+        tc::fence_proxy_async();  // these stores feed the tensor cores
+        tc::mbar_arrive(bar_stage + t);
+    }
+    if (tid == 0) {
+        const uint32_t sbo_b = (uint32_t)(njc / 8) * 128;
+        for (int t = 0; t < 4 && ok; t++) {
+            const int b = t & 1;
+            ok = tc::mbar_wait(bar_stage + t, 0) && tc::mbar_wait(bar_tma + b, (t >> 1) & 1);
+            if (!ok) break;
+            tc::fence_after_sync();
+            const int ncp = fwd_ncp<NLT>(t);
+            const uint32_t idesc1 = tc::idesc_bf16(128, (nprod == 6 ? 3 : 2) * ncp);
+            const uint32_t idesc2 = tc::idesc_bf16(128, ncp);
+            const uint32_t X = tmem + (uint32_t)f3_colbase<NLT>(t);
+            const uint64_t db = tc::smem_desc(dat + doffs[t], 128, sbo_b);
+            uint32_t jo = 0;
+            for (int j0 = 0; j0 < njc; j0 += 32) {
+                const int jw = njc - j0 < 32 ? njc - j0 : 32;
+                const uint32_t tt = (uint32_t)2 * R * jw * 2;   // one stacked tile
+                const uint64_t da1 = tc::smem_desc(tabb[b] + jo, 128, (uint32_t)(jw / 8) * 128);
+                const uint64_t da2 = tc::desc_add(da1, tt);
+                for (int kc = 0; kc < jw / 16; kc++) {
+                    const uint64_t dbk = tc::desc_add(db, (j0 / 8) * 128 + kc * 256);
+                    tc::mma_bf16(X, tc::desc_add(da1, kc * 256), dbk, idesc1, j0 > 0 || kc > 0);
+                    if (nprod == 6) tc::mma_bf16(X, tc::desc_add(da2, kc * 256), dbk, idesc2, true);
+                }
+                jo += 2 * tt;
+            }
+            if (t <= 1) tc::mma_commit(bar_mma + b);
+            // refill the other buffer with table t+1 once table t-1's MMAs have read it
+            if (t >= 1 && t + 1 < 4) {
+                const int bn = (t + 1) & 1;
+                ok = tc::mbar_wait(bar_mma + bn, 0);
+                if (!ok) break;
+                tc::mbar_arrive_expect_tx(bar_tma + bn, tbytes);
+                tc::bulk_g2s(tabb[bn], A.tab + A.off[(m * 4 + t + 1) * 2 + p], tbytes, bar_tma + bn);
+            }
+        }
+        if (ok) tc::mma_commit(bar_done);
+        if (!ok) atomicExch(&g_tc_error, 5);
+    }
+    __syncthreads();
+    ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, 0));  // warp-uniform for the .sync.aligned TMEM loads
+    if (!ok && lane == 0) atomicExch(&g_tc_error, 6);
+    tc::fence_after_sync();
+    // epilogue (warps 0-3, one per TMEM lane quarter): row r holds mode r (r < R)
+    // or corrections of mode r - R (R <= r < 2R); rows >= R hand their partial
+    // outputs to rows < R through shared memory
+    constexpr int NO = NLT * 8 + 2;
+    float *E = reinterpret_cast<float *>(dat);   // [64][NO]; the operands are dead now
+    const int r = quarter * 32 + lane;
+    const bool drain = ok && warp < 4;            // warp-uniform (ok is)
+    float o[NLT][4][2], ov[2] = {0.f, 0.f};
+#pragma unroll
+    for (int li = 0; li < NLT; li++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[li][k][0] = o[li][k][1] = 0.f;
+    if (drain) {
+        const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int ncp = fwd_ncp<NLT>(t);
+            const uint32_t X = tmem + lane_addr + (uint32_t)f3_colbase<NLT>(t);
+#pragma unroll
+            for (int c0 = 0; c0 < 48; c0 += 16) {
+                if (c0 >= ncp) break;
+                uint32_t x0[16], x1[16], x2[16];
+                tc::tmem_ld16_nw(X + c0, x0);
+                tc::tmem_ld16_nw(X + ncp + c0, x1);
+                if (nprod == 6) tc::tmem_ld16_nw(X + 2 * ncp + c0, x2);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    float v = __uint_as_float(x0[i]) + __uint_as_float(x1[i]);
+                    if (nprod == 6) v += __uint_as_float(x2[i]);
+                    f3_combine<NLT>(t, c0 + i, v, o, ov);
+                }
+            }
+        }
+        if (r >= R && r < 2 * R) {
+            float *e = E + (size_t)(r - R) * NO;
+#pragma unroll
+            for (int li = 0; li < NLT; li++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    e[(li * 4 + k) * 2] = o[li][k][0];
+                    e[(li * 4 + k) * 2 + 1] = o[li][k][1];
+                }
+            e[NLT * 8] = ov[0];
+            e[NLT * 8 + 1] = ov[1];
+        }
+    }
+    __syncthreads();
+    if (drain && r < Kq) {
+        const float *e = E + (size_t)r * NO;
+        const int k = 2 * r + p;  // n - m
+        const float fl = A.filt[m + k];
+        const size_t wo = 2 * (size_t)(A.woff[m] + k);
+        const int nfo = 4 * L + 1;
+#pragma unroll
+        for (int li = 0; li < NLT; li++) {
+            if (li >= nl) break;
+            const int l = l0 + li;
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                float2 *dst = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + kk * L + l) * A.nrsp + wo);
+                *dst = make_float2((o[li][kk][0] + e[(li * 4 + kk) * 2]) * fl,
+                                   (o[li][kk][1] + e[(li * 4 + kk) * 2 + 1]) * fl);
+            }
+        }
+        if (with_vpp) {
+            float2 *sp = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + 4 * L) * A.nrsp + wo);
+            *sp = make_float2((ov[0] + e[NLT * 8]) * fl, (ov[1] + e[NLT * 8 + 1]) * fl);
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 512);
+}
+
+// shared memory of a stacked-split forward job (tables of at most 64 modes per parity)
+static size_t fwd3_smem(int njc, int nlt) {
+    size_t d = 0;
+    for (int t = 0; t < 4; t++) d += 3 * (size_t)fwd_ncp_rt(nlt, t) * njc * 2;
+    return 2 * (size_t)8 * 64 * njc + 128 * 32 * 2 + d + 128;
 }

@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
                 }
             }
             __syncthreads();
-            const bool mok = tc::mbar_wait(bar_mma, phase & 1);
+            const bool mok = __all_sync(0xffffffffu, tc::mbar_wait(bar_mma, phase & 1));
             phase++;
             if (!mok) { if (lane == 0) atomicExch(&g_surr_error, 2); ok = false; }
             tc::fence_after_sync();
