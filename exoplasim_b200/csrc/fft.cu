@@ -18,7 +18,8 @@
 
 namespace exotx {
 
-template <typename T> struct cpx { T x, y; };
+// complex value; every complex array here starts on a multiple of its size
+template <typename T> struct __align__(2 * sizeof(T)) cpx { T x, y; };
 template <typename T> __device__ __forceinline__ cpx<T> cmul(cpx<T> a, cpx<T> b) {
     return cpx<T>{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
 }
@@ -252,16 +253,23 @@ __host__ __device__ constexpr int radix_at(int h, int idx) {
     return 8;
 }
 
+// Rows in shared memory keep 2 spare complex slots after every 16 elements:
+// the passes' strided reads and writes then spread over the banks (about half
+// the wavefronts of a dense row), and even indices stay 16-byte aligned for the
+// vector copies.  H is a multiple of 16 for every specialised length.
+__host__ __device__ constexpr int fpad(int j) { return j + 2 * (j >> 4); }
+template <int H> __host__ __device__ constexpr int fpad_row() { return H + 2 * (H / 16); }
+
 template <typename T, int S, int H, int ROWS, int R, int NS>
 __device__ __forceinline__ void pass_ct(const cpx<T> *src, cpx<T> *dst, const cpx<T> *tw) {
-    constexpr int NQ = H / R, STEP = H / (NS * R), NIT = ROWS * NQ;
+    constexpr int NQ = H / R, STEP = H / (NS * R), NIT = ROWS * NQ, HP = fpad_row<H>();
     for (int it = threadIdx.x; it < NIT; it += blockDim.x) {
         const int row = it / NQ, t = it - row * NQ, k = t % NS;
-        const cpx<T> *s = src + row * H;
-        cpx<T> *d = dst + row * H;
+        const cpx<T> *s = src + row * HP;
+        cpx<T> *d = dst + row * HP;
         cpx<T> v[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) v[r] = s[t + r * NQ];
+        for (int r = 0; r < R; r++) v[r] = s[fpad(t + r * NQ)];
 #pragma unroll
         for (int r = 1; r < R; r++) {
             cpx<T> w = tw[r * k * STEP];
@@ -271,7 +279,7 @@ __device__ __forceinline__ void pass_ct(const cpx<T> *src, cpx<T> *dst, const cp
         dftR<T, S, R>(v);
         const int base = (t / NS) * NS * R + k;
 #pragma unroll
-        for (int r = 0; r < R; r++) d[base + r * NS] = v[r];
+        for (int r = 0; r < R; r++) d[fpad(base + r * NS)] = v[r];
     }
 }
 
@@ -295,11 +303,11 @@ template <typename T, int N, int ROWS>
 __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long lot, int kf, long long f_rs,
                                                  long long f_ms, const cpx<T> *__restrict__ wtab,
                                                  const cpx<T> *__restrict__ rtab, long long blk) {
-    constexpr int H = N / 2;
+    constexpr int H = N / 2, HP = fpad_row<H>();
     extern __shared__ __align__(16) unsigned char smraw[];
     cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
-    cpx<T> *b1 = b0 + ROWS * H;
-    cpx<T> *tw = b1 + ROWS * H;
+    cpx<T> *b1 = b0 + ROWS * HP;
+    cpx<T> *tw = b1 + ROWS * HP;
     cpx<T> *rt = tw + H;
     const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
@@ -308,14 +316,16 @@ __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long l
     {
         // rows are contiguous: two complex (= 4 reals for FP32) per vector load
         using V = typename vec2<T>::t;
-        constexpr int PER = (int)(sizeof(V) / sizeof(T));
+        constexpr int PER = (int)(sizeof(V) / sizeof(T)), CPV = PER / 2;
         const V *src = reinterpret_cast<const V *>(gp + row0 * N);
-        V *dst = reinterpret_cast<V *>(b0);
         const int nv = rows * N / PER;
-        for (int i = threadIdx.x; i < nv; i += blockDim.x) dst[i] = src[i];
-        if (rows < ROWS) {
-            T *raw = reinterpret_cast<T *>(b0);
-            for (int i = rows * N + threadIdx.x; i < ROWS * N; i += blockDim.x) raw[i] = 0;
+        for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+            const int cj = i * CPV, row = cj / H, j = cj - row * H;
+            *reinterpret_cast<V *>(b0 + row * HP + fpad(j)) = src[i];
+        }
+        for (int cj = rows * H + threadIdx.x; cj < ROWS * H; cj += blockDim.x) {
+            const int row = cj / H, j = cj - row * H;
+            b0[row * HP + fpad(j)] = cpx<T>{0, 0};
         }
     }
     __syncthreads();
@@ -324,13 +334,13 @@ __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long l
     for (int it = threadIdx.x; it < ROWS * kf; it += blockDim.x) {
         const int row = it % ROWS, k = it / ROWS;
         if (row >= rows) continue;
-        const cpx<T> *z = Z + row * H;
+        const cpx<T> *z = Z + row * HP;
         T re, im;
         if (k == 0) {
             re = (z[0].x + z[0].y) * scale;
             im = 0;
         } else {
-            cpx<T> a = z[k], b = z[H - k];
+            cpx<T> a = z[fpad(k)], b = z[fpad(H - k)];
             cpx<T> E{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
             cpx<T> O{(T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x)};
             cpx<T> wo = cmul(rt[k], O);
@@ -338,8 +348,7 @@ __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long l
             im = (E.y + wo.y) * scale;
         }
         const size_t o = 2 * ((row0 + row) * f_rs + (long long)k * f_ms);
-        fc[o] = re;
-        fc[o + 1] = im;
+        *reinterpret_cast<cpx<T> *>(fc + o) = cpx<T>{re, im};
     }
 }
 
@@ -347,11 +356,11 @@ template <typename T, int N, int ROWS>
 __device__ __forceinline__ void rfft_inv_ct_body(const T *fc, T *gp, long long lot, int kf, long long f_rs,
                                                  long long f_ms, const cpx<T> *__restrict__ wtab,
                                                  const cpx<T> *__restrict__ rtab, long long blk) {
-    constexpr int H = N / 2;
+    constexpr int H = N / 2, HP = fpad_row<H>();
     extern __shared__ __align__(16) unsigned char smraw[];
     cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
-    cpx<T> *b1 = b0 + ROWS * H;
-    cpx<T> *tw = b1 + ROWS * H;
+    cpx<T> *b1 = b0 + ROWS * HP;
+    cpx<T> *tw = b1 + ROWS * HP;
     cpx<T> *rt = tw + H;
     const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
@@ -363,32 +372,34 @@ __device__ __forceinline__ void rfft_inv_ct_body(const T *fc, T *gp, long long l
         cpx<T> c{0, 0};
         if (k < kf && row < rows) {
             const size_t o = 2 * ((row0 + row) * f_rs + (long long)k * f_ms);
-            c.x = fc[o];
-            c.y = (k == 0) ? (T)0 : fc[o + 1];
+            c = *reinterpret_cast<const cpx<T> *>(fc + o);
+            if (k == 0) c.y = 0;
         }
-        b1[row * H + k] = c;
+        b1[row * HP + fpad(k)] = c;
     }
     __syncthreads();
     for (int it = threadIdx.x; it < ROWS * H; it += blockDim.x) {
         const int row = it / H, k = it - row * H;
-        const cpx<T> *c = b1 + row * H;
-        cpx<T> a = c[k];
-        cpx<T> b = (k == 0) ? cpx<T>{0, 0} : c[H - k];
+        const cpx<T> *c = b1 + row * HP;
+        cpx<T> a = c[fpad(k)];
+        cpx<T> b = (k == 0) ? cpx<T>{0, 0} : c[fpad(H - k)];
         cpx<T> E{a.x + b.x, a.y - b.y};
         cpx<T> D{a.x - b.x, a.y + b.y};
         cpx<T> w = rt[k];
         w.y = -w.y;
         cpx<T> O = cmul(D, w);
-        b0[row * H + k] = cpx<T>{E.x - O.y, E.y + O.x};
+        b0[row * HP + fpad(k)] = cpx<T>{E.x - O.y, E.y + O.x};
     }
     __syncthreads();
     const cpx<T> *z = passes_ct<T, +1, H, ROWS, 0, 1>(b0, b1, tw);
     using V = typename vec2<T>::t;
-    constexpr int PER = (int)(sizeof(V) / sizeof(T));
-    const V *src = reinterpret_cast<const V *>(z);
+    constexpr int PER = (int)(sizeof(V) / sizeof(T)), CPV = PER / 2;
     V *dst = reinterpret_cast<V *>(gp + row0 * N);
     const int nv = rows * N / PER;
-    for (int i = threadIdx.x; i < nv; i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+        const int cj = i * CPV, row = cj / H, j = cj - row * H;
+        dst[i] = *reinterpret_cast<const V *>(z + row * HP + fpad(j));
+    }
 }
 
 template <typename T, int N, int ROWS>
@@ -473,7 +484,8 @@ exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s) 
         a.r = reinterpret_cast<const cpx<float> *>(t->r32);
         a.block0 = blocks;
         blocks += (int)((g.lot + rows - 1) / rows);
-        smem = std::max(smem, (2 * (size_t)rows * (g.n / 2) + g.n / 2 + g.n / 2 + 1) * sizeof(cpx<float>));
+        const int hp = g.n / 2 + 2 * (g.n / 32);   // padded row, as fpad_row
+        smem = std::max(smem, (2 * (size_t)rows * hp + g.n / 2 + g.n / 2 + 1) * sizeof(cpx<float>));
     }
     if (blocks == 0) return EXOTX_OK;
     const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
@@ -495,7 +507,7 @@ template <typename T, int N>
 static exotx_status launch_ct(bool fwd, const T *in, T *out, long long lot, int kf, long long f_rs, long long f_ms,
                               const cpx<T> *w, const cpx<T> *r, cudaStream_t s) {
     constexpr int ROWS = ct_rows<T>(N);
-    const size_t smem = (2 * ROWS * (N / 2) + N / 2 + N / 2 + 1) * sizeof(cpx<T>);
+    const size_t smem = (2 * ROWS * fpad_row<N / 2>() + N / 2 + N / 2 + 1) * sizeof(cpx<T>);
     const long long nb = (lot + ROWS - 1) / ROWS;
     const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
     if (fwd) {
