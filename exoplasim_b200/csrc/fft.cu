@@ -270,11 +270,13 @@ __device__ __forceinline__ void pass_ct(const cpx<T> *src, cpx<T> *dst, const cp
         cpx<T> v[R];
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = s[fpad(t + r * NQ)];
+        if constexpr (NS > 1) {  // the first pass has unit twiddles only
 #pragma unroll
-        for (int r = 1; r < R; r++) {
-            cpx<T> w = tw[r * k * STEP];
-            if (S > 0) w.y = -w.y;
-            v[r] = cmul(v[r], w);
+            for (int r = 1; r < R; r++) {
+                cpx<T> w = tw[r * k * STEP];
+                if (S > 0) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
         }
         dftR<T, S, R>(v);
         const int base = (t / NS) * NS * R + k;
