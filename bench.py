@@ -192,18 +192,18 @@ def relerr_fields(a, b):
 
 def run_ours(a, rank, world, local_rank):
     import torch
-    import torch.distributed as dist
 
     from exoplasim_b200 import radiation as R
     from exoplasim_b200 import synthetic as S
+    from exoplasim_b200.replicas import barrier, max_over_ranks, unit_seed
     from exoplasim_b200.transforms import Plan, kernel_time, kernel_timing, launch_count
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     B = a.batch
     plan = Plan(NLAT)
-    spin64 = torch.as_tensor(S.transform_state(plan.ntru, NLEV, seed=3 + rank, kind="steep"), device=dev)
-    gin64 = torch.as_tensor(S.grid_tendencies(NLAT, NLEV, seed=4 + rank), device=dev)
+    spin64 = torch.as_tensor(S.transform_state(plan.ntru, NLEV, seed=unit_seed(3, rank), kind="steep"), device=dev)
+    gin64 = torch.as_tensor(S.grid_tendencies(NLAT, NLEV, seed=unit_seed(4, rank)), device=dev)
 
     def make(dtype):
         pr = "fp64" if dtype == torch.float64 else "fp32"
@@ -220,10 +220,6 @@ def run_ours(a, rank, world, local_rank):
             plan.inverse_set_batch(spin, NLEV, precision=prec, out=gout)
             plan.forward_set_batch(gin, NLEV, precision=prec, out=sout)
         return f
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
 
     def time_graph(fn, steps, warmup):
         fn()  # eager call: allocates work buffers and FFT tables outside capture
@@ -254,13 +250,6 @@ def run_ours(a, rank, world, local_rank):
         ms = e0.elapsed_time(e1)
         del g
         return ms, per_step
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     results = {}
     # FP64 reference outputs for the error columns
@@ -371,7 +360,7 @@ def run_ours(a, rank, world, local_rank):
     del bufs, h_spin, h_gin, h_gout, h_sout
 
     # radiation column pass: 8192 columns at L20 (T42 grid), plain kernel
-    cols, g = S.radiation_columns(RAD_NLAT, RAD_NLEV, seed=2 + rank)
+    cols, g = S.radiation_columns(RAD_NLAT, RAD_NLEV, seed=unit_seed(2, rank))
     rad = {}
     for rprec, rdt in (() if a.skip_radiation else (("fp64", torch.float64), ("fp32", torch.float32))):
         dev_cols = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=rdt, device=dev) for k, v in cols.items()}
@@ -433,8 +422,9 @@ def run_ours(a, rank, world, local_rank):
         sp_i, gi_i = [], []
         for i, (nlat, L) in enumerate(zip(nl_e, lv_e)):
             ntru = (2 * nlat - 1) // 3
-            sp_i.append(torch.as_tensor(S.transform_state(ntru, L, seed=7 + i, kind="nn1"), device=dev).float())
-            gi_i.append(torch.as_tensor(S.grid_tendencies(nlat, L, seed=500 + i), device=dev).float())
+            spi = S.transform_state(ntru, L, seed=unit_seed(7, rank, i), kind="nn1")
+            sp_i.append(torch.as_tensor(spi, device=dev).float())
+            gi_i.append(torch.as_tensor(S.grid_tendencies(nlat, L, seed=unit_seed(500, rank, i)), device=dev).float())
         spin_e, gin_e = E.pack("spec", sp_i), E.pack("gin", gi_i)
         _, gout_e, _, spout_e = E.buffers()
         choice = E.tune(spin_e, gout_e, gin_e, spout_e, reps=3)
@@ -456,8 +446,7 @@ def run_ours(a, rank, world, local_rank):
                "one_by_one_round_trips_per_s": world * 96 * a.steps / (ms_1 / 1000.0),
                "one_by_one_launches_per_step": nlch_1, "tuned": choice}
         del E, eplans
-    if world > 1:
-        dist.barrier()
+    barrier()
     if rank != 0:
         return
     cpu = None

@@ -156,3 +156,42 @@ def test_radstep_transparent_isothermal_lw(oracle):
     out = oracle.radstep(p, cols["sid"], cols["cola"], cols)
     assert np.all(out["dftd"][0] == 0)
     assert np.allclose(out["dftu"][10], -0.98 * 5.67e-8 * 250.0 ** 4, rtol=1e-12)
+
+
+def test_pyfft_compositions(oracle):
+    """The pyfft restatement (oracle/pyfft_oracle.py): sp2gp against the scipy
+    golden grid times pyfft's sqrt(2), and the identities pyfft's pairs obey
+    for band-limited fields (gp2sp o sp2gp, gpvsp o spvgp with reciprocal
+    radius factors, uv2dv o dv2uv); f2py's Fortran-ordered shapes."""
+    from exoplasim_b200 import synthetic as S
+    from oracle import pyfft_oracle as PO
+    g = np.load(GOLDEN)
+    sp = g["t21_sp"]
+    gp = PO.sp2gp(sp[:, None], 32, 64, 21)
+    assert gp.shape == (64, 32, 1)
+    assert relerr(gp[:, :, 0].T, g["t21_grid"] * PO.SQRT2) < 1e-13
+    assert relerr(PO.gp2sp(gp, 32, 64, 21)[:, 0], sp) < 1e-13
+    rng = np.random.default_rng(7)
+    sd = S.spectral_field(rng, 21, 3, "nn1").T.copy()
+    sz = S.spectral_field(rng, 21, 3, "nn1").T.copy()
+    sd[0:2] = sz[0:2] = 0.0                 # no n=0 divergence or vorticity
+    sid, _ = PO.inigau(32)
+    cs = np.sqrt(1.0 - sid ** 2)
+    gu, gv = PO.spvgp(sd, sz, 6.371e6 / cs, 64, 21)
+    assert gu.shape == gv.shape == (64, 32, 3)
+    d2, z2 = PO.gpvsp(gu, gv, cs / 6.371e6, 21)
+    assert relerr(d2, sd) < 1e-12 and relerr(z2, sz) < 1e-12
+    pu, pv = PO.dv2uv(sd, sz, 32, 64, 21)
+    assert pu.shape == (2, 32, 32, 3)
+    pd, pz = PO.uv2dv(pu, pv, 32, 64, 21)
+    assert pd.shape == (2, 253, 3)
+    assert relerr(pd.transpose(1, 0, 2).reshape(-1, 3), sd) < 1e-12
+    fc = PO.sp3fc(sp[:, None], 32, 64, 21)
+    assert fc.shape == (2, 32, 32, 1)
+    # gp3fc is fftmod's packing of numpy's DFT, scaled by 1/n
+    a = rng.standard_normal((64, 32, 2))
+    c = PO.gp3fc(a)
+    X = np.fft.rfft(a, axis=0) / 64
+    assert relerr(c[2::2], X.real[1:32]) < 1e-14 and relerr(c[3::2], X.imag[1:32]) < 1e-14
+    # the FFT991 variant (pyfft991 for NLAT 192 and 320) agrees with fftmod
+    assert relerr(PO.gp3fc(a, use991=True), c) < 1e-14
