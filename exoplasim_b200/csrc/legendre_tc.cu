@@ -458,7 +458,7 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.nj8 = T->nj8; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
         A.plavor = (float)p->desc.plavor;
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
-        k_tc_inverse<<<nj, TCT2, smem, s>>>(P);
+        k_tc_inverse<<<nj, TCI, smem, s>>>(P);
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
         EXOTX_TRY(fft_inverse_l<float>((const float *)p->d_work, gpout + (size_t)i0 * nfo * nhor, p->nlon, A.nrows,
@@ -613,7 +613,7 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
         }
         EXOTX_CUDA(cudaFuncSetAttribute(k_tc_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
-        k_tc_inverse<<<njobs, TCT2, smem, s>>>(P);
+        k_tc_inverse<<<njobs, TCI, smem, s>>>(P);
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
     } else {

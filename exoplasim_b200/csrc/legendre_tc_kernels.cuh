@@ -1,9 +1,8 @@
 // Tensor-core Legendre kernels (included by legendre_tc.cu).
 //
-// One CTA of 256 threads per job.  Warps w and w+4 share TMEM lane quarter
-// w % 4; in the epilogue the two halves split the work (the inverse by
-// column chunks, the forward by parity).  Thread 0 issues the TMA table
-// copies and the MMAs; everybody stages operands and drains accumulators.
+// One CTA per job.  Thread 0 issues the TMA table copies and the MMAs; the
+// other threads stage operands and drain accumulators.  Warps w, w+4, ...
+// share TMEM lane quarter w % 4.
 #pragma once
 
 constexpr int TCT2 = 256;
@@ -50,13 +49,17 @@ __device__ __forceinline__ const float2 *inv_row(const TcInvArgs &A, int group, 
     return reinterpret_cast<const float2 *>(A.spin + ((size_t)inst * nf + f) * A.nrsp);
 }
 
-__global__ void __launch_bounds__(TCT2) k_tc_inverse(const __grid_constant__ TcInvLaunch P) {
+// 16 warps: all stage operands; thread 0 issues the table copies and MMAs;
+// in the epilogue warp w drains TMEM lane quarter w % 4 for column chunk w / 4
+constexpr int TCI = 512;
+
+__global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcInvLaunch P) {
     extern __shared__ __align__(128) unsigned char sm[];
     const int4 jb = P.jobs[blockIdx.x];
     const TcInvArgs &A = P.seg[jb.y >> 2];
     const int nprod = P.nprod;
     const int m = jb.x, group = jb.y & 3, c0 = jb.z, nc = jb.w;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, half = warp >> 2;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, sub = warp >> 2;
     const int K = A.ntp1 - m;
     const int Kq[2] = {kpar(K, 0), kpar(K, 1)};
     const int Kp[2] = {pad16(Kq[0]), pad16(Kq[1])};
@@ -86,45 +89,57 @@ __global__ void __launch_bounds__(TCT2) k_tc_inverse(const __grid_constant__ TcI
     }
     // stage the spectral columns of both parities.  A unit is one column pair
     // (re, im) and 8 modes of one parity: one 16-byte core-matrix row per
-    // column and split term.
-    size_t doff = 0;
-    for (int p = 0; p < 2; p++) {
-        if (!Kq[p]) break;
-        const int kp = Kp[p];
-        const int npair = ncp >> 1, ngk = kp >> 3;
-        for (int u = tid; u < npair * ngk; u += TCT2) {
-            const int q = u % npair, g = u / npair;
-            const int c = 2 * q;
-            float xr[8], xi[8];
+    // column and split term.  The units of both parities form one index space;
+    // each thread first loads INV_SLOTS units, then splits and stores them, so
+    // the global loads of all its units are in flight together.
+    {
+        const int npair = ncp >> 1;
+        const int U0 = npair * (Kp[0] >> 3), U = U0 + (Kq[1] ? npair * (Kp[1] >> 3) : 0);
+        const int w0 = A.woff[m];
+        constexpr int INV_SLOTS = 2;
+        for (int base = 0; base < U; base += INV_SLOTS * TCI) {
+            float2 x[INV_SLOTS][8];
+            float fl[INV_SLOTS][8];
 #pragma unroll
-            for (int e = 0; e < 8; e++) xr[e] = xi[e] = 0.f;
-            if (c < nc) {
-                bool zv;
-                const float2 *row = inv_row(A, group, (c0 + c) >> 1, &zv);
-                const int w0 = A.woff[m];
+            for (int s = 0; s < INV_SLOTS; s++) {
+                const int u = base + s * TCI + tid;
+                const int p = u >= U0, uu = u - (p ? U0 : 0);
+                const int q = uu % npair, g = uu / npair;
+                const int c = 2 * q;
+                bool zv = false;
+                const float2 *row = (u < U && c < nc) ? inv_row(A, group, (c0 + c) >> 1, &zv) : nullptr;
 #pragma unroll
                 for (int e = 0; e < 8; e++) {
-                    const int k = 8 * g + e;
-                    if (k < Kq[p]) {
-                        const int nm = 2 * k + p;  // n - m
-                        float2 x = __ldg(row + w0 + nm);
-                        if (zv && m == 0 && nm == 1) x.x -= A.plavor;  // dv2uv, legmod.f90:332
-                        const float fl = __ldg(A.filt + m + nm);
-                        xr[e] = x.x * fl;
-                        xi[e] = x.y * fl;
-                    }
+                    const int k = 8 * g + e, nm = 2 * k + p;  // nm = n - m
+                    const bool in = row != nullptr && k < Kq[p];
+                    x[s][e] = in ? __ldg(row + w0 + nm) : make_float2(0.f, 0.f);
+                    fl[s][e] = in ? __ldg(A.filt + m + nm) : 0.f;
+                    if (in && zv && m == 0 && nm == 1) x[s][e].x -= A.plavor;  // dv2uv, legmod.f90:332
                 }
             }
-            const uint32_t o = tc::kmajor_off(c, 8 * g, kp);  // re row; the im row follows at +16
-            unsigned char *d0 = dat + doff;
-            uint4 h, mm, l;
-            tc::split3x8(xr, h, mm, l);
-            st_shared16(d0 + o, h); st_shared16(d0 + dtile[p] + o, mm); st_shared16(d0 + 2 * dtile[p] + o, l);
-            tc::split3x8(xi, h, mm, l);
-            st_shared16(d0 + o + 16, h); st_shared16(d0 + dtile[p] + o + 16, mm);
-            st_shared16(d0 + 2 * dtile[p] + o + 16, l);
+#pragma unroll
+            for (int s = 0; s < INV_SLOTS; s++) {
+                const int u = base + s * TCI + tid;
+                if (u >= U) break;
+                const int p = u >= U0, uu = u - (p ? U0 : 0);
+                const int q = uu % npair, g = uu / npair;
+                float xr[8], xi[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    xr[e] = x[s][e].x * fl[s][e];
+                    xi[e] = x[s][e].y * fl[s][e];
+                }
+                const uint32_t o = tc::kmajor_off(2 * q, 8 * g, Kp[p]);  // re row; the im row follows at +16
+                unsigned char *d0 = dat + (p ? 3 * dtile[0] : 0);
+                const size_t dtp = dtile[p];
+                uint4 h, mm, l;
+                tc::split3x8(xr, h, mm, l);
+                st_shared16(d0 + o, h); st_shared16(d0 + dtp + o, mm); st_shared16(d0 + 2 * dtp + o, l);
+                tc::split3x8(xi, h, mm, l);
+                st_shared16(d0 + o + 16, h); st_shared16(d0 + dtp + o + 16, mm);
+                st_shared16(d0 + 2 * dtp + o + 16, l);
+            }
         }
-        doff += 3 * dtile[p];
     }
     tc::fence_proxy_async();
     tc::fence_before_sync();
@@ -173,80 +188,105 @@ __global__ void __launch_bounds__(TCT2) k_tc_inverse(const __grid_constant__ TcI
         if (!ok) atomicExch(&g_tc_error, 1);
     }
     __syncthreads();
-    ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, 0));  // warp-uniform for the .sync.aligned TMEM loads  // single-phase barrier, bounded
+    ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, 0));  // warp-uniform for the .sync.aligned TMEM loads
     if (!ok && lane == 0) atomicExch(&g_tc_error, 2);
     tc::fence_after_sync();
-    if (ok) {
-        const int j = quarter * 32 + lane;  // TMEM lane = latitude pair
+    // epilogue: TMEM lane = latitude pair j; quarters past the last pair hold
+    // nothing (a warp-uniform test, as the TMEM loads need whole warps)
+    if (ok && quarter * 32 < A.nlath) {
+        const int j = quarter * 32 + lane;
         const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
         const int L = A.L, nfo = 6 * L + 3, nf = 4 * L + 1;
         const bool has1 = Kq[1] > 0;
-        for (int cc = half * 16; cc < ncp; cc += 32) {
-            float d[4][16];
-            uint32_t rm[4][16], rc[4][16];
-#pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const int ti = r >> 1, p = r & 1;
-                if (ti >= ntab || (p == 1 && !has1)) continue;
-                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp + cc), rm[r]);
-                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp + cc), rc[r]);
-            }
-            tc::tmem_wait_ld();
-#pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const bool z = (r >> 1) >= ntab || ((r & 1) && !has1);
-#pragma unroll
-                for (int i = 0; i < 16; i++) d[r][i] = z ? 0.f : __uint_as_float(rm[r][i]) + __uint_as_float(rc[r][i]);
-            }
-            if (j >= A.nlath) continue;
-            const int latN = j, latS = A.nlat - 1 - j;
-            if (group < 2) {
-                // P-type qi: N = D0 + D1, S = D0 - D1; Q-type qj: S = D1 - D0
-                const float ss = group == 0 ? 1.f : -1.f;
+        const bool row_ok = j < A.nlath;
+        const int latN = j, latS = A.nlat - 1 - j;
+        float2 *Wm = A.W + (size_t)m * A.nrows;
+        if (group < 2) {
+            // P-type qi: N = D0 + D1, S = D0 - D1; Q-type qj: S = D1 - D0
+            const float ss = group == 0 ? 1.f : -1.f;
+            for (int cc = sub * 16; cc < ncp; cc += 64) {
+                uint32_t rm0[16], rc0[16], rm1[16], rc1[16];
+                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(0 * ncp + cc), rm0);
+                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(1 * ncp + cc), rc0);
+                if (has1) {
+                    tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(2 * ncp + cc), rm1);
+                    tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(3 * ncp + cc), rc1);
+                }
+                tc::tmem_wait_ld();
+                // column pair gq = (c0 + cc)/2 + i/2: instance and field without a
+                // division per pair (a chunk holds 8 pairs, fewer than nf)
+                const int gq0 = (c0 + cc) >> 1;
+                const int inst0 = group == 0 ? gq0 / nf : gq0, f0 = group == 0 ? gq0 - inst0 * nf : 4 * L;
 #pragma unroll
                 for (int i = 0; i < 16; i += 2) {
-                    if (cc + i >= nc) break;
-                    const int gq = (c0 + cc + i) >> 1;
-                    int inst, f;
-                    if (group == 0) { inst = gq / nf; f = gq % nf; }
-                    else { inst = gq; f = 4 * L; }
-                    float2 vn = make_float2(d[0][i] + d[1][i], d[0][i + 1] + d[1][i + 1]);
-                    float2 vs = make_float2(ss * (d[0][i] - d[1][i]), ss * (d[0][i + 1] - d[1][i + 1]));
+                    const float d0r = __uint_as_float(rm0[i]) + __uint_as_float(rc0[i]);
+                    const float d0i = __uint_as_float(rm0[i + 1]) + __uint_as_float(rc0[i + 1]);
+                    const float d1r = has1 ? __uint_as_float(rm1[i]) + __uint_as_float(rc1[i]) : 0.f;
+                    const float d1i = has1 ? __uint_as_float(rm1[i + 1]) + __uint_as_float(rc1[i + 1]) : 0.f;
+                    if (!row_ok || cc + i >= nc) continue;
+                    int inst = inst0, f = f0;
+                    if (group == 0) {
+                        f += i >> 1;
+                        if (f >= nf) { f -= nf; inst++; }
+                    } else {
+                        inst += i >> 1;
+                    }
+                    const float2 vn = make_float2(d0r + d1r, d0i + d1i);
+                    const float2 vs = make_float2(ss * (d0r - d1r), ss * (d0i - d1i));
                     int F;
                     if (group == 1) F = 6 * L;                    // gpj
                     else if (f < L) F = 3 * L + f;                // sd -> gd
                     else if (f < 2 * L) F = f + L;                // st -> gt
                     else if (f < 4 * L) F = f + 2 * L;            // sz -> gz, sq -> gq
                     else F = 6 * L + 2;                           // sp -> gp
-                    const size_t rb = (size_t)m * A.nrows + (size_t)(inst * nfo + F) * A.nlat;
-                    A.W[rb + latN] = vn;
-                    A.W[rb + latS] = vs;
+                    float2 *wr = Wm + (size_t)(inst * nfo + F) * A.nlat;
+                    wr[latN] = vn;
+                    wr[latS] = vs;
                     if (group == 0 && f == 4 * L) {               // gpmt = i*m*gp
                         const float fm = (float)m;
-                        const size_t rt = (size_t)m * A.nrows + (size_t)(inst * nfo + 6 * L + 1) * A.nlat;
-                        A.W[rt + latN] = make_float2(-fm * vn.y, fm * vn.x);
-                        A.W[rt + latS] = make_float2(-fm * vs.y, fm * vs.x);
+                        float2 *wt = Wm + (size_t)(inst * nfo + 6 * L + 1) * A.nlat;
+                        wt[latN] = make_float2(-fm * vn.y, fm * vn.x);
+                        wt[latS] = make_float2(-fm * vs.y, fm * vs.x);
                     }
                 }
-            } else {
-                // dv2uv: u = qv*Z - i*qu*D, v = -i*qu*Z - qv*D; qu P-type, qv Q-type
-                // d[0]=qu p0, d[1]=qu p1, d[2]=qv p0, d[3]=qv p1; columns Dr,Di,Zr,Zi per level
+            }
+        } else {
+            // dv2uv: u = qv*Z - i*qu*D, v = -i*qu*Z - qv*D; qu P-type, qv Q-type.
+            // accumulators r = (table, parity): 0 qu p0, 1 qu p1, 2 qv p0, 3 qv p1;
+            // columns Dr, Di, Zr, Zi per level; a chunk of 8 columns is 2 levels
+            for (int cc = sub * 8; cc < ncp; cc += 32) {
+                uint32_t rm[4][8], rc[4][8];
 #pragma unroll
-                for (int i = 0; i < 16; i += 4) {
-                    if (cc + i >= nc) break;
-                    const int gc = c0 + cc + i;
-                    const int inst = gc / (4 * L), l = (gc % (4 * L)) >> 2;
+                for (int r = 0; r < 4; r++) {
+                    if ((r & 1) && !has1) continue;
+                    tc::tmem_ld8_nw(tmem + lane_addr + (uint32_t)((r * 2 + 0) * ncp + cc), rm[r]);
+                    tc::tmem_ld8_nw(tmem + lane_addr + (uint32_t)((r * 2 + 1) * ncp + cc), rc[r]);
+                }
+                tc::tmem_wait_ld();
+                float d[4][8];
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int i = 0; i < 8; i++)
+                        d[r][i] = ((r & 1) && !has1) ? 0.f : __uint_as_float(rm[r][i]) + __uint_as_float(rc[r][i]);
+                const int q0 = (c0 + cc) >> 2;                    // (instance, level) of the chunk's first level
+                const int inst0 = q0 / L, l0 = q0 - inst0 * L;
+#pragma unroll
+                for (int i = 0; i < 8; i += 4) {
+                    if (!row_ok || cc + i >= nc) continue;
+                    int inst = inst0, l = l0 + (i >> 2);
+                    if (l >= L) { l -= L; inst++; }
                     const int Dr = i, Di = i + 1, Zr = i + 2, Zi = i + 3;
                     const float urs = d[0][Di] + d[3][Zr], ura = d[1][Di] + d[2][Zr];
                     const float uis = -d[0][Dr] + d[3][Zi], uia = -d[1][Dr] + d[2][Zi];
                     const float vrs = d[0][Zi] - d[3][Dr], vra = d[1][Zi] - d[2][Dr];
                     const float vis = -d[0][Zr] - d[3][Di], via = -d[1][Zr] - d[2][Di];
-                    const size_t ru = (size_t)m * A.nrows + (size_t)(inst * nfo + l) * A.nlat;
-                    const size_t rv = (size_t)m * A.nrows + (size_t)(inst * nfo + L + l) * A.nlat;
-                    A.W[ru + latN] = make_float2(urs + ura, uis + uia);
-                    A.W[ru + latS] = make_float2(urs - ura, uis - uia);
-                    A.W[rv + latN] = make_float2(vrs + vra, vis + via);
-                    A.W[rv + latS] = make_float2(vrs - vra, vis - via);
+                    float2 *wu = Wm + (size_t)(inst * nfo + l) * A.nlat;
+                    float2 *wv = Wm + (size_t)(inst * nfo + L + l) * A.nlat;
+                    wu[latN] = make_float2(urs + ura, uis + uia);
+                    wu[latS] = make_float2(urs - ura, uis - uia);
+                    wv[latN] = make_float2(vrs + vra, vis + via);
+                    wv[latS] = make_float2(vrs - vra, vis - via);
                 }
             }
         }
@@ -669,6 +709,95 @@ __device__ __forceinline__ void f3_combine(int t, int c, float v, float (*o)[4][
     }
 }
 
+// load the north and south rows of one staging unit (column pair u % npair of
+// table t, latitude pairs 8 (u / npair) ..+7); zeros outside the job
+template <int NLT>
+__device__ __forceinline__ void f3_load(const TcFwd3Args &A, int m, int inst, int l0, int nl, bool with_vpp, int t,
+                                        int u, float2 *vn, float2 *vs) {
+    const int nf = c_fwd_nf[t];
+    const int npair = fwd_ncp<NLT>(t) >> 1, ng = A.njc >> 3;
+    const int nreal = nf * NLT + ((t == 0) ? 1 : 0);
+    const int q = u % npair, g = u / npair;
+    long long rb = -1;
+    if (g < ng && q < nreal) {
+        if (t == 0 && q == nf * NLT) { if (with_vpp) rb = fwd_row(A.L, inst, 7, 0); }
+        else {
+            const int fi = q / NLT, li = q - fi * NLT;
+            if (li < nl) rb = fwd_row(A.L, inst, c_fwd_fields[t][fi], l0 + li);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 8; e++) vn[e] = vs[e] = make_float2(0.f, 0.f);
+    if (rb < 0) return;
+    const int nlat = A.nlat, j0 = 8 * g;
+    const float2 *wr = A.W + (size_t)m * A.nrows + (size_t)rb * nlat;
+    if (j0 + 8 <= A.nlath) {
+        // rows j0..j0+7 north, and nlat-8-j0..nlat-1-j0 south (reversed)
+        const float4 *pn = reinterpret_cast<const float4 *>(wr + j0);
+        const float4 *ps = reinterpret_cast<const float4 *>(wr + nlat - 8 - j0);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float4 x = __ldg(pn + i), y = __ldg(ps + i);
+            vn[2 * i] = make_float2(x.x, x.y);
+            vn[2 * i + 1] = make_float2(x.z, x.w);
+            vs[7 - 2 * i] = make_float2(y.x, y.y);
+            vs[6 - 2 * i] = make_float2(y.z, y.w);
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; e++)
+            if (j0 + e < A.nlath) {
+                vn[e] = __ldg(wr + j0 + e);
+                vs[e] = __ldg(wr + nlat - 1 - j0 - e);
+            }
+    }
+}
+
+// fold a loaded unit for parity p, split it into three BF16 terms and store
+// the re and im core-matrix rows of every term
+template <int NLT>
+__device__ __forceinline__ void f3_store(int t, int p, int u, int njc, unsigned char *bt, const float2 *vn,
+                                         const float2 *vs) {
+    const int ncp = fwd_ncp<NLT>(t), npair = ncp >> 1;
+    const int q = u % npair, g = u / npair;
+    const bool diff = (t != 1) ? (p == 1) : (p == 0);
+    float xr[8], xi[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+        xr[e] = diff ? vn[e].x - vs[e].x : vn[e].x + vs[e].x;
+        xi[e] = diff ? vn[e].y - vs[e].y : vn[e].y + vs[e].y;
+    }
+    const uint32_t dt = (uint32_t)ncp * njc * 2;
+    const uint32_t o = tc::kmajor_off(2 * q, 8 * g, njc);
+    uint4 h, mm, l;
+    tc::split3x8(xr, h, mm, l);
+    st_shared16(bt + o, h); st_shared16(bt + dt + o, mm); st_shared16(bt + 2 * dt + o, l);
+    tc::split3x8(xi, h, mm, l);
+    st_shared16(bt + o + 16, h); st_shared16(bt + dt + o + 16, mm); st_shared16(bt + 2 * dt + o + 16, l);
+}
+
+// sum the split blocks of table T's accumulator columns for this thread's TMEM
+// row and fold them into the partial outputs
+template <int NLT, int T>
+__device__ __forceinline__ void f3_drain(uint32_t taddr, int nprod, float (*o)[4][2], float *ov) {
+    constexpr int ncp = fwd_ncp<NLT>(T);
+    const uint32_t X = taddr + (uint32_t)f3_colbase<NLT>(T);
+#pragma unroll
+    for (int c0 = 0; c0 < ncp; c0 += 16) {
+        uint32_t x0[16], x1[16], x2[16];
+        tc::tmem_ld16_nw(X + c0, x0);
+        tc::tmem_ld16_nw(X + ncp + c0, x1);
+        if (nprod == 6) tc::tmem_ld16_nw(X + 2 * ncp + c0, x2);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            float v = __uint_as_float(x0[i]) + __uint_as_float(x1[i]);
+            if (nprod == 6) v += __uint_as_float(x2[i]);
+            f3_combine<NLT>(T, c0 + i, v, o, ov);
+        }
+    }
+}
+
 // 16 warps: warp 0 issues copies and MMAs, warps 1-15 stage operands (the
 // staging loads are latency-bound, so more warps keep more of them in flight),
 // warps 0-3 drain TMEM
@@ -684,7 +813,7 @@ __global__ void __launch_bounds__(TCT3) k_tc_forward3(const __grid_constant__ Tc
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3;
     const int K = A.ntp1 - m;
     const int Kq = kpar(K, p), R = pad8(Kq);
-    const int njc = A.njc, L = A.L, nlat = A.nlat;
+    const int njc = A.njc, L = A.L;
     const bool with_vpp = (l0 == 0);
     const uint32_t tbytes = (uint32_t)8 * R * njc;   // one (m, table, parity) block
     const uint32_t tbuf = (uint32_t)8 * 64 * njc;    // buffer for the widest block
@@ -693,7 +822,11 @@ __global__ void __launch_bounds__(TCT3) k_tc_forward3(const __grid_constant__ Tc
     unsigned char *dat = sm + 2 * tbuf + 128 * 32 * 2;
     size_t doffs[4], dbytes = 0;
     for (int t = 0; t < 4; t++) { doffs[t] = dbytes; dbytes += 3 * (size_t)fwd_ncp<NLT>(t) * njc * 2; }
-    unsigned char *tail = dat + dbytes;
+    // the epilogue's partial outputs reuse the table and operand space; the
+    // barriers lie past both
+    constexpr int NO = NLT * 8 + 2;
+    constexpr size_t ebytes = 4 * 128 * NO * sizeof(float);
+    unsigned char *tail = (size_t)(dat + dbytes - sm) > ebytes ? dat + dbytes : sm + ebytes;
     uint64_t *bars = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
     uint64_t *bar_tma = bars;       // [2] table buffer b landed
     uint64_t *bar_mma = bars + 2;   // [2] MMAs reading table buffer b completed
@@ -718,68 +851,28 @@ __global__ void __launch_bounds__(TCT3) k_tc_forward3(const __grid_constant__ Tc
     // warps 1-15 stage the folded columns each table needs for this parity,
     // table by table, while warp 0 issues the MMAs of every table already
     // staged.  P-type tables (qc, qm, qq) take N+S on even n-m and N-S on odd,
-    // Q-type (qe) the reverse.
-    const int ng = njc >> 3;
-    for (int t = 0; t < 4 && warp != 0; t++) {
-        const int nf = c_fwd_nf[t];
-        const int ncp = fwd_ncp<NLT>(t), npair = ncp >> 1;
-        const int nreal = nf * NLT + ((t == 0) ? 1 : 0);
-        const bool diff = (t != 1) ? (p == 1) : (p == 0);
-        const uint32_t dt = (uint32_t)ncp * njc * 2;
-        unsigned char *bt = dat + doffs[t];
-        const int nunit = npair * ng;
-        for (int u = tid - 32; u < nunit; u += TCT3 - 32) {
-            const int q = u % npair, g = u / npair;
-            long long rb = -1;
-            if (q < nreal) {
-                if (t == 0 && q == nf * NLT) { if (with_vpp) rb = fwd_row(L, inst, 7, 0); }
-                else {
-                    const int fi = q / NLT, li = q - fi * NLT;
-                    if (li < nl) rb = fwd_row(L, inst, c_fwd_fields[t][fi], l0 + li);
-                }
+    // Q-type (qe) the reverse.  A unit (column pair, 8 latitude pairs) of the
+    // next table is loaded before the current one is split and stored, so the
+    // loads of successive tables overlap.
+    if (warp != 0) {
+        const int stid = tid - 32;
+        float2 vn[8], vs[8];
+        f3_load<NLT>(A, m, inst, l0, nl, with_vpp, 0, stid, vn, vs);
+        for (int t = 0; t < 4; t++) {
+            const int nunit = (fwd_ncp<NLT>(t) >> 1) * (njc >> 3);
+            float2 wn[8], ws[8];
+            if (t + 1 < 4) f3_load<NLT>(A, m, inst, l0, nl, with_vpp, t + 1, stid, wn, ws);
+            if (stid < nunit) f3_store<NLT>(t, p, stid, njc, dat + doffs[t], vn, vs);
+            // more units than staging threads (not at NLAT <= 192, where every table has fewer)
+            for (int u = stid + (TCT3 - 32); u < nunit; u += TCT3 - 32) {
+                f3_load<NLT>(A, m, inst, l0, nl, with_vpp, t, u, vn, vs);
+                f3_store<NLT>(t, p, u, njc, dat + doffs[t], vn, vs);
             }
-            const int j0 = 8 * g;
-            float xr[8], xi[8];
-            float2 vn[8], vs[8];
+            tc::fence_proxy_async();  // these stores feed the tensor cores
+            tc::mbar_arrive(bar_stage + t);
 #pragma unroll
-            for (int e = 0; e < 8; e++) vn[e] = vs[e] = make_float2(0.f, 0.f);
-            if (rb >= 0) {
-                const float2 *wr = A.W + (size_t)m * A.nrows + (size_t)rb * nlat;
-                if (j0 + 8 <= A.nlath) {
-                    // rows j0..j0+7 north, and nlat-8-j0..nlat-1-j0 south (reversed)
-                    const float4 *pn = reinterpret_cast<const float4 *>(wr + j0);
-                    const float4 *ps = reinterpret_cast<const float4 *>(wr + nlat - 8 - j0);
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const float4 x = __ldg(pn + i), y = __ldg(ps + i);
-                        vn[2 * i] = make_float2(x.x, x.y);
-                        vn[2 * i + 1] = make_float2(x.z, x.w);
-                        vs[7 - 2 * i] = make_float2(y.x, y.y);
-                        vs[6 - 2 * i] = make_float2(y.z, y.w);
-                    }
-                } else {
-#pragma unroll
-                    for (int e = 0; e < 8; e++)
-                        if (j0 + e < A.nlath) {
-                            vn[e] = __ldg(wr + j0 + e);
-                            vs[e] = __ldg(wr + nlat - 1 - j0 - e);
-                        }
-                }
-            }
-#pragma unroll
-            for (int e = 0; e < 8; e++) {
-                xr[e] = diff ? vn[e].x - vs[e].x : vn[e].x + vs[e].x;
-                xi[e] = diff ? vn[e].y - vs[e].y : vn[e].y + vs[e].y;
-            }
-            const uint32_t o = tc::kmajor_off(2 * q, j0, njc);
-            uint4 h, mm, l;
-            tc::split3x8(xr, h, mm, l);
-            st_shared16(bt + o, h); st_shared16(bt + dt + o, mm); st_shared16(bt + 2 * dt + o, l);
-            tc::split3x8(xi, h, mm, l);
-            st_shared16(bt + o + 16, h); st_shared16(bt + dt + o + 16, mm); st_shared16(bt + 2 * dt + o + 16, l);
+            for (int e = 0; e < 8; e++) { vn[e] = wn[e]; vs[e] = ws[e]; }
         }
-        tc::fence_proxy_async();  // these stores feed the tensor cores
-        tc::mbar_arrive(bar_stage + t);
     }
     if (tid == 0) {
         const uint32_t sbo_b = (uint32_t)(njc / 8) * 128;
@@ -823,42 +916,26 @@ __global__ void __launch_bounds__(TCT3) k_tc_forward3(const __grid_constant__ Tc
     ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, 0));  // warp-uniform for the .sync.aligned TMEM loads
     if (!ok && lane == 0) atomicExch(&g_tc_error, 6);
     tc::fence_after_sync();
-    // epilogue (warps 0-3, one per TMEM lane quarter): row r holds mode r (r < R)
-    // or corrections of mode r - R (R <= r < 2R); rows >= R hand their partial
-    // outputs to rows < R through shared memory
-    constexpr int NO = NLT * 8 + 2;
-    float *E = reinterpret_cast<float *>(dat);   // [64][NO]; the operands are dead now
+    // epilogue: warp w drains table w / 4 for TMEM lane quarter w % 4.  Row r
+    // holds mode r (r < R) or corrections of mode r - R (R <= r < 2R); every
+    // (table, row) hands its partial outputs to shared memory, and the sums
+    // over tables and both rows of a mode are formed there.
+    float *E = reinterpret_cast<float *>(sm);   // [4][128][NO]; tables and operands are dead now
     const int r = quarter * 32 + lane;
-    const bool drain = ok && warp < 4;            // warp-uniform (ok is)
-    float o[NLT][4][2], ov[2] = {0.f, 0.f};
-#pragma unroll
-    for (int li = 0; li < NLT; li++)
-#pragma unroll
-        for (int k = 0; k < 4; k++) o[li][k][0] = o[li][k][1] = 0.f;
-    if (drain) {
+    const int gw = warp >> 2;
+    if (ok && quarter * 32 < 2 * R) {           // warp-uniform (ok is)
         const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+        float o[NLT][4][2], ov[2] = {0.f, 0.f};
 #pragma unroll
-        for (int t = 0; t < 4; t++) {
-            const int ncp = fwd_ncp<NLT>(t);
-            const uint32_t X = tmem + lane_addr + (uint32_t)f3_colbase<NLT>(t);
+        for (int li = 0; li < NLT; li++)
 #pragma unroll
-            for (int c0 = 0; c0 < 48; c0 += 16) {
-                if (c0 >= ncp) break;
-                uint32_t x0[16], x1[16], x2[16];
-                tc::tmem_ld16_nw(X + c0, x0);
-                tc::tmem_ld16_nw(X + ncp + c0, x1);
-                if (nprod == 6) tc::tmem_ld16_nw(X + 2 * ncp + c0, x2);
-                tc::tmem_wait_ld();
-#pragma unroll
-                for (int i = 0; i < 16; i++) {
-                    float v = __uint_as_float(x0[i]) + __uint_as_float(x1[i]);
-                    if (nprod == 6) v += __uint_as_float(x2[i]);
-                    f3_combine<NLT>(t, c0 + i, v, o, ov);
-                }
-            }
-        }
-        if (r >= R && r < 2 * R) {
-            float *e = E + (size_t)(r - R) * NO;
+            for (int k = 0; k < 4; k++) o[li][k][0] = o[li][k][1] = 0.f;
+        if (gw == 0) f3_drain<NLT, 0>(tmem + lane_addr, nprod, o, ov);
+        else if (gw == 1) f3_drain<NLT, 1>(tmem + lane_addr, nprod, o, ov);
+        else if (gw == 2) f3_drain<NLT, 2>(tmem + lane_addr, nprod, o, ov);
+        else f3_drain<NLT, 3>(tmem + lane_addr, nprod, o, ov);
+        if (r < 2 * R) {
+            float *e = E + (size_t)(gw * 128 + r) * NO;
 #pragma unroll
             for (int li = 0; li < NLT; li++)
 #pragma unroll
@@ -871,26 +948,32 @@ __global__ void __launch_bounds__(TCT3) k_tc_forward3(const __grid_constant__ Tc
         }
     }
     __syncthreads();
-    if (drain && r < Kq) {
-        const float *e = E + (size_t)r * NO;
-        const int k = 2 * r + p;  // n - m
-        const float fl = A.filt[m + k];
-        const size_t wo = 2 * (size_t)(A.woff[m] + k);
-        const int nfo = 4 * L + 1;
-#pragma unroll
-        for (int li = 0; li < NLT; li++) {
-            if (li >= nl) break;
-            const int l = l0 + li;
-#pragma unroll
-            for (int kk = 0; kk < 4; kk++) {
-                float2 *dst = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + kk * L + l) * A.nrsp + wo);
-                *dst = make_float2((o[li][kk][0] + e[(li * 4 + kk) * 2]) * fl,
-                                   (o[li][kk][1] + e[(li * 4 + kk) * 2 + 1]) * fl);
+    if (ok) {
+        // outputs: Kq modes x (4 fields x NLT levels + spf); consecutive threads take consecutive modes
+        const int nout = 4 * NLT + 1, nfo = 4 * L + 1;
+        const size_t wb = (size_t)A.woff[m];
+        for (int idx = tid; idx < Kq * nout; idx += TCT3) {
+            const int oi = idx / Kq, rr = idx - oi * Kq;
+            size_t fr;                                   // output field row
+            if (oi < 4 * NLT) {
+                const int li = oi >> 2, kk = oi & 3;
+                if (li >= nl) continue;
+                fr = (size_t)inst * nfo + kk * L + l0 + li;
+            } else {
+                if (!with_vpp) continue;
+                fr = (size_t)inst * nfo + 4 * L;
             }
-        }
-        if (with_vpp) {
-            float2 *sp = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + 4 * L) * A.nrsp + wo);
-            *sp = make_float2((ov[0] + e[NLT * 8]) * fl, (ov[1] + e[NLT * 8 + 1]) * fl);
+            float sr = 0.f, si = 0.f;
+#pragma unroll
+            for (int g = 0; g < 4; g++) {
+                const float *e0 = E + (size_t)(g * 128 + rr) * NO + 2 * oi;
+                const float *e1 = E + (size_t)(g * 128 + R + rr) * NO + 2 * oi;
+                sr += e0[0] + e1[0];
+                si += e0[1] + e1[1];
+            }
+            const int k = 2 * rr + p;                    // n - m
+            const float fl = A.filt[m + k];
+            reinterpret_cast<float2 *>(A.spout + fr * A.nrsp)[wb + k] = make_float2(sr * fl, si * fl);
         }
     }
     tc::fence_before_sync();
@@ -898,9 +981,10 @@ __global__ void __launch_bounds__(TCT3) k_tc_forward3(const __grid_constant__ Tc
     if (warp == 0) tc::tmem_dealloc(tmem, 512);
 }
 
-// shared memory of a stacked-split forward job (tables of at most 64 modes per parity)
 static size_t fwd3_smem(int njc, int nlt) {
     size_t d = 0;
     for (int t = 0; t < 4; t++) d += 3 * (size_t)fwd_ncp_rt(nlt, t) * njc * 2;
-    return 2 * (size_t)8 * 64 * njc + 128 * 32 * 2 + d + 128;
+    const size_t ops = 2 * (size_t)8 * 64 * njc + 128 * 32 * 2 + d;
+    const size_t ebytes = 4 * 128 * (size_t)(nlt * 8 + 2) * sizeof(float);
+    return std::max(ops, ebytes) + 128;
 }
