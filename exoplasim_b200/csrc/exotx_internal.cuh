@@ -52,6 +52,9 @@ const FftTables *fft_tables(int n, exotx_status *st);
 
 // Mixed-precision table copies built on first use (see legendre_tc.cu).
 struct TcTables;
+// Device slots, streams and events of the host-memory set pipeline (host_sets.cu).
+struct HostPipe;
+void host_pipe_free(exotx_plan p);
 
 }  // namespace exotx
 
@@ -74,6 +77,7 @@ struct exotx_plan_s {
     void *d_work = nullptr;
     size_t work_bytes = 0;
     exotx::TcTables *tc = nullptr;
+    exotx::HostPipe *hpipe = nullptr;  // device slots and streams of exotx_sets_host
 };
 
 namespace exotx {

@@ -1,0 +1,150 @@
+// Transform sets of many instances whose arrays live in host memory.
+//
+// A host model (the Fortran gridpointa, plasim.f90:2396-2486, or a driver of
+// many planets) keeps its spectral and grid-point arrays in host memory.  Here
+// the instances stream through three device slots on three streams: while the
+// transforms of group k run, the inputs of group k+1 are copied in and the
+// outputs of group k-1 are copied out, so the PCIe link carries data in both
+// directions while the GPU computes.  Every slot is reused only after the
+// copy-out of its previous group has finished (events order the streams).
+#include <algorithm>
+#include "exotx_internal.cuh"
+
+namespace exotx {
+
+struct HostPipe {
+    static constexpr int NSLOT = 3;
+    int prec = -1, nlev = 0, group = 0;
+    void *d_spin[NSLOT] = {}, *d_gout[NSLOT] = {}, *d_gin[NSLOT] = {}, *d_sout[NSLOT] = {};
+    cudaStream_t s_in = nullptr, s_run = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in[NSLOT] = {}, ev_run[NSLOT] = {}, ev_out[NSLOT] = {}, ev_edge = nullptr;
+
+    void free_buffers() {
+        for (int i = 0; i < NSLOT; i++) {
+            cudaFree(d_spin[i]); cudaFree(d_gout[i]); cudaFree(d_gin[i]); cudaFree(d_sout[i]);
+            d_spin[i] = d_gout[i] = d_gin[i] = d_sout[i] = nullptr;
+        }
+        prec = -1; nlev = 0; group = 0;
+    }
+    ~HostPipe() {
+        if (s_in) cudaStreamSynchronize(s_in);
+        if (s_run) cudaStreamSynchronize(s_run);
+        if (s_out) cudaStreamSynchronize(s_out);
+        free_buffers();
+        for (int i = 0; i < NSLOT; i++) {
+            if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+            if (ev_run[i]) cudaEventDestroy(ev_run[i]);
+            if (ev_out[i]) cudaEventDestroy(ev_out[i]);
+        }
+        if (ev_edge) cudaEventDestroy(ev_edge);
+        if (s_in) cudaStreamDestroy(s_in);
+        if (s_run) cudaStreamDestroy(s_run);
+        if (s_out) cudaStreamDestroy(s_out);
+    }
+};
+
+void host_pipe_free(exotx_plan p) {
+    delete p->hpipe;
+    p->hpipe = nullptr;
+}
+
+// bytes of one instance's arrays: spectral in/out, grid out (6L+3 fields), grid in (9L+1)
+static void inst_bytes(exotx_plan p, int prec, int L, size_t *sp, size_t *go, size_t *gi) {
+    const size_t esz = prec == EXOTX_FP64 ? 8 : 4;
+    const size_t nhor = (size_t)p->nlat * p->nlon;
+    *sp = (size_t)(4 * L + 1) * 2 * p->ncsp * esz;
+    *go = (size_t)(6 * L + 3) * nhor * esz;
+    *gi = (size_t)(9 * L + 1) * nhor * esz;
+}
+
+static exotx_status pipe_setup(exotx_plan p, int prec, int L, int ninst, HostPipe **out) {
+    if (!p->hpipe) p->hpipe = new HostPipe();
+    HostPipe *h = p->hpipe;
+    if (!h->s_in) {
+        EXOTX_CUDA(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking));
+        EXOTX_CUDA(cudaStreamCreateWithFlags(&h->s_run, cudaStreamNonBlocking));
+        EXOTX_CUDA(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
+        for (int i = 0; i < HostPipe::NSLOT; i++) {
+            EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_in[i], cudaEventDisableTiming));
+            EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_run[i], cudaEventDisableTiming));
+            EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_out[i], cudaEventDisableTiming));
+        }
+        EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_edge, cudaEventDisableTiming));
+    }
+    size_t sp, go, gi;
+    inst_bytes(p, prec, L, &sp, &go, &gi);
+    // instances per slot: about 256 MB of arrays, so the transform launches
+    // still cover several instances at small resolutions while the first
+    // copy in and the last copy out (which nothing overlaps) stay short
+    const size_t per = 2 * sp + go + gi;
+    int g = (int)std::max<size_t>(1, (256u << 20) / per);
+    g = std::min(g, std::max(ninst, 1));
+    if (h->prec != prec || h->nlev != L || h->group < g) {
+        EXOTX_CUDA(cudaStreamSynchronize(h->s_in));
+        EXOTX_CUDA(cudaStreamSynchronize(h->s_run));
+        EXOTX_CUDA(cudaStreamSynchronize(h->s_out));
+        h->free_buffers();
+        for (int i = 0; i < HostPipe::NSLOT; i++) {
+            EXOTX_CUDA(cudaMalloc(&h->d_spin[i], sp * g));
+            EXOTX_CUDA(cudaMalloc(&h->d_sout[i], sp * g));
+            EXOTX_CUDA(cudaMalloc(&h->d_gout[i], go * g));
+            EXOTX_CUDA(cudaMalloc(&h->d_gin[i], gi * g));
+        }
+        h->prec = prec; h->nlev = L; h->group = g;
+    }
+    *out = h;
+    return EXOTX_OK;
+}
+
+}  // namespace exotx
+
+using namespace exotx;
+
+EXOTX_API exotx_status exotx_sets_host(exotx_plan p, int prec, const void *h_spin, void *h_gpout, const void *h_gpin,
+                                       void *h_spout, int nlev, int ninst, exotx_stream s) {
+    if (!p || (prec != EXOTX_FP64 && prec != EXOTX_FP32 && prec != EXOTX_MIXED)) return EXOTX_BAD_ARG;
+    if (nlev < 1 || ninst < 0) return EXOTX_BAD_ARG;
+    const bool inv = h_spin || h_gpout, fwd = h_gpin || h_spout;
+    if ((inv && !(h_spin && h_gpout)) || (fwd && !(h_gpin && h_spout)) || !(inv || fwd)) return EXOTX_BAD_ARG;
+    if (ninst == 0) return EXOTX_OK;
+    HostPipe *h;
+    EXOTX_TRY(pipe_setup(p, prec, nlev, ninst, &h));
+    size_t sp, go, gi;
+    inst_bytes(p, prec, nlev, &sp, &go, &gi);
+    const cudaStream_t cs = (cudaStream_t)s;
+    // the pipeline starts after the work already queued on the caller's stream
+    EXOTX_CUDA(cudaEventRecord(h->ev_edge, cs));
+    EXOTX_CUDA(cudaStreamWaitEvent(h->s_in, h->ev_edge, 0));
+    const int g = h->group;
+    for (int k = 0, i0 = 0; i0 < ninst; k++, i0 += g) {
+        const int ni = std::min(g, ninst - i0), b = k % HostPipe::NSLOT;
+        // copy in: the slot is free once its previous group's outputs are out
+        // (in this call or an earlier one; a never-recorded event is no wait)
+        EXOTX_CUDA(cudaStreamWaitEvent(h->s_in, h->ev_out[b], 0));
+        if (inv)
+            EXOTX_CUDA(cudaMemcpyAsync(h->d_spin[b], (const char *)h_spin + sp * i0, sp * ni,
+                                       cudaMemcpyHostToDevice, h->s_in));
+        if (fwd)
+            EXOTX_CUDA(cudaMemcpyAsync(h->d_gin[b], (const char *)h_gpin + gi * i0, gi * ni, cudaMemcpyHostToDevice,
+                                       h->s_in));
+        EXOTX_CUDA(cudaEventRecord(h->ev_in[b], h->s_in));
+        // transforms
+        EXOTX_CUDA(cudaStreamWaitEvent(h->s_run, h->ev_in[b], 0));
+        if (inv) EXOTX_TRY(exotx_inverse_set_batch(p, prec, h->d_spin[b], h->d_gout[b], nlev, ni, h->s_run));
+        if (fwd) EXOTX_TRY(exotx_forward_set_batch(p, prec, h->d_gin[b], h->d_sout[b], nlev, ni, h->s_run));
+        EXOTX_CUDA(cudaEventRecord(h->ev_run[b], h->s_run));
+        // copy out
+        EXOTX_CUDA(cudaStreamWaitEvent(h->s_out, h->ev_run[b], 0));
+        if (inv)
+            EXOTX_CUDA(cudaMemcpyAsync((char *)h_gpout + go * i0, h->d_gout[b], go * ni, cudaMemcpyDeviceToHost,
+                                       h->s_out));
+        if (fwd)
+            EXOTX_CUDA(cudaMemcpyAsync((char *)h_spout + sp * i0, h->d_sout[b], sp * ni, cudaMemcpyDeviceToHost,
+                                       h->s_out));
+        EXOTX_CUDA(cudaEventRecord(h->ev_out[b], h->s_out));
+    }
+    // the caller's stream continues once every output is in host memory
+    EXOTX_CUDA(cudaEventRecord(h->ev_edge, h->s_out));
+    EXOTX_CUDA(cudaStreamWaitEvent(cs, h->ev_edge, 0));
+    return EXOTX_OK;
+}

@@ -228,6 +228,7 @@ exotx_status ensure_work(exotx_plan p, size_t bytes) {
 
 static void plan_free(exotx_plan p) {
     if (!p) return;
+    host_pipe_free(p);
     tc_free(p);
     cudaFree(p->d_woff);
     cudaFree(p->d_sid);

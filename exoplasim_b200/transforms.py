@@ -248,6 +248,30 @@ class Plan:
         call("exotx_forward_set_batch", self._h, p, _ptr(gpin), _ptr(out), nlev, ninst, _stream())
         return out
 
+    def sets_host(self, nlev, spin=None, gpout=None, gpin=None, spout=None, precision="mixed"):
+        """Both transform sets for states held in HOST tensors (page-locked for
+        overlap): spin (ninst, 4L+1, NRSP) -> gpout (ninst, 6L+3, NLAT, NLON) and
+        gpin (ninst, 9L+1, NLAT, NLON) -> spout (ninst, 4L+1, NRSP); leave out a
+        half by passing None for both of its tensors.  The copies and transforms
+        of neighbouring states overlap; the current stream waits for the last
+        copy out, so synchronise it before reading the outputs."""
+        p = _prec(precision)
+        dt = _dtype(p)
+        ninst = (spin if spin is not None else gpin).shape[0]
+        shapes = {"spin": (ninst, 4 * nlev + 1, self.nrsp), "gpout": (ninst, 6 * nlev + 3, self.nlat, self.nlon),
+                  "gpin": (ninst, 9 * nlev + 1, self.nlat, self.nlon), "spout": (ninst, 4 * nlev + 1, self.nrsp)}
+        ptrs = []
+        for name, t in (("spin", spin), ("gpout", gpout), ("gpin", gpin), ("spout", spout)):
+            if t is None:
+                ptrs.append(None)
+                continue
+            if not isinstance(t, torch.Tensor) or t.is_cuda:
+                raise TypeError(f"{name} must be a host tensor")
+            if t.dtype != dt or tuple(t.shape) != shapes[name] or not t.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous {dt} tensor of shape {shapes[name]}")
+            ptrs.append(_ptr(t))
+        call("exotx_sets_host", self._h, p, *ptrs, nlev, ninst, _stream())
+
 
 def tc_error():
     """Read and reset the tensor-core kernels' error word (0 = no bounded wait gave up)."""

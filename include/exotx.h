@@ -126,6 +126,18 @@ exotx_status exotx_inverse_set_batch(exotx_plan p, int prec, const void *spin, v
                                      int nlev, int ninst, exotx_stream s);
 exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const void *gpin, void *spout,
                                      int nlev, int ninst, exotx_stream s);
+/* Both sets for ninst states whose arrays are in HOST memory, laid out as for
+ * the _batch calls (h_spin -> h_gpout by the inverse set, h_gpin -> h_spout by
+ * the forward set; pass both pointers of a half as NULL to skip it).  The
+ * states stream through three device slots on the plan's own three streams,
+ * so copies in, transforms and copies out of neighbouring groups of states
+ * overlap; host memory should be page-locked (cudaHostAlloc) for that.  The
+ * work starts after what is queued on s, and s waits for the last copy out:
+ * synchronise s before reading the outputs.  This is the drop-in for a host
+ * model's gridpointa (plasim.f90:2396-2486), whose arrays live in host memory. */
+exotx_status exotx_sets_host(exotx_plan p, int prec, const void *h_spin, void *h_gpout,
+                             const void *h_gpin, void *h_spout, int nlev, int ninst,
+                             exotx_stream s);
 /* Uneven ensembles (no counterpart in the reference, which runs one model
  * state per process): ninst instances with their own nlat (NLON = 2 NLAT) and
  * level count, MIXED precision (float arrays).  Instances of one resolution
