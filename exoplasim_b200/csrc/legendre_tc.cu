@@ -141,9 +141,11 @@ __device__ __forceinline__ void split3d(double x, __nv_bfloat16 &h, __nv_bfloat1
     l = __double2bfloat16(r2);
 }
 
-// inverse block (m, t) = [p][split][rows nj8][Kp_p] (K-major core matrices)
-__global__ void k_build_tc_inv(const double *qref, const int *woff, const long long *off, int nlat, int nlath,
-                               int ncsp, int ntp1, int nj8, int t, int tref, unsigned char *base) {
+// inverse block (m, t) = [p][split][rows nj8][Kp_p] (K-major core matrices); the
+// spectral filter skspgp(n) (legmod.f90:241) is folded into the table entries
+__global__ void k_build_tc_inv(const double *qref, const int *woff, const long long *off, const double *filt,
+                               int nlat, int nlath, int ncsp, int ntp1, int nj8, int t, int tref,
+                               unsigned char *base) {
     const int m = blockIdx.x;
     const int K = ntp1 - m;
     unsigned char *blk = base + off[m * 4 + t];
@@ -156,7 +158,7 @@ __global__ void k_build_tc_inv(const double *qref, const int *woff, const long l
         for (int idx = threadIdx.x; idx < nj8 * Kp; idx += blockDim.x) {
             const int r = idx / Kp, k = idx % Kp;
             double v = 0.0;
-            if (r < nlath && k < Kq) v = q[(size_t)r * ncsp + woff[m] + 2 * k + p];
+            if (r < nlath && k < Kq) v = q[(size_t)r * ncsp + woff[m] + 2 * k + p] * filt[m + 2 * k + p];
             __nv_bfloat16 h, mm, l;
             split3d(v, h, mm, l);
             const uint32_t o = tc::kmajor_off(r, k, Kp);
@@ -282,8 +284,8 @@ static exotx_status tc_tables(exotx_plan p, TcTables **out) {
         }
     }
     for (int t = 0; t < 4; t++) {
-        k_build_tc_inv<<<ntp1, 256>>>(p->d_qref, p->d_woff, T->d_inv_off, p->nlat, p->nlath, p->ncsp, ntp1, T->nj8,
-                                      t, kInvRef[t], T->inv);
+        k_build_tc_inv<<<ntp1, 256>>>(p->d_qref, p->d_woff, T->d_inv_off, p->d_fs64, p->nlat, p->nlath, p->ncsp,
+                                      ntp1, T->nj8, t, kInvRef[t], T->inv);
         note_launch();
         k_build_tc_fwd<<<ntp1, 256>>>(p->d_qref, p->d_woff, T->d_fwd_off, p->nlat, p->nlath, p->ncsp, ntp1, T->njc,
                                       t, kFwdRef[t], T->fwd);
@@ -332,13 +334,25 @@ static int fwd_level(exotx_plan p, const TcTables *T) {
         if (fwd_smem(p->ntp1, T->njc, kFwdNlt[v], kFwdOne[v]) <= TC_SMEM_MAX) return v;
     return -1;
 }
-// the stacked-split forward kernel runs wherever its tables exist and fit
-static bool use_fwd3(const TcTables *T) { return T->has3 && fwd3_smem(T->njc, F3_NLT) <= TC_SMEM_MAX; }
-static exotx_status launch_fwd3(const TcFwd3Launch &P, int njobs, size_t smem, cudaStream_t s) {
-    EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward3<F3_NLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// the persistent stacked-split forward kernel runs wherever its tables exist and fit
+static bool use_fwd3(const TcTables *T) { return T->has3 && fpipe_smem(T->njc) <= TC_SMEM_MAX; }
+// the persistent stacked-split forward kernel: one CTA per SM walks the job list
+static exotx_status launch_fwd_pipe(TcFwd3Launch &P, int njobs, int njmax, cudaStream_t s) {
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        EXOTX_CUDA(cudaGetDevice(&dev));
+        EXOTX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const size_t smem = fpipe_smem(njmax);
+    if (smem > TC_SMEM_MAX) return EXOTX_BAD_DIM;
+    P.njobs = njobs;
+    P.njmax = njmax;
+    EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward_pipe<F3_NLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)TC_SMEM_MAX));
+    const int grid = std::max(1, std::min(njobs, nsm));
     cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
-    k_tc_forward3<F3_NLT><<<njobs, TCT3, smem, s>>>(P);
+    k_tc_forward_pipe<F3_NLT><<<grid, FP_THREADS, smem, s>>>(P);
     EXOTX_CHECK_LAUNCH();
     ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
     return EXOTX_OK;
@@ -482,7 +496,7 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
     const bool v3 = use_fwd3(T);
     const int lv = fwd_level(p, T);
     if (!v3 && lv < 0) return EXOTX_BAD_DIM;
-    const size_t smem = v3 ? fwd3_smem(T->njc, F3_NLT) : fwd_smem(p->ntp1, T->njc, kFwdNlt[lv], kFwdOne[lv]);
+    const size_t smem = v3 ? 0 : fwd_smem(p->ntp1, T->njc, kFwdNlt[lv], kFwdOne[lv]);
     for (int i0 = 0; i0 < ninst; i0 += chunk) {
         const int ni = std::min(chunk, ninst - i0);
         const int4 *jl = jobs;
@@ -496,7 +510,7 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
             P3.jobs = jl;
             P3.nprod = 6;
             fwd3_args(P3.seg[0], p, T, L, (const float2 *)p->d_work, nrows, spout + (size_t)i0 * (4 * L + 1) * nrsp);
-            EXOTX_TRY(launch_fwd3(P3, nj, smem, s));
+            EXOTX_TRY(launch_fwd_pipe(P3, nj, T->njc, s));
             continue;
         }
         TcFwdLaunch P;
@@ -558,7 +572,7 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
                     v.push_back({2 * kw * b, make_int4(m, 2 | (sgi << 2), c, std::min(b, n2 - c))});
             }
         } else if (v3) {
-            smax = std::max(smax, fwd3_smem(T->njc, F3_NLT));
+            smax = std::max(smax, fpipe_smem(T->njc));
             fwd3_jobs(p, T, L, ni, sgi, v);
         } else {
             const int nlt = kFwdNlt[lv];
@@ -634,14 +648,16 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
             TcFwd3Launch P3;
             P3.jobs = d_jobs;
             P3.nprod = nprod;
+            int njmax = 16;
             for (int i = 0; i < nseg; i++) {
                 const EnsSeg &g = segs[i];
                 TcTables *T;
                 EXOTX_TRY(tc_tables(g.p, &T));
                 fwd3_args(P3.seg[i], g.p, T, g.L, (const float2 *)g.W,
                           (long long)g.ninst * (9 * g.L + 1) * g.p->nlat, g.spout);
+                njmax = std::max(njmax, T->njc);
             }
-            return launch_fwd3(P3, njobs, smem, s);
+            return launch_fwd_pipe(P3, njobs, njmax, s);
         }
         P.onebuf = kFwdOne[lv];
         for (int i = 0; i < nseg; i++) {

@@ -8,6 +8,8 @@
 constexpr int TCT2 = 256;
 
 __device__ __forceinline__ void st_shared16(unsigned char *p, uint4 v) { *reinterpret_cast<uint4 *>(p) = v; }
+__device__ __forceinline__ void st_shared4(unsigned char *p, uint32_t v) { *reinterpret_cast<uint32_t *>(p) = v; }
+__device__ __forceinline__ void st_shared8(unsigned char *p, uint2 v) { *reinterpret_cast<uint2 *>(p) = v; }
 
 // ------------------------------------------------------------ inverse
 struct TcInvArgs {
@@ -15,7 +17,7 @@ struct TcInvArgs {
     const long long *off;
     const int *woff;
     const float *spin;      // [inst][4L+1][NRSP]
-    const float *filt;      // skspgp
+    const float *filt;      // skspgp (unused: folded into the tables)
     float2 *W;              // [m][row], row = (inst*(6L+3) + field)*nlat + lat
     long long nrows;
     int L, nlat, nlath, nj8, ntp1, nrsp;
@@ -68,7 +70,8 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
     const int nj8 = A.nj8;
     const size_t ttile[2] = {(size_t)nj8 * Kp[0] * 2, (size_t)nj8 * Kp[1] * 2};
     const size_t tbytes = 3 * (ttile[0] + ttile[1]);
-    const size_t dtile[2] = {(size_t)ncp * Kp[0] * 2, (size_t)ncp * Kp[1] * 2};
+    // data tiles use the padded operand layout (core matrices 144 bytes apart along K)
+    const size_t dtile[2] = {(size_t)(ncp / 8) * (Kp[0] / 8) * tc::kPadLbo, (size_t)(ncp / 8) * (Kp[1] / 8) * tc::kPadLbo};
     unsigned char *tab = sm;
     unsigned char *dat = sm + tbytes;
     unsigned char *tail = dat + 3 * (dtile[0] + dtile[1]) + (size_t)(128 - nj8) * 64 * 2 + 128;
@@ -87,57 +90,52 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
         tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
         tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0], (uint32_t)tbytes, bar_tma);
     }
-    // stage the spectral columns of both parities.  A unit is one column pair
-    // (re, im) and 8 modes of one parity: one 16-byte core-matrix row per
-    // column and split term.  The units of both parities form one index space;
-    // each thread first loads INV_SLOTS units, then splits and stores them, so
-    // the global loads of all its units are in flight together.
+    // stage the spectral columns of both parities.  A slot is one column pair
+    // q (re, im) and the modes k = 2l, 2l+1 of both parities, i.e. the four
+    // consecutive spectral entries n - m = 4l .. 4l+3: consecutive threads
+    // read consecutive 32-byte pieces of a row, and each stores 4-byte words
+    // (two K-elements) into the padded operand layout, where a warp's stores
+    // for one pair fall in 32 distinct banks.  The filter is in the tables.
+    // Each thread has the loads of INV_SLOTS slots in flight before it splits
+    // and stores them.
     {
-        const int npair = ncp >> 1;
-        const int U0 = npair * (Kp[0] >> 3), U = U0 + (Kq[1] ? npair * (Kp[1] >> 3) : 0);
+        constexpr int INV_SLOTS = 4;
+        const int npair = ncp >> 1, hk = Kp[0] >> 1;   // Kp[0] >= Kp[1]
+        const int nslot = npair * hk;
         const int w0 = A.woff[m];
-        constexpr int INV_SLOTS = 2;
-        for (int base = 0; base < U; base += INV_SLOTS * TCI) {
-            float2 x[INV_SLOTS][8];
-            float fl[INV_SLOTS][8];
+        for (int s0 = tid; s0 < nslot; s0 += INV_SLOTS * TCI) {
+            float2 x[INV_SLOTS][2][2];   // [slot][parity][k - 2l]
 #pragma unroll
-            for (int s = 0; s < INV_SLOTS; s++) {
-                const int u = base + s * TCI + tid;
-                const int p = u >= U0, uu = u - (p ? U0 : 0);
-                const int q = uu % npair, g = uu / npair;
-                const int c = 2 * q;
+            for (int i = 0; i < INV_SLOTS; i++) {
+                const int s = s0 + i * TCI, q = s / hk, l = s - q * hk;
                 bool zv = false;
-                const float2 *row = (u < U && c < nc) ? inv_row(A, group, (c0 + c) >> 1, &zv) : nullptr;
+                const float2 *row = (s < nslot && 2 * q < nc) ? inv_row(A, group, (c0 + 2 * q) >> 1, &zv) : nullptr;
 #pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    const int k = 8 * g + e, nm = 2 * k + p;  // nm = n - m
-                    const bool in = row != nullptr && k < Kq[p];
-                    x[s][e] = in ? __ldg(row + w0 + nm) : make_float2(0.f, 0.f);
-                    fl[s][e] = in ? __ldg(A.filt + m + nm) : 0.f;
-                    if (in && zv && m == 0 && nm == 1) x[s][e].x -= A.plavor;  // dv2uv, legmod.f90:332
-                }
+                for (int p = 0; p < 2; p++)
+#pragma unroll
+                    for (int e = 0; e < 2; e++) {
+                        const int k = 2 * l + e, nm = 2 * k + p;  // nm = n - m
+                        const bool in = row != nullptr && k < Kq[p];
+                        x[i][p][e] = in ? __ldg(row + w0 + nm) : make_float2(0.f, 0.f);
+                        if (in && zv && m == 0 && nm == 1) x[i][p][e].x -= A.plavor;  // dv2uv, legmod.f90:332
+                    }
             }
 #pragma unroll
-            for (int s = 0; s < INV_SLOTS; s++) {
-                const int u = base + s * TCI + tid;
-                if (u >= U) break;
-                const int p = u >= U0, uu = u - (p ? U0 : 0);
-                const int q = uu % npair, g = uu / npair;
-                float xr[8], xi[8];
+            for (int i = 0; i < INV_SLOTS; i++) {
+                const int s = s0 + i * TCI, q = s / hk, l = s - q * hk;
+                if (s >= nslot) break;
 #pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    xr[e] = x[s][e].x * fl[s][e];
-                    xi[e] = x[s][e].y * fl[s][e];
+                for (int p = 0; p < 2; p++) {
+                    if (2 * l >= Kp[p]) continue;   // past this parity's (padded) modes
+                    uint32_t hr, mr, lr, hi, mi, li;
+                    tc::split3x2(x[i][p][0].x, x[i][p][1].x, hr, mr, lr);
+                    tc::split3x2(x[i][p][0].y, x[i][p][1].y, hi, mi, li);
+                    unsigned char *d0 = dat + (p ? 3 * dtile[0] : 0);
+                    const size_t dtp = dtile[p];
+                    const uint32_t o = tc::kpad_off(2 * q, 2 * l, Kp[p] >> 3);  // re row; the im row follows at +16
+                    st_shared4(d0 + o, hr); st_shared4(d0 + dtp + o, mr); st_shared4(d0 + 2 * dtp + o, lr);
+                    st_shared4(d0 + o + 16, hi); st_shared4(d0 + dtp + o + 16, mi); st_shared4(d0 + 2 * dtp + o + 16, li);
                 }
-                const uint32_t o = tc::kmajor_off(2 * q, 8 * g, Kp[p]);  // re row; the im row follows at +16
-                unsigned char *d0 = dat + (p ? 3 * dtile[0] : 0);
-                const size_t dtp = dtile[p];
-                uint4 h, mm, l;
-                tc::split3x8(xr, h, mm, l);
-                st_shared16(d0 + o, h); st_shared16(d0 + dtp + o, mm); st_shared16(d0 + 2 * dtp + o, l);
-                tc::split3x8(xi, h, mm, l);
-                st_shared16(d0 + o + 16, h); st_shared16(d0 + dtp + o + 16, mm);
-                st_shared16(d0 + 2 * dtp + o + 16, l);
             }
         }
     }
@@ -168,15 +166,16 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
                 // large term's chain short bounds that error), summed in the epilogue
                 const uint32_t dm = tmem + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp);
                 const uint32_t dc = tmem + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp);
-                const uint32_t sbo = (uint32_t)(Kp[p] / 8) * 128;
-                const uint64_t da0 = tc::smem_desc(tab + to, 128, sbo), db0 = tc::smem_desc(dat + dd, 128, sbo);
+                const uint32_t sbo = (uint32_t)(Kp[p] / 8) * 128, sbo_b = (uint32_t)(Kp[p] / 8) * tc::kPadLbo;
+                const uint64_t da0 = tc::smem_desc(tab + to, 128, sbo);
+                const uint64_t db0 = tc::smem_desc(dat + dd, tc::kPadLbo, sbo_b);
                 const uint32_t tt = (uint32_t)ttile[p], dt = (uint32_t)dtile[p];
                 for (int kc = 0; kc < Kp[p] / 16; kc++) {
 #pragma unroll
                     for (int pr = 0; pr < 6; pr++)
                         if (pr < nprod)
                             tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
-                                         tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 256), idesc,
+                                         tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 2 * tc::kPadLbo), idesc,
                                          kc > 0 || pr > 1);
                 }
                 to += 3 * ttile[p];
@@ -298,8 +297,8 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
 
 static size_t inv_smem(int nj8, int K, int ncp) {
     const int Kp0 = pad16(kpar(K, 0)), Kp1 = pad16(kpar(K, 1));
-    return 3 * (size_t)nj8 * (Kp0 + Kp1) * 2 + 3 * (size_t)ncp * (Kp0 + Kp1) * 2 + (size_t)(128 - nj8) * 64 * 2 +
-           128 + 80;
+    return 3 * (size_t)nj8 * (Kp0 + Kp1) * 2 + 3 * (size_t)(ncp / 8) * ((Kp0 + Kp1) / 8) * tc::kPadLbo +
+           (size_t)(128 - nj8) * 64 * 2 + 128 + 80;
 }
 
 // ------------------------------------------------------------ forward
@@ -673,11 +672,10 @@ struct TcFwd3Launch {
     TcFwd3Args seg[TC_MAXSEG];
     const int4 *jobs;       // (m, inst | seg << 16, first level, levels | parity << 8)
     int nprod;              // 6: all six products; 3: a0b0, a0b1, a1b0 (and a1b1)
+    int njobs;              // jobs in the list (the persistent kernel walks them)
+    int njmax;              // largest njc over the segments (sizes the persistent kernel's rings)
 };
-template <int NLT> __host__ __device__ constexpr int f3_colbase(int t) {
-    return t == 0 ? 0 : f3_colbase<NLT>(t - 1) + 3 * fwd_ncp<NLT>(t - 1);
-}
-constexpr int F3_NLT = 5;   // levels per job: 3 x (32 + 48 + 48 + 16) = 432 TMEM columns
+constexpr int F3_NLT = 5;   // levels per job; the widest table then has 48 columns (3 x 48 TMEM columns)
 
 // partial outputs of one table's columns: d, t, z, q per level (re, im) and spf
 template <int NLT>
@@ -709,282 +707,378 @@ __device__ __forceinline__ void f3_combine(int t, int c, float v, float (*o)[4][
     }
 }
 
-// load the north and south rows of one staging unit (column pair u % npair of
-// table t, latitude pairs 8 (u / npair) ..+7); zeros outside the job
+// Fourier row of column pair q of table t in a job, or -1 for a padding pair
+template <int NLT>
+__device__ __forceinline__ long long f3_row(const TcFwd3Args &A, int inst, int l0, int nl, bool with_vpp, int t,
+                                            int q) {
+    const int nf = c_fwd_nf[t];
+    if (q >= nf * NLT + ((t == 0) ? 1 : 0)) return -1;
+    if (t == 0 && q == nf * NLT) return with_vpp ? fwd_row(A.L, inst, 7, 0) : -1;
+    const int fi = q / NLT, li = q - fi * NLT;
+    return li < nl ? fwd_row(A.L, inst, c_fwd_fields[t][fi], l0 + li) : -1;
+}
+
+// Operand staging works on slots: a slot is one column pair q (a field level,
+// re and im) and the four latitude pairs j = 4jq .. 4jq+3.  Consecutive threads
+// take consecutive jq of a pair, so a warp's loads read 1 KB of a Fourier row's
+// northern half and of its mirrored southern half, and its 8-byte stores fall
+// in distinct banks of the padded operand layout (one half-warp per wavefront).
+struct F3Slot {
+    float2 n[4], s[4];  // north and south values at latitude pairs j .. j+3
+};
+
 template <int NLT>
 __device__ __forceinline__ void f3_load(const TcFwd3Args &A, int m, int inst, int l0, int nl, bool with_vpp, int t,
-                                        int u, float2 *vn, float2 *vs) {
-    const int nf = c_fwd_nf[t];
-    const int npair = fwd_ncp<NLT>(t) >> 1, ng = A.njc >> 3;
-    const int nreal = nf * NLT + ((t == 0) ? 1 : 0);
-    const int q = u % npair, g = u / npair;
-    long long rb = -1;
-    if (g < ng && q < nreal) {
-        if (t == 0 && q == nf * NLT) { if (with_vpp) rb = fwd_row(A.L, inst, 7, 0); }
-        else {
-            const int fi = q / NLT, li = q - fi * NLT;
-            if (li < nl) rb = fwd_row(A.L, inst, c_fwd_fields[t][fi], l0 + li);
-        }
-    }
+                                        int sl, F3Slot &v) {
+    const int hj = A.njc >> 2;
+    const int q = sl / hj, jq = sl - q * hj;
 #pragma unroll
-    for (int e = 0; e < 8; e++) vn[e] = vs[e] = make_float2(0.f, 0.f);
+    for (int e = 0; e < 4; e++) v.n[e] = v.s[e] = make_float2(0.f, 0.f);
+    if (q >= (fwd_ncp<NLT>(t) >> 1)) return;
+    const long long rb = f3_row<NLT>(A, inst, l0, nl, with_vpp, t, q);
     if (rb < 0) return;
-    const int nlat = A.nlat, j0 = 8 * g;
+    const int j = 4 * jq, nlat = A.nlat, nlath = A.nlath;
     const float2 *wr = A.W + (size_t)m * A.nrows + (size_t)rb * nlat;
-    if (j0 + 8 <= A.nlath) {
-        // rows j0..j0+7 north, and nlat-8-j0..nlat-1-j0 south (reversed)
-        const float4 *pn = reinterpret_cast<const float4 *>(wr + j0);
-        const float4 *ps = reinterpret_cast<const float4 *>(wr + nlat - 8 - j0);
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const float4 x = __ldg(pn + i), y = __ldg(ps + i);
-            vn[2 * i] = make_float2(x.x, x.y);
-            vn[2 * i + 1] = make_float2(x.z, x.w);
-            vs[7 - 2 * i] = make_float2(y.x, y.y);
-            vs[6 - 2 * i] = make_float2(y.z, y.w);
-        }
+    if (j + 4 <= nlath) {
+        // north rows j .. j+3; south rows nlat-4-j .. nlat-1-j (pairs j+3 .. j)
+        const float4 x0 = __ldg(reinterpret_cast<const float4 *>(wr + j));
+        const float4 x1 = __ldg(reinterpret_cast<const float4 *>(wr + j + 2));
+        const float4 y0 = __ldg(reinterpret_cast<const float4 *>(wr + nlat - 4 - j));
+        const float4 y1 = __ldg(reinterpret_cast<const float4 *>(wr + nlat - 2 - j));
+        v.n[0] = make_float2(x0.x, x0.y); v.n[1] = make_float2(x0.z, x0.w);
+        v.n[2] = make_float2(x1.x, x1.y); v.n[3] = make_float2(x1.z, x1.w);
+        v.s[3] = make_float2(y0.x, y0.y); v.s[2] = make_float2(y0.z, y0.w);
+        v.s[1] = make_float2(y1.x, y1.y); v.s[0] = make_float2(y1.z, y1.w);
     } else {
 #pragma unroll
-        for (int e = 0; e < 8; e++)
-            if (j0 + e < A.nlath) {
-                vn[e] = __ldg(wr + j0 + e);
-                vs[e] = __ldg(wr + nlat - 1 - j0 - e);
+        for (int e = 0; e < 4; e++)
+            if (j + e < nlath) {
+                v.n[e] = __ldg(wr + j + e);
+                v.s[e] = __ldg(wr + nlat - 1 - j - e);
             }
     }
 }
 
-// fold a loaded unit for parity p, split it into three BF16 terms and store
-// the re and im core-matrix rows of every term
+// fold a slot for parity p, split it into three BF16 terms and store the re
+// and im words of every term
 template <int NLT>
-__device__ __forceinline__ void f3_store(int t, int p, int u, int njc, unsigned char *bt, const float2 *vn,
-                                         const float2 *vs) {
-    const int ncp = fwd_ncp<NLT>(t), npair = ncp >> 1;
-    const int q = u % npair, g = u / npair;
+__device__ __forceinline__ void f3_store(int t, int p, int sl, int njc, unsigned char *bt, const F3Slot &v) {
+    const int hj = njc >> 2, ngk = njc >> 3;
+    const int q = sl / hj, jq = sl - q * hj;
+    const int ncp = fwd_ncp<NLT>(t);
+    if (q >= (ncp >> 1)) return;
     const bool diff = (t != 1) ? (p == 1) : (p == 0);
-    float xr[8], xi[8];
+    float xr[4], xi[4];
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-        xr[e] = diff ? vn[e].x - vs[e].x : vn[e].x + vs[e].x;
-        xi[e] = diff ? vn[e].y - vs[e].y : vn[e].y + vs[e].y;
+    for (int e = 0; e < 4; e++) {
+        xr[e] = diff ? v.n[e].x - v.s[e].x : v.n[e].x + v.s[e].x;
+        xi[e] = diff ? v.n[e].y - v.s[e].y : v.n[e].y + v.s[e].y;
     }
-    const uint32_t dt = (uint32_t)ncp * njc * 2;
-    const uint32_t o = tc::kmajor_off(2 * q, 8 * g, njc);
-    uint4 h, mm, l;
-    tc::split3x8(xr, h, mm, l);
-    st_shared16(bt + o, h); st_shared16(bt + dt + o, mm); st_shared16(bt + 2 * dt + o, l);
-    tc::split3x8(xi, h, mm, l);
-    st_shared16(bt + o + 16, h); st_shared16(bt + dt + o + 16, mm); st_shared16(bt + 2 * dt + o + 16, l);
+    uint2 hr, mr, lr, hi, mi, li;
+    tc::split3x2(xr[0], xr[1], hr.x, mr.x, lr.x);
+    tc::split3x2(xr[2], xr[3], hr.y, mr.y, lr.y);
+    tc::split3x2(xi[0], xi[1], hi.x, mi.x, li.x);
+    tc::split3x2(xi[2], xi[3], hi.y, mi.y, li.y);
+    const uint32_t dt = (uint32_t)(ncp >> 3) * ngk * tc::kPadLbo;  // one split term
+    const uint32_t o = tc::kpad_off(2 * q, 4 * jq, ngk);            // re row; the im row follows at +16
+    st_shared8(bt + o, hr); st_shared8(bt + dt + o, mr); st_shared8(bt + 2 * dt + o, lr);
+    st_shared8(bt + o + 16, hi); st_shared8(bt + dt + o + 16, mi); st_shared8(bt + 2 * dt + o + 16, li);
 }
 
-// sum the split blocks of table T's accumulator columns for this thread's TMEM
-// row and fold them into the partial outputs
+// ------------------------------------------------------------ forward, pipelined
+// Persistent form of the stacked-split forward kernel.  One CTA per SM walks
+// the jobs blockIdx.x, blockIdx.x + gridDim.x, ... of the launch; a job's four
+// tables are four tiles, and tiles flow through rings so that different
+// warps work on different tiles at once:
+//   warp 1 (one lane)       copies table blocks into a 2-slot ring
+//   warps 2-3, 8-15         stage the folded, split operands into a 2-slot ring
+//   warp 0 (one lane)       issues the MMAs of a tile into one of 3 TMEM slots
+//   warps 4-7               drain TMEM (lane quarter = warp - 4), accumulate a
+//                           job's outputs over its tiles and store them
+// Each ring slot has a full and an empty mbarrier; every wait is bounded, and
+// a wait that times out raises an abort flag that ends every role's loop.
+constexpr int FP_THREADS = 512;
+constexpr int FP_NST = 320;              // staging threads
+constexpr int FP_ACC = 144;              // TMEM columns of a slot: 3 x the widest table's columns
+constexpr int FP_SLOTS = 2;              // staging slots per thread kept in flight for one tile
+
+struct FpLayout {
+    uint32_t tb, ob;                     // bytes of a table slot and of an operand slot
+    uint32_t op, e, bars;                // offsets of the operand ring, the exchange area, the barriers
+};
+__host__ __device__ inline FpLayout fp_layout(int njmax) {
+    FpLayout L;
+    L.tb = 8u * 64u * (uint32_t)njmax;
+    L.ob = 3u * (48u / 8u) * (uint32_t)(njmax / 8) * tc::kPadLbo;
+    L.op = 2 * L.tb + 128 * 32 * 2;       // rows >= 2R of a table tile read up to 8 KB past it
+    L.e = L.op + 2 * L.ob;
+    L.bars = L.e + 128 * (F3_NLT * 8 + 2) * 4;
+    L.bars = (L.bars + 15) & ~15u;
+    return L;
+}
+static size_t fpipe_smem(int njmax) { return fp_layout(njmax).bars + 32 * 8; }
+
+// bounded wait that also gives up as soon as another role has aborted
+__device__ __forceinline__ bool fp_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    const uint32_t addr = tc::smem_u32(bar);
+    for (uint32_t i = 0; i < tc::kSpinLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 255) == 255 && *abort) return false;
+    }
+    *abort = 1;
+    return false;
+}
+
+// barrier of the 128 epilogue threads on an mbarrier (count 128), bounded like every wait
+__device__ __forceinline__ bool fp_epi_sync(uint64_t *bar, uint32_t &phase, volatile int *abort) {
+    tc::mbar_arrive(bar);
+    const bool ok = fp_wait(bar, phase, abort);
+    phase ^= 1;
+    return ok;
+}
+
+// one TMEM slot holds table T's split blocks at columns 0, ncp, 2 ncp; drained
+// 8 columns at a time (fewer live registers than the 16-wide loads)
 template <int NLT, int T>
-__device__ __forceinline__ void f3_drain(uint32_t taddr, int nprod, float (*o)[4][2], float *ov) {
+__device__ __forceinline__ void fp_drain_t(uint32_t X, int nprod, float (*o)[4][2], float *ov) {
     constexpr int ncp = fwd_ncp<NLT>(T);
-    const uint32_t X = taddr + (uint32_t)f3_colbase<NLT>(T);
 #pragma unroll
-    for (int c0 = 0; c0 < ncp; c0 += 16) {
-        uint32_t x0[16], x1[16], x2[16];
-        tc::tmem_ld16_nw(X + c0, x0);
-        tc::tmem_ld16_nw(X + ncp + c0, x1);
-        if (nprod == 6) tc::tmem_ld16_nw(X + 2 * ncp + c0, x2);
+    for (int c0 = 0; c0 < ncp; c0 += 8) {
+        uint32_t x0[8], x1[8], x2[8];
+        tc::tmem_ld8_nw(X + c0, x0);
+        tc::tmem_ld8_nw(X + ncp + c0, x1);
+        if (nprod == 6) tc::tmem_ld8_nw(X + 2 * ncp + c0, x2);
         tc::tmem_wait_ld();
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
+        for (int i = 0; i < 8; i++) {
             float v = __uint_as_float(x0[i]) + __uint_as_float(x1[i]);
             if (nprod == 6) v += __uint_as_float(x2[i]);
             f3_combine<NLT>(T, c0 + i, v, o, ov);
         }
     }
 }
-
-// 16 warps: warp 0 issues copies and MMAs, warps 1-15 stage operands (the
-// staging loads are latency-bound, so more warps keep more of them in flight),
-// warps 0-3 drain TMEM
-constexpr int TCT3 = 512;
-
 template <int NLT>
-__global__ void __launch_bounds__(TCT3) k_tc_forward3(const __grid_constant__ TcFwd3Launch P) {
-    extern __shared__ __align__(128) unsigned char sm[];
-    const int4 jb = P.jobs[blockIdx.x];
-    const TcFwd3Args &A = P.seg[jb.y >> 16];
-    const int nprod = P.nprod;
-    const int m = jb.x, inst = jb.y & 0xffff, l0 = jb.z, nl = jb.w & 0xff, p = jb.w >> 8;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3;
-    const int K = A.ntp1 - m;
-    const int Kq = kpar(K, p), R = pad8(Kq);
-    const int njc = A.njc, L = A.L;
-    const bool with_vpp = (l0 == 0);
-    const uint32_t tbytes = (uint32_t)8 * R * njc;   // one (m, table, parity) block
-    const uint32_t tbuf = (uint32_t)8 * 64 * njc;    // buffer for the widest block
-    unsigned char *tabb[2] = {sm, sm + tbuf};
-    // rows >= 2R of the M=128 tiles read past a block (their TMEM lanes are unused)
-    unsigned char *dat = sm + 2 * tbuf + 128 * 32 * 2;
-    size_t doffs[4], dbytes = 0;
-    for (int t = 0; t < 4; t++) { doffs[t] = dbytes; dbytes += 3 * (size_t)fwd_ncp<NLT>(t) * njc * 2; }
-    // the epilogue's partial outputs reuse the table and operand space; the
-    // barriers lie past both
-    constexpr int NO = NLT * 8 + 2;
-    constexpr size_t ebytes = 4 * 128 * NO * sizeof(float);
-    unsigned char *tail = (size_t)(dat + dbytes - sm) > ebytes ? dat + dbytes : sm + ebytes;
-    uint64_t *bars = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
-    uint64_t *bar_tma = bars;       // [2] table buffer b landed
-    uint64_t *bar_mma = bars + 2;   // [2] MMAs reading table buffer b completed
-    uint64_t *bar_done = bars + 4;
-    uint64_t *bar_stage = bars + 5; // [4] operands of table t staged (warps 1-15 arrive)
-    uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 9);
-    if (warp == 0) tc::tmem_alloc(slot, 512);
-    if (tid == 0) {
-        for (int i = 0; i < 5; i++) tc::mbar_init(bars + i, 1);
-        for (int t = 0; t < 4; t++) tc::mbar_init(bar_stage + t, TCT3 - 32);
-        tc::mbar_fence_init();
-        for (int t = 0; t < 2; t++) {
-            tc::mbar_arrive_expect_tx(bar_tma + t, tbytes);
-            tc::bulk_g2s(tabb[t], A.tab + A.off[(m * 4 + t) * 2 + p], tbytes, bar_tma + t);
-        }
-    }
-    tc::fence_before_sync();
-    __syncthreads();  // barriers initialised, TMEM address published
-    tc::fence_after_sync();
-    const uint32_t tmem = *slot;
-    bool ok = true;
-    // warps 1-15 stage the folded columns each table needs for this parity,
-    // table by table, while warp 0 issues the MMAs of every table already
-    // staged.  P-type tables (qc, qm, qq) take N+S on even n-m and N-S on odd,
-    // Q-type (qe) the reverse.  A unit (column pair, 8 latitude pairs) of the
-    // next table is loaded before the current one is split and stored, so the
-    // loads of successive tables overlap.
-    if (warp != 0) {
-        const int stid = tid - 32;
-        float2 vn[8], vs[8];
-        f3_load<NLT>(A, m, inst, l0, nl, with_vpp, 0, stid, vn, vs);
-        for (int t = 0; t < 4; t++) {
-            const int nunit = (fwd_ncp<NLT>(t) >> 1) * (njc >> 3);
-            float2 wn[8], ws[8];
-            if (t + 1 < 4) f3_load<NLT>(A, m, inst, l0, nl, with_vpp, t + 1, stid, wn, ws);
-            if (stid < nunit) f3_store<NLT>(t, p, stid, njc, dat + doffs[t], vn, vs);
-            // more units than staging threads (not at NLAT <= 192, where every table has fewer)
-            for (int u = stid + (TCT3 - 32); u < nunit; u += TCT3 - 32) {
-                f3_load<NLT>(A, m, inst, l0, nl, with_vpp, t, u, vn, vs);
-                f3_store<NLT>(t, p, u, njc, dat + doffs[t], vn, vs);
-            }
-            tc::fence_proxy_async();  // these stores feed the tensor cores
-            tc::mbar_arrive(bar_stage + t);
-#pragma unroll
-            for (int e = 0; e < 8; e++) { vn[e] = wn[e]; vs[e] = ws[e]; }
-        }
-    }
-    if (tid == 0) {
-        const uint32_t sbo_b = (uint32_t)(njc / 8) * 128;
-        for (int t = 0; t < 4 && ok; t++) {
-            const int b = t & 1;
-            ok = tc::mbar_wait(bar_stage + t, 0) && tc::mbar_wait(bar_tma + b, (t >> 1) & 1);
-            if (!ok) break;
-            tc::fence_after_sync();
-            const int ncp = fwd_ncp<NLT>(t);
-            const uint32_t idesc1 = tc::idesc_bf16(128, (nprod == 6 ? 3 : 2) * ncp);
-            const uint32_t idesc2 = tc::idesc_bf16(128, ncp);
-            const uint32_t X = tmem + (uint32_t)f3_colbase<NLT>(t);
-            const uint64_t db = tc::smem_desc(dat + doffs[t], 128, sbo_b);
-            uint32_t jo = 0;
-            for (int j0 = 0; j0 < njc; j0 += 32) {
-                const int jw = njc - j0 < 32 ? njc - j0 : 32;
-                const uint32_t tt = (uint32_t)2 * R * jw * 2;   // one stacked tile
-                const uint64_t da1 = tc::smem_desc(tabb[b] + jo, 128, (uint32_t)(jw / 8) * 128);
-                const uint64_t da2 = tc::desc_add(da1, tt);
-                for (int kc = 0; kc < jw / 16; kc++) {
-                    const uint64_t dbk = tc::desc_add(db, (j0 / 8) * 128 + kc * 256);
-                    tc::mma_bf16(X, tc::desc_add(da1, kc * 256), dbk, idesc1, j0 > 0 || kc > 0);
-                    if (nprod == 6) tc::mma_bf16(X, tc::desc_add(da2, kc * 256), dbk, idesc2, true);
-                }
-                jo += 2 * tt;
-            }
-            if (t <= 1) tc::mma_commit(bar_mma + b);
-            // refill the other buffer with table t+1 once table t-1's MMAs have read it
-            if (t >= 1 && t + 1 < 4) {
-                const int bn = (t + 1) & 1;
-                ok = tc::mbar_wait(bar_mma + bn, 0);
-                if (!ok) break;
-                tc::mbar_arrive_expect_tx(bar_tma + bn, tbytes);
-                tc::bulk_g2s(tabb[bn], A.tab + A.off[(m * 4 + t + 1) * 2 + p], tbytes, bar_tma + bn);
-            }
-        }
-        if (ok) tc::mma_commit(bar_done);
-        if (!ok) atomicExch(&g_tc_error, 5);
-    }
-    __syncthreads();
-    ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, 0));  // warp-uniform for the .sync.aligned TMEM loads
-    if (!ok && lane == 0) atomicExch(&g_tc_error, 6);
-    tc::fence_after_sync();
-    // epilogue: warp w drains table w / 4 for TMEM lane quarter w % 4.  Row r
-    // holds mode r (r < R) or corrections of mode r - R (R <= r < 2R); every
-    // (table, row) hands its partial outputs to shared memory, and the sums
-    // over tables and both rows of a mode are formed there.
-    float *E = reinterpret_cast<float *>(sm);   // [4][128][NO]; tables and operands are dead now
-    const int r = quarter * 32 + lane;
-    const int gw = warp >> 2;
-    if (ok && quarter * 32 < 2 * R) {           // warp-uniform (ok is)
-        const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
-        float o[NLT][4][2], ov[2] = {0.f, 0.f};
-#pragma unroll
-        for (int li = 0; li < NLT; li++)
-#pragma unroll
-            for (int k = 0; k < 4; k++) o[li][k][0] = o[li][k][1] = 0.f;
-        if (gw == 0) f3_drain<NLT, 0>(tmem + lane_addr, nprod, o, ov);
-        else if (gw == 1) f3_drain<NLT, 1>(tmem + lane_addr, nprod, o, ov);
-        else if (gw == 2) f3_drain<NLT, 2>(tmem + lane_addr, nprod, o, ov);
-        else f3_drain<NLT, 3>(tmem + lane_addr, nprod, o, ov);
-        if (r < 2 * R) {
-            float *e = E + (size_t)(gw * 128 + r) * NO;
-#pragma unroll
-            for (int li = 0; li < NLT; li++)
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    e[(li * 4 + k) * 2] = o[li][k][0];
-                    e[(li * 4 + k) * 2 + 1] = o[li][k][1];
-                }
-            e[NLT * 8] = ov[0];
-            e[NLT * 8 + 1] = ov[1];
-        }
-    }
-    __syncthreads();
-    if (ok) {
-        // outputs: Kq modes x (4 fields x NLT levels + spf); consecutive threads take consecutive modes
-        const int nout = 4 * NLT + 1, nfo = 4 * L + 1;
-        const size_t wb = (size_t)A.woff[m];
-        for (int idx = tid; idx < Kq * nout; idx += TCT3) {
-            const int oi = idx / Kq, rr = idx - oi * Kq;
-            size_t fr;                                   // output field row
-            if (oi < 4 * NLT) {
-                const int li = oi >> 2, kk = oi & 3;
-                if (li >= nl) continue;
-                fr = (size_t)inst * nfo + kk * L + l0 + li;
-            } else {
-                if (!with_vpp) continue;
-                fr = (size_t)inst * nfo + 4 * L;
-            }
-            float sr = 0.f, si = 0.f;
-#pragma unroll
-            for (int g = 0; g < 4; g++) {
-                const float *e0 = E + (size_t)(g * 128 + rr) * NO + 2 * oi;
-                const float *e1 = E + (size_t)(g * 128 + R + rr) * NO + 2 * oi;
-                sr += e0[0] + e1[0];
-                si += e0[1] + e1[1];
-            }
-            const int k = 2 * rr + p;                    // n - m
-            const float fl = A.filt[m + k];
-            reinterpret_cast<float2 *>(A.spout + fr * A.nrsp)[wb + k] = make_float2(sr * fl, si * fl);
-        }
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 512);
+__device__ __forceinline__ void fp_drain(int t, uint32_t X, int nprod, float (*o)[4][2], float *ov) {
+    if (t == 0) fp_drain_t<NLT, 0>(X, nprod, o, ov);
+    else if (t == 1) fp_drain_t<NLT, 1>(X, nprod, o, ov);
+    else if (t == 2) fp_drain_t<NLT, 2>(X, nprod, o, ov);
+    else fp_drain_t<NLT, 3>(X, nprod, o, ov);
 }
 
-static size_t fwd3_smem(int njc, int nlt) {
-    size_t d = 0;
-    for (int t = 0; t < 4; t++) d += 3 * (size_t)fwd_ncp_rt(nlt, t) * njc * 2;
-    const size_t ops = 2 * (size_t)8 * 64 * njc + 128 * 32 * 2 + d;
-    const size_t ebytes = 4 * 128 * (size_t)(nlt * 8 + 2) * sizeof(float);
-    return std::max(ops, ebytes) + 128;
+template <int NLT>
+__global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_constant__ TcFwd3Launch P) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const FpLayout LY = fp_layout(P.njmax);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned char *tabr = sm, *opr = sm + LY.op;
+    float *E = reinterpret_cast<float *>(sm + LY.e);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + LY.bars);
+    uint64_t *tab_full = bars, *tab_empty = bars + 2, *op_full = bars + 4, *op_empty = bars + 6;
+    uint64_t *acc_full = bars + 8, *acc_empty = bars + 11, *ep_bar = bars + 14;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 15);
+    volatile int *abort = reinterpret_cast<volatile int *>(bars + 16);
+    const int nprod = P.nprod;
+    const int njobs = P.njobs;
+    // tiles of this CTA: jobs blockIdx.x + k gridDim.x, four tables each
+    const int mine = njobs > (int)blockIdx.x ? (njobs - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int ntile = 4 * mine;
+    if (warp == 0) tc::tmem_alloc(slot, 512);
+    if (tid == 0) {
+        for (int i = 0; i < 2; i++) {
+            tc::mbar_init(tab_full + i, 1);
+            tc::mbar_init(tab_empty + i, 1);
+            tc::mbar_init(op_full + i, FP_NST);
+            tc::mbar_init(op_empty + i, 1);
+        }
+        for (int i = 0; i < 3; i++) {
+            tc::mbar_init(acc_full + i, 1);
+            tc::mbar_init(acc_empty + i, 4);
+        }
+        tc::mbar_init(ep_bar, 128);
+        *abort = 0;
+        tc::mbar_fence_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+
+    if (warp == 1) {
+        // ---------------------------------------------------------- table copies
+        if (lane == 0) {
+            int issued[2] = {0, 0};
+            for (int i = 0; i < ntile; i++) {
+                const int b = i & 1, u = i >> 1;
+                if (!fp_wait(tab_empty + b, (u & 1) ^ 1, abort)) break;
+                const int4 jb = P.jobs[blockIdx.x + (i >> 2) * gridDim.x];
+                const TcFwd3Args &A = P.seg[jb.y >> 16];
+                const int m = jb.x, p = jb.w >> 8, t = i & 3;
+                const uint32_t tbytes = 8u * (uint32_t)pad8(kpar(A.ntp1 - m, p)) * (uint32_t)A.njc;
+                tc::mbar_arrive_expect_tx(tab_full + b, tbytes);
+                tc::bulk_g2s(tabr + b * LY.tb, A.tab + A.off[(m * 4 + t) * 2 + p], tbytes, tab_full + b);
+                issued[b] = u + 1;
+            }
+            if (*abort) {
+                // copies still in flight land before the block exits
+                for (int b = 0; b < 2; b++)
+                    if (issued[b]) tc::mbar_wait(tab_full + b, (issued[b] - 1) & 1);
+            }
+        }
+    } else if (warp == 0) {
+        // ---------------------------------------------------------------- MMAs
+        if (lane == 0) {
+            for (int i = 0; i < ntile; i++) {
+                const int b = i & 1, u = i >> 1, a = i % 3, ua = i / 3;
+                if (!fp_wait(tab_full + b, u & 1, abort) || !fp_wait(op_full + b, u & 1, abort) ||
+                    !fp_wait(acc_empty + a, (ua & 1) ^ 1, abort))
+                    break;
+                tc::fence_after_sync();
+                const int4 jb = P.jobs[blockIdx.x + (i >> 2) * gridDim.x];
+                const TcFwd3Args &A = P.seg[jb.y >> 16];
+                const int m = jb.x, p = jb.w >> 8, t = i & 3;
+                const int R = pad8(kpar(A.ntp1 - m, p)), njc = A.njc;
+                const int ncp = fwd_ncp<NLT>(t);
+                const uint32_t idesc1 = tc::idesc_bf16(128, (nprod == 6 ? 3 : 2) * ncp);
+                const uint32_t idesc2 = tc::idesc_bf16(128, ncp);
+                const uint32_t X = tmem + (uint32_t)(a * FP_ACC);
+                const uint64_t db = tc::smem_desc(opr + b * LY.ob, tc::kPadLbo, (uint32_t)(njc / 8) * tc::kPadLbo);
+                unsigned char *tb = tabr + b * LY.tb;
+                uint32_t jo = 0;
+                for (int j0 = 0; j0 < njc; j0 += 32) {
+                    const int jw = njc - j0 < 32 ? njc - j0 : 32;
+                    const uint32_t tt = (uint32_t)2 * R * jw * 2;   // one stacked tile
+                    const uint64_t da1 = tc::smem_desc(tb + jo, 128, (uint32_t)(jw / 8) * 128);
+                    const uint64_t da2 = tc::desc_add(da1, tt);
+                    for (int kc = 0; kc < jw / 16; kc++) {
+                        const uint64_t dbk = tc::desc_add(db, (uint32_t)(j0 / 8 + 2 * kc) * tc::kPadLbo);
+                        tc::mma_bf16(X, tc::desc_add(da1, kc * 256), dbk, idesc1, j0 > 0 || kc > 0);
+                        if (nprod == 6) tc::mma_bf16(X, tc::desc_add(da2, kc * 256), dbk, idesc2, true);
+                    }
+                    jo += 2 * tt;
+                }
+                tc::mma_commit(tab_empty + b);
+                tc::mma_commit(op_empty + b);
+                tc::mma_commit(acc_full + a);
+            }
+        }
+    } else if (warp >= 4 && warp < 8) {
+        // ------------------------------------------------------------ epilogue
+        const int quarter = warp - 4, r = quarter * 32 + lane;
+        const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+        constexpr int NO = NLT * 8 + 2;
+        float o[NLT][4][2], ov[2];
+        bool ok = true;
+        uint32_t ep_phase = 0;
+        for (int i = 0; i < ntile && ok; i++) {
+            const int a = i % 3, ua = i / 3, t = i & 3;
+            const int4 jb = P.jobs[blockIdx.x + (i >> 2) * gridDim.x];
+            const TcFwd3Args &A = P.seg[jb.y >> 16];
+            const int m = jb.x, inst = jb.y & 0xffff, l0 = jb.z, nl = jb.w & 0xff, p = jb.w >> 8;
+            const int Kq = kpar(A.ntp1 - m, p), R = pad8(Kq);
+            if (t == 0) {
+#pragma unroll
+                for (int li = 0; li < NLT; li++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) o[li][k][0] = o[li][k][1] = 0.f;
+                ov[0] = ov[1] = 0.f;
+            }
+            ok = __all_sync(0xffffffffu, fp_wait(acc_full + a, ua & 1, abort));   // warp-uniform
+            if (!ok) break;
+            tc::fence_after_sync();
+            if (quarter * 32 < 2 * R) fp_drain<NLT>(t, tmem + lane_addr + (uint32_t)(a * FP_ACC), nprod, o, ov);
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(acc_empty + a);
+            if (t < 3) continue;
+            // the job's four tables are in: rows R..2R-1 hand their corrections to rows 0..R-1
+            if (r >= R && r < 2 * R) {
+                float *e = E + (size_t)(r - R) * NO;
+#pragma unroll
+                for (int li = 0; li < NLT; li++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        e[(li * 4 + k) * 2] = o[li][k][0];
+                        e[(li * 4 + k) * 2 + 1] = o[li][k][1];
+                    }
+                e[NLT * 8] = ov[0];
+                e[NLT * 8 + 1] = ov[1];
+            }
+            ok = __all_sync(0xffffffffu, fp_epi_sync(ep_bar, ep_phase, abort));
+            if (!ok) break;
+            if (r < Kq) {
+                const float *e = E + (size_t)r * NO;
+                const int L = A.L, nfo = 4 * L + 1, k = 2 * r + p;   // k = n - m
+                const float fl = A.filt[m + k];
+                const size_t wo = (size_t)A.woff[m] + k;
+#pragma unroll
+                for (int li = 0; li < NLT; li++) {
+                    if (li >= nl) break;
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) {
+                        float2 *dst = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + kk * L + l0 + li) * A.nrsp);
+                        dst[wo] = make_float2((o[li][kk][0] + e[(li * 4 + kk) * 2]) * fl,
+                                              (o[li][kk][1] + e[(li * 4 + kk) * 2 + 1]) * fl);
+                    }
+                }
+                if (l0 == 0) {
+                    float2 *dst = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + 4 * L) * A.nrsp);
+                    dst[wo] = make_float2((ov[0] + e[NLT * 8]) * fl, (ov[1] + e[NLT * 8 + 1]) * fl);
+                }
+            }
+            ok = __all_sync(0xffffffffu, fp_epi_sync(ep_bar, ep_phase, abort));   // E is free again
+        }
+    } else {
+        // ------------------------------------------------------------- staging
+        const int stid = (warp < 4 ? warp - 2 : warp - 6) * 32 + lane;
+        F3Slot cur[FP_SLOTS], nxt[FP_SLOTS];
+        if (ntile > 0) {
+            const int4 jb = P.jobs[blockIdx.x];
+            const TcFwd3Args &A = P.seg[jb.y >> 16];
+#pragma unroll
+            for (int k = 0; k < FP_SLOTS; k++)
+                f3_load<NLT>(A, jb.x, jb.y & 0xffff, jb.z, jb.w & 0xff, jb.z == 0, 0, stid + k * FP_NST, cur[k]);
+        }
+        for (int i = 0; i < ntile; i++) {
+            const int b = i & 1, u = i >> 1, t = i & 3;
+            const int4 jb = P.jobs[blockIdx.x + (i >> 2) * gridDim.x];
+            const TcFwd3Args &A = P.seg[jb.y >> 16];
+            const int njc = A.njc, p = jb.w >> 8;
+            if (i + 1 < ntile) {
+                // the next tile's loads are in flight while this one is stored
+                const int4 jn = P.jobs[blockIdx.x + ((i + 1) >> 2) * gridDim.x];
+                const TcFwd3Args &An = P.seg[jn.y >> 16];
+#pragma unroll
+                for (int k = 0; k < FP_SLOTS; k++)
+                    f3_load<NLT>(An, jn.x, jn.y & 0xffff, jn.z, jn.w & 0xff, jn.z == 0, (i + 1) & 3, stid + k * FP_NST,
+                                 nxt[k]);
+            }
+            if (!fp_wait(op_empty + b, (u & 1) ^ 1, abort)) break;
+            unsigned char *bt = opr + b * LY.ob;
+            const int nslot = (fwd_ncp<NLT>(t) >> 1) * (njc >> 2);
+#pragma unroll
+            for (int k = 0; k < FP_SLOTS; k++)
+                if (stid + k * FP_NST < nslot) f3_store<NLT>(t, p, stid + k * FP_NST, njc, bt, cur[k]);
+            for (int s = stid + FP_SLOTS * FP_NST; s < nslot; s += FP_NST) {   // beyond the slots in flight
+                F3Slot v;
+                f3_load<NLT>(A, jb.x, jb.y & 0xffff, jb.z, jb.w & 0xff, jb.z == 0, t, s, v);
+                f3_store<NLT>(t, p, s, njc, bt, v);
+            }
+            tc::fence_proxy_async();   // these stores feed the tensor cores
+            tc::mbar_arrive(op_full + b);
+#pragma unroll
+            for (int k = 0; k < FP_SLOTS; k++) cur[k] = nxt[k];
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (*abort && tid == 0) atomicExch(&g_tc_error, 7);
+    if (warp == 0) tc::tmem_dealloc(tmem, 512);
 }

@@ -156,6 +156,28 @@ __host__ __device__ __forceinline__ uint32_t kmajor_off(int r, int k, int kt) {
     return (uint32_t)(((r >> 3) * (kt >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
+// The same layout with the K-adjacent core matrices 144 bytes apart (16 bytes
+// of padding after each): a warp storing one 4-byte word (2 K-elements) per
+// lane for 32 consecutive K-pairs of one row then touches 32 distinct banks.
+// ngk = K-groups of 8 in a row group; the row-group stride (SBO) is ngk * 144.
+constexpr uint32_t kPadLbo = 144;
+__host__ __device__ __forceinline__ uint32_t kpad_off(int r, int k, int ngk) {
+    return (uint32_t)(((r >> 3) * ngk + (k >> 3)) * kPadLbo + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// three-term BF16 split of two values into BF16x2 words (a in the low half)
+__device__ __forceinline__ void split3x2(float a, float b, uint32_t &h, uint32_t &m, uint32_t &l) {
+    const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+    const float2 hf = __bfloat1622float2(h2);
+    const float r0 = a - hf.x, r1 = b - hf.y;
+    const __nv_bfloat162 m2 = __floats2bfloat162_rn(r0, r1);
+    const float2 mf = __bfloat1622float2(m2);
+    const __nv_bfloat162 l2 = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+    h = *reinterpret_cast<const uint32_t *>(&h2);
+    m = *reinterpret_cast<const uint32_t *>(&m2);
+    l = *reinterpret_cast<const uint32_t *>(&l2);
+}
+
 // three-term BF16 split: x ~= h + m + l with |x - (h+m+l)| <= 2^-24 |x| (normal range)
 __device__ __forceinline__ void split3(float x, __nv_bfloat16 &h, __nv_bfloat16 &m, __nv_bfloat16 &l) {
     h = __float2bfloat16_rn(x);
