@@ -311,6 +311,9 @@ exotx_status tc_available() { return EXOTX_OK; }
 // forward groups: 0 = qc,qe,qm,qq on the mktend/qtend/fc2sp inputs (one level slab)
 // job = (m, group, first column, number of columns)
 static constexpr size_t TC_SMEM_MAX = 227 * 1024;
+// the persistent kernel sizes its grid to the SM count and allocates all 512
+// TMEM columns, so it asks for enough shared memory that two CTAs never share an SM
+static constexpr size_t kPersistSmemMin = 116 * 1024;
 
 #include "legendre_tc_kernels.cuh"
 
@@ -344,7 +347,7 @@ static exotx_status launch_fwd_pipe(TcFwd3Launch &P, int njobs, int njmax, cudaS
         EXOTX_CUDA(cudaGetDevice(&dev));
         EXOTX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     }
-    const size_t smem = fpipe_smem(njmax);
+    const size_t smem = std::max(fpipe_smem(njmax), kPersistSmemMin);   // one CTA per SM
     if (smem > TC_SMEM_MAX) return EXOTX_BAD_DIM;
     P.njobs = njobs;
     P.njmax = njmax;
