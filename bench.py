@@ -63,8 +63,8 @@ def fft_bytes(nlat, nlev, half, esz):
 # DRAM bytes per launch of the dominant kernel from one ncu capture (dram__bytes_read.sum
 # + dram__bytes_write.sum), keyed by (kernel, workload); the summary with its command is
 # in profiles/.
-# k_tc_forward3 on one T127 L20 instance, one cold-cache ncu capture: 63.8 MB read + 3.0 MB written
-NCU_TRAFFIC = {("tc_forward", WORKLOAD): 63.769344e6 + 3.000832e6}
+# k_tc_forward_pipe on one T127 L20 instance, one cold-cache ncu capture: 63.8 MB read + 0.86 MB written
+NCU_TRAFFIC = {("tc_forward", WORKLOAD): 63.786752e6 + 0.864256e6}
 
 
 def args_():
