@@ -297,6 +297,67 @@ __device__ __forceinline__ const cpx<T> *passes_ct(cpx<T> *src, cpx<T> *dst, con
     }
 }
 
+// First pass of a forward transform (unit twiddles), reading its inputs straight
+// from the grid rows in global memory: consecutive threads take consecutive
+// butterflies of a row, so each of the R loads is a contiguous run per row.
+template <typename T, int H, int ROWS, int R>
+__device__ __forceinline__ void pass_ct_first_global(const cpx<T> *__restrict__ g, int rows, cpx<T> *dst) {
+    constexpr int NQ = H / R, NIT = ROWS * NQ, HP = fpad_row<H>();
+    for (int it = threadIdx.x; it < NIT; it += blockDim.x) {
+        const int row = it / NQ, t = it - row * NQ;
+        cpx<T> v[R];
+        if (row < rows) {
+            const cpx<T> *s = g + (size_t)row * H;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = s[t + r * NQ];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = cpx<T>{0, 0};
+        }
+        dftR<T, -1, R>(v);
+        cpx<T> *d = dst + row * HP;
+#pragma unroll
+        for (int r = 0; r < R; r++) d[fpad(t * R + r)] = v[r];
+    }
+}
+
+// Passes IDX.. of a transform whose last pass writes the rows < rows straight
+// to global memory (row-contiguous): in the last pass NS*R = H, so output
+// t + r*NS of consecutive threads is a contiguous run.
+template <typename T, int S, int H, int ROWS, int IDX, int NS>
+__device__ __forceinline__ void passes_ct_to_global(cpx<T> *src, cpx<T> *dst, const cpx<T> *tw, cpx<T> *g,
+                                                    int rows) {
+    constexpr int R = radix_at(H, IDX);
+    if constexpr (IDX + 1 < radix_count(H)) {
+        pass_ct<T, S, H, ROWS, R, NS>(src, dst, tw);
+        __syncthreads();
+        passes_ct_to_global<T, S, H, ROWS, IDX + 1, NS * R>(dst, src, tw, g, rows);
+    } else {
+        static_assert(NS * R == H, "last pass");
+        constexpr int NQ = H / R, NIT = ROWS * NQ, STEP = H / (NS * R), HP = fpad_row<H>();
+        for (int it = threadIdx.x; it < NIT; it += blockDim.x) {
+            const int row = it / NQ, t = it - row * NQ, k = t % NS;
+            if (row >= rows) continue;
+            const cpx<T> *s = src + row * HP;
+            cpx<T> v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = s[fpad(t + r * NQ)];
+            if constexpr (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    cpx<T> w = tw[r * k * STEP];
+                    if (S > 0) w.y = -w.y;
+                    v[r] = cmul(v[r], w);
+                }
+            }
+            dftR<T, S, R>(v);
+            cpx<T> *d = g + (size_t)row * H;
+#pragma unroll
+            for (int r = 0; r < R; r++) d[t + r * NS] = v[r];
+        }
+    }
+}
+
 template <typename T> struct vec2 { using t = float4; };
 template <> struct vec2<double> { using t = double2; };
 
@@ -315,23 +376,11 @@ __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long l
     const int rows = (int)min((long long)ROWS, lot - row0);
     for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
     for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
-    {
-        // rows are contiguous: two complex (= 4 reals for FP32) per vector load
-        using V = typename vec2<T>::t;
-        constexpr int PER = (int)(sizeof(V) / sizeof(T)), CPV = PER / 2;
-        const V *src = reinterpret_cast<const V *>(gp + row0 * N);
-        const int nv = rows * N / PER;
-        for (int i = threadIdx.x; i < nv; i += blockDim.x) {
-            const int cj = i * CPV, row = cj / H, j = cj - row * H;
-            *reinterpret_cast<V *>(b0 + row * HP + fpad(j)) = src[i];
-        }
-        for (int cj = rows * H + threadIdx.x; cj < ROWS * H; cj += blockDim.x) {
-            const int row = cj / H, j = cj - row * H;
-            b0[row * HP + fpad(j)] = cpx<T>{0, 0};
-        }
-    }
+    // the first pass reads the grid rows directly (unit twiddles); the rest run in shared memory
+    constexpr int R0 = radix_at(H, 0);
+    pass_ct_first_global<T, H, ROWS, R0>(reinterpret_cast<const cpx<T> *>(gp + row0 * N), rows, b1);
     __syncthreads();
-    const cpx<T> *Z = passes_ct<T, -1, H, ROWS, 0, 1>(b0, b1, tw);
+    const cpx<T> *Z = passes_ct<T, -1, H, ROWS, 1, R0>(b1, b0, tw);
     const T scale = (T)1 / (T)N;
     for (int it = threadIdx.x; it < ROWS * kf; it += blockDim.x) {
         const int row = it % ROWS, k = it / ROWS;
@@ -393,15 +442,8 @@ __device__ __forceinline__ void rfft_inv_ct_body(const T *fc, T *gp, long long l
         b0[row * HP + fpad(k)] = cpx<T>{E.x - O.y, E.y + O.x};
     }
     __syncthreads();
-    const cpx<T> *z = passes_ct<T, +1, H, ROWS, 0, 1>(b0, b1, tw);
-    using V = typename vec2<T>::t;
-    constexpr int PER = (int)(sizeof(V) / sizeof(T)), CPV = PER / 2;
-    V *dst = reinterpret_cast<V *>(gp + row0 * N);
-    const int nv = rows * N / PER;
-    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
-        const int cj = i * CPV, row = cj / H, j = cj - row * H;
-        dst[i] = *reinterpret_cast<const V *>(z + row * HP + fpad(j));
-    }
+    // the last pass writes the grid rows directly
+    passes_ct_to_global<T, +1, H, ROWS, 0, 1>(b0, b1, tw, reinterpret_cast<cpx<T> *>(gp + row0 * N), rows);
 }
 
 template <typename T, int N, int ROWS>
