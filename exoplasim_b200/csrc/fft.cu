@@ -416,30 +416,30 @@ __device__ __forceinline__ void rfft_inv_ct_body(const T *fc, T *gp, long long l
     const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
     for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
-    for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
-    // c_k for k < kf (row fastest: consecutive rows are adjacent on the m-major side)
-    for (int it = threadIdx.x; it < ROWS * H; it += blockDim.x) {
-        const int row = it % ROWS, k = it / ROWS;
-        cpx<T> c{0, 0};
-        if (k < kf && row < rows) {
-            const size_t o = 2 * ((row0 + row) * f_rs + (long long)k * f_ms);
-            c = *reinterpret_cast<const cpx<T> *>(fc + o);
-            if (k == 0) c.y = 0;
-        }
-        b1[row * HP + fpad(k)] = c;
-    }
-    __syncthreads();
-    for (int it = threadIdx.x; it < ROWS * H; it += blockDim.x) {
-        const int row = it / H, k = it - row * H;
-        const cpx<T> *c = b1 + row * HP;
-        cpx<T> a = c[fpad(k)];
-        cpx<T> b = (k == 0) ? cpx<T>{0, 0} : c[fpad(H - k)];
-        cpx<T> E{a.x + b.x, a.y - b.y};
-        cpx<T> D{a.x - b.x, a.y + b.y};
-        cpx<T> w = rt[k];
+    // Z_k and Z_{H-k} of the half-length complex transform from c_k and c_{H-k}
+    // (c = 0 for k >= kf, and the m = 0 imaginary part ignored), one load of
+    // each coefficient; rows fastest, so consecutive threads read adjacent
+    // entries of the m-major side
+    auto unfold = [](cpx<T> a, cpx<T> b, cpx<T> w) {
+        const cpx<T> E{a.x + b.x, a.y - b.y};
+        const cpx<T> D{a.x - b.x, a.y + b.y};
         w.y = -w.y;
-        cpx<T> O = cmul(D, w);
-        b0[row * HP + fpad(k)] = cpx<T>{E.x - O.y, E.y + O.x};
+        const cpx<T> O = cmul(D, w);
+        return cpx<T>{E.x - O.y, E.y + O.x};
+    };
+    for (int it = threadIdx.x; it < ROWS * (H / 2 + 1); it += blockDim.x) {
+        const int row = it % ROWS, k = it / ROWS, k2 = H - k;
+        cpx<T> a{0, 0}, b{0, 0};
+        if (row < rows) {
+            const T *fr = fc + 2 * ((row0 + row) * f_rs);
+            if (k < kf) {
+                a = *reinterpret_cast<const cpx<T> *>(fr + 2 * (long long)k * f_ms);
+                if (k == 0) a.y = 0;
+            }
+            if (k > 0 && k2 < kf) b = *reinterpret_cast<const cpx<T> *>(fr + 2 * (long long)k2 * f_ms);
+        }
+        b0[row * HP + fpad(k)] = unfold(a, b, rtab[k]);
+        if (k > 0 && k2 != k) b0[row * HP + fpad(k2)] = unfold(b, a, rtab[k2]);
     }
     __syncthreads();
     // the last pass writes the grid rows directly
