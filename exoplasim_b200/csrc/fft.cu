@@ -382,24 +382,29 @@ __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long l
     __syncthreads();
     const cpx<T> *Z = passes_ct<T, -1, H, ROWS, 1, R0>(b1, b0, tw);
     const T scale = (T)1 / (T)N;
-    for (int it = threadIdx.x; it < ROWS * kf; it += blockDim.x) {
-        const int row = it % ROWS, k = it / ROWS;
+    // X_k and X_{H-k} from Z_k and Z_{H-k} (k <= H/2), each Z read once; only
+    // k < kf are stored.  Rows fastest: consecutive threads write adjacent
+    // entries of the m-major side.
+    auto fold = [&](cpx<T> a, cpx<T> b, int k) {
+        const cpx<T> E{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
+        const cpx<T> O{(T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x)};
+        const cpx<T> wo = cmul(rt[k], O);
+        return cpx<T>{(E.x + wo.x) * scale, (E.y + wo.y) * scale};
+    };
+    const int kh = min(H / 2, kf - 1);   // pairs (k, H-k) with k <= kh cover every k < kf
+    for (int it = threadIdx.x; it < ROWS * (kh + 1); it += blockDim.x) {
+        const int row = it % ROWS, k = it / ROWS, k2 = H - k;
         if (row >= rows) continue;
         const cpx<T> *z = Z + row * HP;
-        T re, im;
+        T *fr = fc + 2 * ((row0 + row) * f_rs);
+        const cpx<T> a = z[fpad(k)];
         if (k == 0) {
-            re = (z[0].x + z[0].y) * scale;
-            im = 0;
-        } else {
-            cpx<T> a = z[fpad(k)], b = z[fpad(H - k)];
-            cpx<T> E{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
-            cpx<T> O{(T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x)};
-            cpx<T> wo = cmul(rt[k], O);
-            re = (E.x + wo.x) * scale;
-            im = (E.y + wo.y) * scale;
+            *reinterpret_cast<cpx<T> *>(fr) = cpx<T>{(a.x + a.y) * scale, (T)0};
+            continue;
         }
-        const size_t o = 2 * ((row0 + row) * f_rs + (long long)k * f_ms);
-        *reinterpret_cast<cpx<T> *>(fc + o) = cpx<T>{re, im};
+        const cpx<T> b = z[fpad(k2)];
+        *reinterpret_cast<cpx<T> *>(fr + 2 * (long long)k * f_ms) = fold(a, b, k);
+        if (k2 < kf && k2 != k) *reinterpret_cast<cpx<T> *>(fr + 2 * (long long)k2 * f_ms) = fold(b, a, k2);
     }
 }
 
