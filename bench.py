@@ -111,6 +111,11 @@ class Clocks:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: begin timing once it is sampling
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
@@ -258,21 +263,21 @@ def run_ours(a, rank, world, local_rank):
     torch.cuda.synchronize()
     ref_gout, ref_sout = b64[2][0].clone(), b64[3][0].clone()
     precisions = [p for p in a.precisions.split(",") if p]
+    # clocks are sampled over the timed regions of every precision (each region
+    # alone is shorter than a few sampling intervals)
     clocks = Clocks(local_rank)
+    clocks.start()
     for prec in precisions:
         bufs = b64 if prec == "fp64" else make(torch.float32)
         fn = step_fn(prec, bufs)
-        if prec == precisions[0]:
-            clocks.start()
         ms, per_step = time_graph(fn, a.steps, a.warmup)
-        if prec == precisions[0]:
-            clk = clocks.stop()
         ms = max_over_ranks(ms)
         err_g = relerr_fields(bufs[2][0], ref_gout) if prec != "fp64" else 0.0
         err_s = relerr_fields(bufs[3][0], ref_sout) if prec != "fp64" else 0.0
         results[prec] = {"ms_per_step": ms / a.steps, "round_trips_per_s": world * B * a.steps / (ms / 1000.0),
                          "launches_per_step": per_step, "max_rel_err_vs_fp64": max(err_g, err_s)}
         del bufs
+    clk = clocks.stop()
     primary = precisions[0]
 
     # per-stage timing of the primary precision

@@ -66,10 +66,11 @@ static exotx_status ens_inverse(exotx_ensemble e, const float *spin, float *gpou
 static exotx_status ens_forward(exotx_ensemble e, const float *gpin, float *spout, cudaStream_t s) {
     std::vector<EnsSeg> v = ens_segs(e, nullptr, spout);
     std::vector<FftEnsSeg> f(v.size());
+    const bool folded = tc_ens_fwd_folded(v.data(), (int)v.size());   // persistent kernel: folded intermediate
     for (size_t i = 0; i < v.size(); i++) {
         const exotx_plan p = v[i].p;
         const long long rows = (long long)v[i].ninst * (9 * v[i].L + 1) * p->nlat;
-        f[i] = FftEnsSeg{gpin + e->seg_gin[i], v[i].W, rows, 1, rows, p->nlon, p->ntp1};
+        f[i] = FftEnsSeg{gpin + e->seg_gin[i], v[i].W, rows, 1, rows, p->nlon, p->ntp1, folded ? p->nlat : 0};
     }
     EXOTX_TRY(fft_ens(true, f.data(), (int)f.size(), s));
     return tc_ens_run(v.data(), (int)v.size(), 1, e->jobs[1], e->njobs[1], e->smem[1], e->nprod, s);

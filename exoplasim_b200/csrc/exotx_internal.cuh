@@ -131,7 +131,12 @@ struct FftEnsSeg {
     float *out;
     long long lot, f_rs, f_ms;
     int n, kf;
+    int fold_nlat = 0;  // forward: > 0 writes the equator-folded layout for nlat-row fields
 };
+// forward FFT into the equator-folded m-major layout of the tensor-core forward
+// kernel (E = north + south rows, then O = north - south, per field) (fft.cu)
+exotx_status fft_forward_fold(const float *in, float *out, int n, int nlat, long long lot, int kf, long long f_ms,
+                              cudaStream_t s);
 exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s);
 
 // radstep over all columns or a device-side column list (radiation.cu)
@@ -161,6 +166,7 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
                          int4 **d_jobs, int *njobs, size_t *smem);
 exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_jobs, int njobs, size_t smem,
                         int nprod, cudaStream_t s);
+bool tc_ens_fwd_folded(const EnsSeg *segs, int nseg);
 exotx_status tc_error_reset(cudaStream_t s);
 exotx_status tc_error_read(int *err, cudaStream_t s);
 exotx_status tc_available();

@@ -321,6 +321,31 @@ __device__ __forceinline__ void pass_ct_first_global(const cpx<T> *__restrict__ 
     }
 }
 
+// The same first pass for rows at arbitrary places: row r of the block is grid
+// row rowg[r] (in units of rows), or zeros where rowg[r] < 0.
+template <typename T, int H, int ROWS, int R>
+__device__ __forceinline__ void pass_ct_first_rows(const cpx<T> *__restrict__ g, const long long *rowg,
+                                                   cpx<T> *dst) {
+    constexpr int NQ = H / R, NIT = ROWS * NQ, HP = fpad_row<H>();
+    for (int it = threadIdx.x; it < NIT; it += blockDim.x) {
+        const int row = it / NQ, t = it - row * NQ;
+        const long long gr = rowg[row];
+        cpx<T> v[R];
+        if (gr >= 0) {
+            const cpx<T> *s = g + gr * H;
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = s[t + r * NQ];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = cpx<T>{0, 0};
+        }
+        dftR<T, -1, R>(v);
+        cpx<T> *d = dst + row * HP;
+#pragma unroll
+        for (int r = 0; r < R; r++) d[fpad(t * R + r)] = v[r];
+    }
+}
+
 // Passes IDX.. of a transform whose last pass writes the rows < rows straight
 // to global memory (row-contiguous): in the last pass NS*R = H, so output
 // t + r*NS of consecutive threads is a contiguous run.
@@ -408,6 +433,68 @@ __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long l
     }
 }
 
+// Forward transform that writes the Fourier side folded about the equator,
+// for the tensor-core Legendre kernel: for a field of nlat grid rows (north to
+// south) and latitude pair j < nlat/2 it stores E = X(j) + X(nlat-1-j) at row
+// field*nlat + j and O = X(j) - X(nlat-1-j) at row field*nlat + nlat/2 + j of
+// the m-major side (complex element (row, m) at row + m*f_ms).  A block takes
+// ROWS/2 latitude pairs of one field: rows r and r + ROWS/2 are a pair's
+// northern and southern rows.  lot is a multiple of nlat.
+template <typename T, int N, int ROWS>
+__device__ __forceinline__ void rfft_fwd_fold_body(const T *gp, T *fc, int nlat, long long lot, int kf,
+                                                   long long f_ms, const cpx<T> *__restrict__ wtab,
+                                                   const cpx<T> *__restrict__ rtab, long long blk) {
+    constexpr int H = N / 2, HP = fpad_row<H>(), PR = ROWS / 2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
+    cpx<T> *b1 = b0 + ROWS * HP;
+    cpx<T> *tw = b1 + ROWS * HP;
+    cpx<T> *rt = tw + H;
+    __shared__ long long rowg[ROWS];
+    const int nlath = nlat / 2, nbpf = (nlath + PR - 1) / PR;
+    const long long field = blk / nbpf;
+    const int j0 = (int)(blk - field * nbpf) * PR;
+    if (threadIdx.x < ROWS) {
+        const int r = threadIdx.x, j = j0 + (r % PR);
+        const int lat = r < PR ? j : nlat - 1 - j;
+        rowg[r] = (j < nlath && field * nlat < lot) ? field * nlat + lat : -1;
+    }
+    for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
+    for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
+    __syncthreads();
+    constexpr int R0 = radix_at(H, 0);
+    pass_ct_first_rows<T, H, ROWS, R0>(reinterpret_cast<const cpx<T> *>(gp), rowg, b1);
+    __syncthreads();
+    const cpx<T> *Z = passes_ct<T, -1, H, ROWS, 1, R0>(b1, b0, tw);
+    const T scale = (T)1 / (T)N;
+    auto fold = [&](cpx<T> a, cpx<T> b, int k) {
+        const cpx<T> E{(T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y)};
+        const cpx<T> O{(T)0.5 * (a.y + b.y), (T)0.5 * (b.x - a.x)};
+        const cpx<T> wo = cmul(rt[k], O);
+        return cpx<T>{(E.x + wo.x) * scale, (E.y + wo.y) * scale};
+    };
+    auto put = [&](long long row, int k, cpx<T> xn, cpx<T> xs) {
+        T *fr = fc + 2 * (row + (long long)k * f_ms);
+        *reinterpret_cast<cpx<T> *>(fr) = cpx<T>{xn.x + xs.x, xn.y + xs.y};
+        *reinterpret_cast<cpx<T> *>(fr + 2 * (long long)nlath) = cpx<T>{xn.x - xs.x, xn.y - xs.y};
+    };
+    const int kh = min(H / 2, kf - 1);   // pairs (k, H-k) with k <= kh cover every k < kf
+    for (int it = threadIdx.x; it < PR * (kh + 1); it += blockDim.x) {
+        const int pr = it % PR, k = it / PR, k2 = H - k, j = j0 + pr;
+        if (rowg[pr] < 0) continue;
+        const long long row = field * nlat + j;     // E row; O is nlath further
+        const cpx<T> *zn = Z + pr * HP, *zs = Z + (pr + PR) * HP;
+        const cpx<T> an = zn[fpad(k)], as = zs[fpad(k)];
+        if (k == 0) {
+            put(row, 0, cpx<T>{(an.x + an.y) * scale, (T)0}, cpx<T>{(as.x + as.y) * scale, (T)0});
+            continue;
+        }
+        const cpx<T> bn = zn[fpad(k2)], bs = zs[fpad(k2)];
+        put(row, k, fold(an, bn, k), fold(as, bs, k));
+        if (k2 < kf && k2 != k) put(row, k2, fold(bn, an, k2), fold(bs, as, k2));
+    }
+}
+
 template <typename T, int N, int ROWS>
 __device__ __forceinline__ void rfft_inv_ct_body(const T *fc, T *gp, long long lot, int kf, long long f_rs,
                                                  long long f_ms, const cpx<T> *__restrict__ wtab,
@@ -468,6 +555,13 @@ template <typename T> constexpr int ct_rows(int n) {
     return (sizeof(T) == 4) ? (n <= 256 ? 16 : 8) : (n <= 256 ? 8 : 4);
 }
 
+template <typename T, int N, int ROWS>
+__global__ void __launch_bounds__(256) k_rfft_fwd_fold(const T *gp, T *fc, int nlat, long long lot, int kf,
+                                                        long long f_ms, const cpx<T> *__restrict__ wtab,
+                                                        const cpx<T> *__restrict__ rtab) {
+    rfft_fwd_fold_body<T, N, ROWS>(gp, fc, nlat, lot, kf, f_ms, wtab, rtab, blockIdx.x);
+}
+
 // ---------------------------------------------------------------- ensembles
 // One launch transforms the rows of up to FFT_ENS_MAXSEG segments of different
 // lengths (an uneven ensemble); block b belongs to the last segment whose
@@ -477,6 +571,7 @@ struct FftEnsArgs {
     float *out;
     long long lot, f_rs, f_ms;
     int n, kf, block0;
+    int fold_nlat;          // forward only: > 0 writes the equator-folded layout (rfft_fwd_fold_body)
     const cpx<float> *w, *r;
 };
 struct FftEnsLaunch {
@@ -493,7 +588,8 @@ __global__ void __launch_bounds__(256) k_rfft_ens(const __grid_constant__ FftEns
     switch (S.n) {
 #define EXOTX_FFT_ENS_CASE(NN)                                                                                 \
     case NN:                                                                                                   \
-        if (FWD) rfft_fwd_ct_body<float, NN, ct_rows<float>(NN)>(S.in, S.out, S.lot, S.kf, S.f_rs, S.f_ms, S.w, S.r, blk); \
+        if (FWD && S.fold_nlat) rfft_fwd_fold_body<float, NN, ct_rows<float>(NN)>(S.in, S.out, S.fold_nlat, S.lot, S.kf, S.f_ms, S.w, S.r, blk); \
+        else if (FWD) rfft_fwd_ct_body<float, NN, ct_rows<float>(NN)>(S.in, S.out, S.lot, S.kf, S.f_rs, S.f_ms, S.w, S.r, blk); \
         else rfft_inv_ct_body<float, NN, ct_rows<float>(NN)>(S.in, S.out, S.lot, S.kf, S.f_rs, S.f_ms, S.w, S.r, blk);    \
         break;
         EXOTX_FFT_ENS_CASE(64)
@@ -529,10 +625,17 @@ exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s) 
         const int rows = ct_rows<float>(g.n);
         FftEnsArgs &a = P.seg[i];
         a.in = g.in; a.out = g.out; a.lot = g.lot; a.f_rs = g.f_rs; a.f_ms = g.f_ms; a.n = g.n; a.kf = g.kf;
+        a.fold_nlat = fwd ? g.fold_nlat : 0;
+        if (a.fold_nlat && (g.n != 2 * g.fold_nlat || g.lot % g.fold_nlat || g.f_rs != 1)) return EXOTX_BAD_ARG;
         a.w = reinterpret_cast<const cpx<float> *>(t->w32);
         a.r = reinterpret_cast<const cpx<float> *>(t->r32);
         a.block0 = blocks;
-        blocks += (int)((g.lot + rows - 1) / rows);
+        if (a.fold_nlat) {
+            const int nbpf = (g.fold_nlat / 2 + rows / 2 - 1) / (rows / 2);
+            blocks += (int)(g.lot / g.fold_nlat) * nbpf;
+        } else {
+            blocks += (int)((g.lot + rows - 1) / rows);
+        }
         const int hp = g.n / 2 + 2 * (g.n / 32);   // padded row, as fpad_row
         smem = std::max(smem, (2 * (size_t)rows * hp + g.n / 2 + g.n / 2 + 1) * sizeof(cpx<float>));
     }
@@ -736,6 +839,47 @@ template exotx_status fft_forward_l<double>(const double *, double *, int, long 
                                             cudaStream_t);
 template exotx_status fft_forward_l<float>(const float *, float *, int, long long, int, long long, long long,
                                            cudaStream_t);
+
+template <int N>
+static exotx_status launch_fold(const float *in, float *out, int nlat, long long lot, int kf, long long f_ms,
+                                const cpx<float> *w, const cpx<float> *r, cudaStream_t s) {
+    constexpr int ROWS = ct_rows<float>(N);
+    const size_t smem = (2 * ROWS * fpad_row<N / 2>() + N / 2 + N / 2 + 1) * sizeof(cpx<float>);
+    const int nbpf = (nlat / 2 + ROWS / 2 - 1) / (ROWS / 2);
+    const long long nb = (lot / nlat) * nbpf;
+    if (smem > 48 * 1024)
+        EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_fold<float, N, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    cudaEvent_t ev = ktimer_start(EXOTX_K_FFT_FORWARD, s);
+    k_rfft_fwd_fold<float, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, nlat, lot, kf, f_ms, w, r);
+    EXOTX_CHECK_LAUNCH();
+    ktimer_stop(EXOTX_K_FFT_FORWARD, s, ev);
+    return EXOTX_OK;
+}
+
+// forward transform of lot = fields x nlat grid rows of length n = 2 nlat into
+// the equator-folded m-major layout (rfft_fwd_fold_body); EXOTX_NOT_BUILT when
+// n has no specialised kernel or the buffers are not 16-byte aligned
+exotx_status fft_forward_fold(const float *in, float *out, int n, int nlat, long long lot, int kf, long long f_ms,
+                              cudaStream_t s) {
+    if (n != 2 * nlat || nlat < 2 || lot % nlat) return EXOTX_BAD_ARG;
+    exotx_status st;
+    const FftTables *t = fft_tables(n, &st);
+    if (!t) return st;
+    if (lot <= 0) return EXOTX_OK;
+    if (!aligned16(in) || !aligned16(out)) return EXOTX_NOT_BUILT;
+    const cpx<float> *w = wt<float>(t), *r = rt<float>(t);
+    switch (n) {
+        case 64: return launch_fold<64>(in, out, nlat, lot, kf, f_ms, w, r, s);
+        case 128: return launch_fold<128>(in, out, nlat, lot, kf, f_ms, w, r, s);
+        case 192: return launch_fold<192>(in, out, nlat, lot, kf, f_ms, w, r, s);
+        case 256: return launch_fold<256>(in, out, nlat, lot, kf, f_ms, w, r, s);
+        case 320: return launch_fold<320>(in, out, nlat, lot, kf, f_ms, w, r, s);
+        case 384: return launch_fold<384>(in, out, nlat, lot, kf, f_ms, w, r, s);
+        case 512: return launch_fold<512>(in, out, nlat, lot, kf, f_ms, w, r, s);
+    }
+    return EXOTX_NOT_BUILT;
+}
 template exotx_status fft_inverse_l<double>(const double *, double *, int, long long, int, long long, long long,
                                             cudaStream_t);
 template exotx_status fft_inverse_l<float>(const float *, float *, int, long long, int, long long, long long,

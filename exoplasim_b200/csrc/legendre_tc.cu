@@ -340,7 +340,7 @@ static int fwd_level(exotx_plan p, const TcTables *T) {
 // the persistent stacked-split forward kernel runs wherever its tables exist and fit
 static bool use_fwd3(const TcTables *T) { return T->has3 && fpipe_smem(T->njc) <= TC_SMEM_MAX; }
 // the persistent stacked-split forward kernel: one CTA per SM walks the job list
-static exotx_status launch_fwd_pipe(TcFwd3Launch &P, int njobs, int njmax, cudaStream_t s) {
+static exotx_status launch_fwd_pipe(TcFwd3Launch &P, int njobs, int njmax, bool folded, cudaStream_t s) {
     static int nsm = 0;
     if (!nsm) {
         int dev = 0;
@@ -351,11 +351,11 @@ static exotx_status launch_fwd_pipe(TcFwd3Launch &P, int njobs, int njmax, cudaS
     if (smem > TC_SMEM_MAX) return EXOTX_BAD_DIM;
     P.njobs = njobs;
     P.njmax = njmax;
-    EXOTX_CUDA(cudaFuncSetAttribute(k_tc_forward_pipe<F3_NLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)TC_SMEM_MAX));
+    auto kern = folded ? k_tc_forward_pipe<F3_NLT, true> : k_tc_forward_pipe<F3_NLT, false>;
+    EXOTX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
     const int grid = std::max(1, std::min(njobs, nsm));
     cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
-    k_tc_forward_pipe<F3_NLT><<<grid, FP_THREADS, smem, s>>>(P);
+    kern<<<grid, FP_THREADS, smem, s>>>(P);
     EXOTX_CHECK_LAUNCH();
     ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
     return EXOTX_OK;
@@ -506,14 +506,24 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
         int nj = njobs;
         if (ni != chunk) EXOTX_TRY(tc_jobs(p, T, 1, L, ni, &jl, &nj));
         const long long nrows = (long long)ni * nfi * p->nlat;
-        EXOTX_TRY(fft_forward_l<float>(gpin + (size_t)i0 * nfi * nhor, (float *)p->d_work, p->nlon, nrows, p->ntp1,
-                                       1, nrows, s));
+        const float *gsrc = gpin + (size_t)i0 * nfi * nhor;
+        // the persistent kernel reads the intermediate folded about the equator where
+        // the grid length has a specialised FFT; otherwise as north and south rows
+        bool folded = false;
+        if (v3) {
+            const exotx_status sf = fft_forward_fold(gsrc, (float *)p->d_work, p->nlon, p->nlat, nrows, p->ntp1,
+                                                     nrows, s);
+            if (sf != EXOTX_OK && sf != EXOTX_NOT_BUILT) return sf;
+            folded = sf == EXOTX_OK;
+        }
+        if (!folded)
+            EXOTX_TRY(fft_forward_l<float>(gsrc, (float *)p->d_work, p->nlon, nrows, p->ntp1, 1, nrows, s));
         if (v3) {
             TcFwd3Launch P3;
             P3.jobs = jl;
             P3.nprod = 6;
             fwd3_args(P3.seg[0], p, T, L, (const float2 *)p->d_work, nrows, spout + (size_t)i0 * (4 * L + 1) * nrsp);
-            EXOTX_TRY(launch_fwd_pipe(P3, nj, T->njc, s));
+            EXOTX_TRY(launch_fwd_pipe(P3, nj, T->njc, folded, s));
             continue;
         }
         TcFwdLaunch P;
@@ -607,6 +617,16 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
     return EXOTX_OK;
 }
 
+// whether the forward tensor-core launch over these segments is the persistent
+// kernel, which reads the intermediate folded about the equator
+bool tc_ens_fwd_folded(const EnsSeg *segs, int nseg) {
+    for (int i = 0; i < nseg; i++) {
+        TcTables *T;
+        if (tc_tables(segs[i].p, &T) != EXOTX_OK || !use_fwd3(T)) return false;
+    }
+    return nseg > 0;
+}
+
 // one tensor-core launch over every segment: inverse (spin -> W) or forward (W -> spout)
 exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_jobs, int njobs, size_t smem,
                         int nprod, cudaStream_t s) {
@@ -660,7 +680,7 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
                           (long long)g.ninst * (9 * g.L + 1) * g.p->nlat, g.spout);
                 njmax = std::max(njmax, T->njc);
             }
-            return launch_fwd_pipe(P3, njobs, njmax, s);
+            return launch_fwd_pipe(P3, njobs, njmax, true, s);   // the ensemble FFT writes the folded form
         }
         P.onebuf = kFwdOne[lv];
         for (int i = 0; i < nseg; i++) {

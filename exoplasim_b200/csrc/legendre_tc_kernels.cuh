@@ -785,6 +785,60 @@ __device__ __forceinline__ void f3_store(int t, int p, int sl, int njc, unsigned
     st_shared8(bt + o + 16, hi); st_shared8(bt + dt + o + 16, mi); st_shared8(bt + 2 * dt + o + 16, li);
 }
 
+// The same staging from the equator-folded intermediate (rfft_fwd_fold_body):
+// each field row holds E = N + S for the latitude pairs, then O = N - S, so a
+// parity reads only the half it needs and a slot covers eight latitude pairs
+// j = 8jg .. 8jg+7 of one row (n[] the first four, s[] the next four), stored
+// as one 16-byte core-matrix row per split term.
+template <int NLT>
+__device__ __forceinline__ void f3_load_fold(const TcFwd3Args &A, int m, int inst, int l0, int nl, bool with_vpp,
+                                             int t, int p, int sl, F3Slot &v) {
+    const int hj = A.njc >> 3;
+    const int q = sl / hj, jg = sl - q * hj;
+#pragma unroll
+    for (int e = 0; e < 4; e++) v.n[e] = v.s[e] = make_float2(0.f, 0.f);
+    if (q >= (fwd_ncp<NLT>(t) >> 1)) return;
+    const long long rb = f3_row<NLT>(A, inst, l0, nl, with_vpp, t, q);
+    if (rb < 0) return;
+    const int j = 8 * jg, nlath = A.nlath;
+    const bool diff = (t != 1) ? (p == 1) : (p == 0);
+    const float2 *wf = A.W + (size_t)m * A.nrows + (size_t)rb * A.nlat + (diff ? nlath : 0);
+    if (j + 8 <= nlath && !(nlath & 1)) {
+        const float4 *w4 = reinterpret_cast<const float4 *>(wf + j);
+        const float4 x0 = __ldg(w4), x1 = __ldg(w4 + 1), x2 = __ldg(w4 + 2), x3 = __ldg(w4 + 3);
+        v.n[0] = make_float2(x0.x, x0.y); v.n[1] = make_float2(x0.z, x0.w);
+        v.n[2] = make_float2(x1.x, x1.y); v.n[3] = make_float2(x1.z, x1.w);
+        v.s[0] = make_float2(x2.x, x2.y); v.s[1] = make_float2(x2.z, x2.w);
+        v.s[2] = make_float2(x3.x, x3.y); v.s[3] = make_float2(x3.z, x3.w);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            if (j + e < nlath) v.n[e] = __ldg(wf + j + e);
+            if (j + 4 + e < nlath) v.s[e] = __ldg(wf + j + 4 + e);
+        }
+    }
+}
+template <int NLT>
+__device__ __forceinline__ void f3_store_fold(int t, int sl, int njc, unsigned char *bt, const F3Slot &v) {
+    const int hj = njc >> 3, ngk = njc >> 3;
+    const int q = sl / hj, jg = sl - q * hj;
+    const int ncp = fwd_ncp<NLT>(t);
+    if (q >= (ncp >> 1)) return;
+    float xr[8], xi[8];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        xr[e] = v.n[e].x; xi[e] = v.n[e].y;
+        xr[e + 4] = v.s[e].x; xi[e + 4] = v.s[e].y;
+    }
+    uint4 h, mm, l;
+    const uint32_t dt = (uint32_t)(ncp >> 3) * ngk * tc::kPadLbo;  // one split term
+    const uint32_t o = tc::kpad_off(2 * q, 8 * jg, ngk);            // re row; the im row follows at +16
+    tc::split3x8(xr, h, mm, l);
+    st_shared16(bt + o, h); st_shared16(bt + dt + o, mm); st_shared16(bt + 2 * dt + o, l);
+    tc::split3x8(xi, h, mm, l);
+    st_shared16(bt + o + 16, h); st_shared16(bt + dt + o + 16, mm); st_shared16(bt + 2 * dt + o + 16, l);
+}
+
 // ------------------------------------------------------------ forward, pipelined
 // Persistent form of the stacked-split forward kernel.  One CTA per SM walks
 // the jobs blockIdx.x, blockIdx.x + gridDim.x, ... of the launch; a job's four
@@ -873,7 +927,8 @@ __device__ __forceinline__ void fp_drain(int t, uint32_t X, int nprod, float (*o
     else fp_drain_t<NLT, 3>(X, nprod, o, ov);
 }
 
-template <int NLT>
+// FOLD: the intermediate is folded about the equator (rfft_fwd_fold_body)
+template <int NLT, bool FOLD>
 __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_constant__ TcFwd3Launch P) {
     extern __shared__ __align__(128) unsigned char sm[];
     const FpLayout LY = fp_layout(P.njmax);
@@ -1039,12 +1094,21 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
         // ------------------------------------------------------------- staging
         const int stid = (warp < 4 ? warp - 2 : warp - 6) * 32 + lane;
         F3Slot cur[FP_SLOTS], nxt[FP_SLOTS];
+        auto load = [&](const TcFwd3Args &A, int4 jb, int t, int sl, F3Slot &v) {
+            if constexpr (FOLD)
+                f3_load_fold<NLT>(A, jb.x, jb.y & 0xffff, jb.z, jb.w & 0xff, jb.z == 0, t, jb.w >> 8, sl, v);
+            else
+                f3_load<NLT>(A, jb.x, jb.y & 0xffff, jb.z, jb.w & 0xff, jb.z == 0, t, sl, v);
+        };
+        auto store = [&](int t, int p, int sl, int njc, unsigned char *bt, const F3Slot &v) {
+            if constexpr (FOLD) f3_store_fold<NLT>(t, sl, njc, bt, v);
+            else f3_store<NLT>(t, p, sl, njc, bt, v);
+        };
         if (ntile > 0) {
             const int4 jb = P.jobs[blockIdx.x];
             const TcFwd3Args &A = P.seg[jb.y >> 16];
 #pragma unroll
-            for (int k = 0; k < FP_SLOTS; k++)
-                f3_load<NLT>(A, jb.x, jb.y & 0xffff, jb.z, jb.w & 0xff, jb.z == 0, 0, stid + k * FP_NST, cur[k]);
+            for (int k = 0; k < FP_SLOTS; k++) load(A, jb, 0, stid + k * FP_NST, cur[k]);
         }
         for (int i = 0; i < ntile; i++) {
             const int b = i & 1, u = i >> 1, t = i & 3;
@@ -1054,22 +1118,19 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             if (i + 1 < ntile) {
                 // the next tile's loads are in flight while this one is stored
                 const int4 jn = P.jobs[blockIdx.x + ((i + 1) >> 2) * gridDim.x];
-                const TcFwd3Args &An = P.seg[jn.y >> 16];
 #pragma unroll
-                for (int k = 0; k < FP_SLOTS; k++)
-                    f3_load<NLT>(An, jn.x, jn.y & 0xffff, jn.z, jn.w & 0xff, jn.z == 0, (i + 1) & 3, stid + k * FP_NST,
-                                 nxt[k]);
+                for (int k = 0; k < FP_SLOTS; k++) load(P.seg[jn.y >> 16], jn, (i + 1) & 3, stid + k * FP_NST, nxt[k]);
             }
             if (!fp_wait(op_empty + b, (u & 1) ^ 1, abort)) break;
             unsigned char *bt = opr + b * LY.ob;
-            const int nslot = (fwd_ncp<NLT>(t) >> 1) * (njc >> 2);
+            const int nslot = (fwd_ncp<NLT>(t) >> 1) * (FOLD ? (njc >> 3) : (njc >> 2));
 #pragma unroll
             for (int k = 0; k < FP_SLOTS; k++)
-                if (stid + k * FP_NST < nslot) f3_store<NLT>(t, p, stid + k * FP_NST, njc, bt, cur[k]);
+                if (stid + k * FP_NST < nslot) store(t, p, stid + k * FP_NST, njc, bt, cur[k]);
             for (int s = stid + FP_SLOTS * FP_NST; s < nslot; s += FP_NST) {   // beyond the slots in flight
                 F3Slot v;
-                f3_load<NLT>(A, jb.x, jb.y & 0xffff, jb.z, jb.w & 0xff, jb.z == 0, t, s, v);
-                f3_store<NLT>(t, p, s, njc, bt, v);
+                load(A, jb, t, s, v);
+                store(t, p, s, njc, bt, v);
             }
             tc::fence_proxy_async();   // these stores feed the tensor cores
             tc::mbar_arrive(op_full + b);
