@@ -445,9 +445,9 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
     EXOTX_TRY(tc_tables(p, &T));
     const long long nrsp = 2LL * p->ncsp, nhor = (long long)p->nlat * p->nlon;
     const int nfo = 6 * L + 3;
-    // chunk instances so the m-major Fourier intermediate stays L2-resident (<= 48 MB)
+    // chunk instances so the m-major Fourier intermediate stays L2-resident (<= 80 MB of the 126 MB L2)
     const size_t per_inst = (size_t)nfo * p->nlat * p->ntp1 * sizeof(float2);
-    int chunk = (int)std::max<size_t>(1, (48u << 20) / per_inst);
+    int chunk = (int)std::max<size_t>(1, (80u << 20) / per_inst);
     chunk = std::min(chunk, ninst);
     EXOTX_TRY(ensure_work(p, per_inst * chunk));
     const int4 *jobs;
@@ -490,7 +490,7 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
     const long long nrsp = 2LL * p->ncsp, nhor = (long long)p->nlat * p->nlon;
     const int nfi = 9 * L + 1;
     const size_t per_inst = (size_t)nfi * p->nlat * p->ntp1 * sizeof(float2);
-    int chunk = (int)std::max<size_t>(1, (48u << 20) / per_inst);
+    int chunk = (int)std::max<size_t>(1, (80u << 20) / per_inst);
     chunk = std::min(chunk, ninst);
     EXOTX_TRY(ensure_work(p, per_inst * chunk));
     const int4 *jobs;
