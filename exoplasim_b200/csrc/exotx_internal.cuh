@@ -38,6 +38,32 @@ inline exotx_status cuda_status(cudaError_t e) {
         if (e_ != cudaSuccess) return ::exotx::cuda_status(e_);     \
     } while (0)
 
+// Programmatic dependent launch.  A kernel launched with launch_pdl may start
+// while the kernel before it in the stream is still finishing (once every
+// block of that kernel has started and called pdl_trigger); before it touches
+// any memory that kernel or an earlier one reads or writes it must call
+// pdl_wait, which returns once the previous kernel has completed and its
+// writes are visible.  Work before pdl_wait may only use constant data (the
+// plan's tables and twiddles).  In a kernel launched without the attribute both
+// calls do nothing.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, static_cast<Args &&>(args)...);
+}
+
 // Real FFT twiddle tables for one length n, owned by a process-wide cache.
 struct FftTables {
     int n = 0, h = 0;            // h = n/2 complex points

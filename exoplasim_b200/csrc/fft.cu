@@ -399,8 +399,10 @@ __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long l
     cpx<T> *rt = tw + H;
     const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
+    pdl_trigger();
     for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
     for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
+    pdl_wait();   // the grid rows may come from the previous kernel
     // the first pass reads the grid rows directly (unit twiddles); the rest run in shared memory
     constexpr int R0 = radix_at(H, 0);
     pass_ct_first_global<T, H, ROWS, R0>(reinterpret_cast<const cpx<T> *>(gp + row0 * N), rows, b1);
@@ -459,9 +461,11 @@ __device__ __forceinline__ void rfft_fwd_fold_body(const T *gp, T *fc, int nlat,
         const int lat = r < PR ? j : nlat - 1 - j;
         rowg[r] = (j < nlath && field * nlat < lot) ? field * nlat + lat : -1;
     }
+    pdl_trigger();
     for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
     for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
     __syncthreads();
+    pdl_wait();   // the grid rows may come from the previous kernel, which may still read the output
     constexpr int R0 = radix_at(H, 0);
     pass_ct_first_rows<T, H, ROWS, R0>(reinterpret_cast<const cpx<T> *>(gp), rowg, b1);
     __syncthreads();
@@ -507,7 +511,9 @@ __device__ __forceinline__ void rfft_inv_ct_body(const T *fc, T *gp, long long l
     cpx<T> *rt = tw + H;
     const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
+    pdl_trigger();
     for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
+    pdl_wait();   // the coefficients come from the previous kernel
     // Z_k and Z_{H-k} of the half-length complex transform from c_k and c_{H-k}
     // (c = 0 for k >= kf, and the m = 0 imaginary part ignored), one load of
     // each coefficient; rows fastest, so consecutive threads read adjacent
@@ -672,10 +678,13 @@ static exotx_status launch_ct(bool fwd, const T *in, T *out, long long lot, int 
                                             (int)smem));
     }
     cudaEvent_t ev = ktimer_start(kid, s);
+    // dependent launch: the block set-up overlaps the previous kernel's tail
     if (fwd)
-        k_rfft_fwd_ct<T, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, lot, kf, f_rs, f_ms, w, r);
+        EXOTX_CUDA(launch_pdl(k_rfft_fwd_ct<T, N, ROWS>, dim3((unsigned)nb), dim3(256), smem, s, in, out, lot, kf,
+                              f_rs, f_ms, w, r));
     else
-        k_rfft_inv_ct<T, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, lot, kf, f_rs, f_ms, w, r);
+        EXOTX_CUDA(launch_pdl(k_rfft_inv_ct<T, N, ROWS>, dim3((unsigned)nb), dim3(256), smem, s, in, out, lot, kf,
+                              f_rs, f_ms, w, r));
     EXOTX_CHECK_LAUNCH();
     ktimer_stop(kid, s, ev);
     return EXOTX_OK;
@@ -851,7 +860,8 @@ static exotx_status launch_fold(const float *in, float *out, int nlat, long long
         EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_fold<float, N, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
     cudaEvent_t ev = ktimer_start(EXOTX_K_FFT_FORWARD, s);
-    k_rfft_fwd_fold<float, N, ROWS><<<(unsigned)nb, 256, smem, s>>>(in, out, nlat, lot, kf, f_ms, w, r);
+    EXOTX_CUDA(launch_pdl(k_rfft_fwd_fold<float, N, ROWS>, dim3((unsigned)nb), dim3(256), smem, s, in, out, nlat, lot,
+                          kf, f_ms, w, r));
     EXOTX_CHECK_LAUNCH();
     ktimer_stop(EXOTX_K_FFT_FORWARD, s, ev);
     return EXOTX_OK;

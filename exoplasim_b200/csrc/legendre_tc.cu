@@ -355,7 +355,7 @@ static exotx_status launch_fwd_pipe(TcFwd3Launch &P, int njobs, int njmax, bool 
     EXOTX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
     const int grid = std::max(1, std::min(njobs, nsm));
     cudaEvent_t ev = ktimer_start(EXOTX_K_TC_FORWARD, s);
-    kern<<<grid, FP_THREADS, smem, s>>>(P);
+    EXOTX_CUDA(launch_pdl(kern, dim3(grid), dim3(FP_THREADS), smem, s, P));   // set-up overlaps the FFT's tail
     EXOTX_CHECK_LAUNCH();
     ktimer_stop(EXOTX_K_TC_FORWARD, s, ev);
     return EXOTX_OK;
@@ -475,7 +475,7 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.nj8 = T->nj8; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
         A.plavor = (float)p->desc.plavor;
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
-        k_tc_inverse<<<nj, TCI, smem, s>>>(P);
+        EXOTX_CUDA(launch_pdl(k_tc_inverse, dim3(nj), dim3(TCI), smem, s, P));   // set-up overlaps the last tail
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
         EXOTX_TRY(fft_inverse_l<float>((const float *)p->d_work, gpout + (size_t)i0 * nfo * nhor, p->nlon, A.nrows,

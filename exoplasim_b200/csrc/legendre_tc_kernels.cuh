@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
     uint64_t *bar_mma = bar_tma + 1;
     uint64_t *bar_done = bar_tma + 2;
     uint32_t *slot = reinterpret_cast<uint32_t *>(bar_tma + 3);
+    pdl_trigger();
     if (warp == 0) tc::tmem_alloc(slot, 512);
     if (tid == 0) {
         tc::mbar_init(bar_tma, 1);
@@ -90,6 +91,7 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
         tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
         tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0], (uint32_t)tbytes, bar_tma);
     }
+    pdl_wait();   // the spectral input and the intermediate are shared with earlier kernels
     // stage the spectral columns of both parities.  A slot is one column pair
     // q (re, im) and the modes k = 2l, 2l+1 of both parities, i.e. the four
     // consecutive spectral entries n - m = 4l .. 4l+3: consecutive threads
@@ -945,6 +947,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
     // tiles of this CTA: jobs blockIdx.x + k gridDim.x, four tables each
     const int mine = njobs > (int)blockIdx.x ? (njobs - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int ntile = 4 * mine;
+    pdl_trigger();
     if (warp == 0) tc::tmem_alloc(slot, 512);
     if (tid == 0) {
         for (int i = 0; i < 2; i++) {
@@ -1027,6 +1030,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
     } else if (warp >= 4 && warp < 8) {
         // ------------------------------------------------------------ epilogue
         const int quarter = warp - 4, r = quarter * 32 + lane;
+        pdl_wait();   // the outputs may be read by earlier kernels
         const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
         constexpr int NO = NLT * 8 + 2;
         float o[NLT][4][2], ov[2];
@@ -1093,6 +1097,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
     } else {
         // ------------------------------------------------------------- staging
         const int stid = (warp < 4 ? warp - 2 : warp - 6) * 32 + lane;
+        pdl_wait();   // the intermediate comes from the previous kernel
         F3Slot cur[FP_SLOTS], nxt[FP_SLOTS];
         auto load = [&](const TcFwd3Args &A, int4 jb, int t, int sl, F3Slot &v) {
             if constexpr (FOLD)
