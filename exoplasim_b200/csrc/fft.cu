@@ -395,13 +395,11 @@ __device__ __forceinline__ void rfft_fwd_ct_body(const T *gp, T *fc, long long l
     extern __shared__ __align__(16) unsigned char smraw[];
     cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
     cpx<T> *b1 = b0 + ROWS * HP;
-    cpx<T> *tw = b1 + ROWS * HP;
-    cpx<T> *rt = tw + H;
+    // twiddles are read from global memory (L1-cached); shared memory holds only the rows
+    const cpx<T> *tw = wtab, *rt = rtab;
     const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
     pdl_trigger();
-    for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
-    for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
     pdl_wait();   // the grid rows may come from the previous kernel
     // the first pass reads the grid rows directly (unit twiddles); the rest run in shared memory
     constexpr int R0 = radix_at(H, 0);
@@ -450,8 +448,8 @@ __device__ __forceinline__ void rfft_fwd_fold_body(const T *gp, T *fc, int nlat,
     extern __shared__ __align__(16) unsigned char smraw[];
     cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
     cpx<T> *b1 = b0 + ROWS * HP;
-    cpx<T> *tw = b1 + ROWS * HP;
-    cpx<T> *rt = tw + H;
+    // twiddles are read from global memory (L1-cached); shared memory holds only the rows
+    const cpx<T> *tw = wtab, *rt = rtab;
     __shared__ long long rowg[ROWS];
     const int nlath = nlat / 2, nbpf = (nlath + PR - 1) / PR;
     const long long field = blk / nbpf;
@@ -462,8 +460,6 @@ __device__ __forceinline__ void rfft_fwd_fold_body(const T *gp, T *fc, int nlat,
         rowg[r] = (j < nlath && field * nlat < lot) ? field * nlat + lat : -1;
     }
     pdl_trigger();
-    for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
-    for (int i = threadIdx.x; i <= H; i += blockDim.x) rt[i] = rtab[i];
     __syncthreads();
     pdl_wait();   // the grid rows may come from the previous kernel, which may still read the output
     constexpr int R0 = radix_at(H, 0);
@@ -507,12 +503,11 @@ __device__ __forceinline__ void rfft_inv_ct_body(const T *fc, T *gp, long long l
     extern __shared__ __align__(16) unsigned char smraw[];
     cpx<T> *b0 = reinterpret_cast<cpx<T> *>(smraw);
     cpx<T> *b1 = b0 + ROWS * HP;
-    cpx<T> *tw = b1 + ROWS * HP;
-    cpx<T> *rt = tw + H;
+    // twiddles are read from global memory (L1-cached); shared memory holds only the rows
+    const cpx<T> *tw = wtab;
     const long long row0 = blk * ROWS;
     const int rows = (int)min((long long)ROWS, lot - row0);
     pdl_trigger();
-    for (int i = threadIdx.x; i < H; i += blockDim.x) tw[i] = wtab[i];
     pdl_wait();   // the coefficients come from the previous kernel
     // Z_k and Z_{H-k} of the half-length complex transform from c_k and c_{H-k}
     // (c = 0 for k >= kf, and the m = 0 imaginary part ignored), one load of
@@ -643,7 +638,7 @@ exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s) 
             blocks += (int)((g.lot + rows - 1) / rows);
         }
         const int hp = g.n / 2 + 2 * (g.n / 32);   // padded row, as fpad_row
-        smem = std::max(smem, (2 * (size_t)rows * hp + g.n / 2 + g.n / 2 + 1) * sizeof(cpx<float>));
+        smem = std::max(smem, 2 * (size_t)rows * hp * sizeof(cpx<float>));
     }
     if (blocks == 0) return EXOTX_OK;
     const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
@@ -665,7 +660,7 @@ template <typename T, int N>
 static exotx_status launch_ct(bool fwd, const T *in, T *out, long long lot, int kf, long long f_rs, long long f_ms,
                               const cpx<T> *w, const cpx<T> *r, cudaStream_t s) {
     constexpr int ROWS = ct_rows<T>(N);
-    const size_t smem = (2 * ROWS * fpad_row<N / 2>() + N / 2 + N / 2 + 1) * sizeof(cpx<T>);
+    const size_t smem = 2 * ROWS * fpad_row<N / 2>() * sizeof(cpx<T>);
     const long long nb = (lot + ROWS - 1) / ROWS;
     const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
     if (fwd) {
@@ -853,7 +848,7 @@ template <int N>
 static exotx_status launch_fold(const float *in, float *out, int nlat, long long lot, int kf, long long f_ms,
                                 const cpx<float> *w, const cpx<float> *r, cudaStream_t s) {
     constexpr int ROWS = ct_rows<float>(N);
-    const size_t smem = (2 * ROWS * fpad_row<N / 2>() + N / 2 + N / 2 + 1) * sizeof(cpx<float>);
+    const size_t smem = 2 * ROWS * fpad_row<N / 2>() * sizeof(cpx<float>);
     const int nbpf = (nlat / 2 + ROWS / 2 - 1) / (ROWS / 2);
     const long long nb = (lot / nlat) * nbpf;
     if (smem > 48 * 1024)
