@@ -1098,7 +1098,11 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
         // ------------------------------------------------------------- staging
         const int stid = (warp < 4 ? warp - 2 : warp - 6) * 32 + lane;
         pdl_wait();   // the intermediate comes from the previous kernel
-        F3Slot cur[FP_SLOTS], nxt[FP_SLOTS];
+        // slots per thread kept in flight for a tile, and how many tiles ahead
+        // they are loaded: the folded intermediate needs one slot per thread
+        // per tile (eight latitude pairs), so its loads run two tiles ahead
+        constexpr int SL = FOLD ? 1 : FP_SLOTS, DEPTH = FOLD ? 2 : 1;
+        F3Slot q0[SL], q1[SL], q2[SL];   // tiles i, i+1, i+2
         auto load = [&](const TcFwd3Args &A, int4 jb, int t, int sl, F3Slot &v) {
             if constexpr (FOLD)
                 f3_load_fold<NLT>(A, jb.x, jb.y & 0xffff, jb.z, jb.w & 0xff, jb.z == 0, t, jb.w >> 8, sl, v);
@@ -1109,30 +1113,38 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             if constexpr (FOLD) f3_store_fold<NLT>(t, sl, njc, bt, v);
             else f3_store<NLT>(t, p, sl, njc, bt, v);
         };
+        auto job = [&](int i) { return P.jobs[blockIdx.x + (i >> 2) * gridDim.x]; };
         if (ntile > 0) {
-            const int4 jb = P.jobs[blockIdx.x];
-            const TcFwd3Args &A = P.seg[jb.y >> 16];
+            const int4 jb = job(0);
 #pragma unroll
-            for (int k = 0; k < FP_SLOTS; k++) load(A, jb, 0, stid + k * FP_NST, cur[k]);
+            for (int k = 0; k < SL; k++) load(P.seg[jb.y >> 16], jb, 0, stid + k * FP_NST, q0[k]);
+        }
+        if (DEPTH == 2 && ntile > 1) {
+            const int4 jb = job(1);
+#pragma unroll
+            for (int k = 0; k < SL; k++) load(P.seg[jb.y >> 16], jb, 1, stid + k * FP_NST, q1[k]);
         }
         for (int i = 0; i < ntile; i++) {
             const int b = i & 1, u = i >> 1, t = i & 3;
-            const int4 jb = P.jobs[blockIdx.x + (i >> 2) * gridDim.x];
+            const int4 jb = job(i);
             const TcFwd3Args &A = P.seg[jb.y >> 16];
             const int njc = A.njc, p = jb.w >> 8;
-            if (i + 1 < ntile) {
-                // the next tile's loads are in flight while this one is stored
-                const int4 jn = P.jobs[blockIdx.x + ((i + 1) >> 2) * gridDim.x];
+            if (i + DEPTH < ntile) {
+                // later tiles' loads are in flight while this one is stored
+                const int4 jn = job(i + DEPTH);
 #pragma unroll
-                for (int k = 0; k < FP_SLOTS; k++) load(P.seg[jn.y >> 16], jn, (i + 1) & 3, stid + k * FP_NST, nxt[k]);
+                for (int k = 0; k < SL; k++) {
+                    if (DEPTH == 2) load(P.seg[jn.y >> 16], jn, (i + DEPTH) & 3, stid + k * FP_NST, q2[k]);
+                    else load(P.seg[jn.y >> 16], jn, (i + DEPTH) & 3, stid + k * FP_NST, q1[k]);
+                }
             }
             if (!fp_wait(op_empty + b, (u & 1) ^ 1, abort)) break;
             unsigned char *bt = opr + b * LY.ob;
             const int nslot = (fwd_ncp<NLT>(t) >> 1) * (FOLD ? (njc >> 3) : (njc >> 2));
 #pragma unroll
-            for (int k = 0; k < FP_SLOTS; k++)
-                if (stid + k * FP_NST < nslot) store(t, p, stid + k * FP_NST, njc, bt, cur[k]);
-            for (int s = stid + FP_SLOTS * FP_NST; s < nslot; s += FP_NST) {   // beyond the slots in flight
+            for (int k = 0; k < SL; k++)
+                if (stid + k * FP_NST < nslot) store(t, p, stid + k * FP_NST, njc, bt, q0[k]);
+            for (int s = stid + SL * FP_NST; s < nslot; s += FP_NST) {   // beyond the slots in flight
                 F3Slot v;
                 load(A, jb, t, s, v);
                 store(t, p, s, njc, bt, v);
@@ -1140,7 +1152,10 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             tc::fence_proxy_async();   // these stores feed the tensor cores
             tc::mbar_arrive(op_full + b);
 #pragma unroll
-            for (int k = 0; k < FP_SLOTS; k++) cur[k] = nxt[k];
+            for (int k = 0; k < SL; k++) {
+                q0[k] = q1[k];
+                if (DEPTH == 2) q1[k] = q2[k];
+            }
         }
     }
     tc::fence_before_sync();
