@@ -219,7 +219,11 @@ EXOTX_API exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const voi
 
 EXOTX_API exotx_status exotx_tc_error(int *code, exotx_stream s) {
     if (!code) return EXOTX_BAD_ARG;
+    int fe = 0;
     EXOTX_TRY(tc_error_read(code, (cudaStream_t)s));
+    EXOTX_TRY(fft_error_read(&fe, (cudaStream_t)s));
+    *code |= fe;
+    EXOTX_TRY(fft_error_reset((cudaStream_t)s));
     return tc_error_reset((cudaStream_t)s);
 }
 

@@ -4,6 +4,8 @@
 // segments of one resolution and level count; each half of the round trip is
 // one tensor-core Legendre launch plus one FFT launch over all segments, so
 // the whole ensemble step is four kernels (and one CUDA graph when captured).
+// Segments whose rows have a register-resident FFT kernel (NLON 384) take one
+// FFT launch more per half when they are mixed with other lengths.
 #include <algorithm>
 #include <cmath>
 #include <map>

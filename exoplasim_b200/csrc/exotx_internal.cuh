@@ -195,6 +195,9 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
 bool tc_ens_fwd_folded(const EnsSeg *segs, int nseg);
 exotx_status tc_error_reset(cudaStream_t s);
 exotx_status tc_error_read(int *err, cudaStream_t s);
+// the same for the FFT kernels' bounded waits (fft.cu)
+exotx_status fft_error_reset(cudaStream_t s);
+exotx_status fft_error_read(int *err, cudaStream_t s);
 exotx_status tc_available();
 void tc_free(exotx_plan p);
 }  // namespace exotx

@@ -15,6 +15,7 @@
 #include <mutex>
 #include <vector>
 #include "exotx_internal.cuh"
+#include "tc_prims.cuh"
 
 namespace exotx {
 
@@ -563,6 +564,408 @@ __global__ void __launch_bounds__(256) k_rfft_fwd_fold(const T *gp, T *fc, int n
     rfft_fwd_fold_body<T, N, ROWS>(gp, fc, nlat, lot, kf, f_ms, wtab, rtab, blockIdx.x);
 }
 
+// ------------------------------------------------ register-resident transforms
+// For h = P*Q complex points with P | Q, P threads work a row:
+//   Z[q + Q m] = sum_t W_P^{t m} W_h^{t q} sum_j z[t + P j] W_Q^{j q}   (W = e^{-2 pi i/.})
+// Thread t takes the Q-point DFT of its column z[t + P j] in registers and
+// applies W_h^{t q}; one transposition through shared memory then hands it the
+// Q/P whole P-point DFTs q = (Q/P) t + i.  The inverse runs the same steps in
+// the other order.  A block of 256 threads works RB = 256/P rows.  The grid
+// rows and the block's Fourier coefficients move between global and shared
+// memory as bulk (TMA) copies, so the load/store unit only serves
+// bank-conflict-free shared-memory accesses; the twiddles W_h^{t q} sit in a
+// per-block table, Q contiguous values per t.
+__device__ int g_fft_error;   // nonzero: a bounded wait in an FFT kernel gave up
+
+template <int N> struct RfShape { static constexpr int P = 0, Q = 0; };
+template <> struct RfShape<384> { static constexpr int P = 8, Q = 24; };
+template <int N> constexpr bool rf_len() { return RfShape<N>::P > 0; }
+// Shared memory (complex units unless noted), P = 8:
+//   region R, reused in turn for the staged grid rows (row stride RG = 8 mod 16:
+//   the two rows of a half-warp on different banks), the transposition (a
+//   thread's Q values at stride RT with RT/2 odd, so 8 row-mates' 16-byte
+//   accesses fall on distinct banks; rows at stride RS = 8 mod 16), the
+//   spectra (odd row stride RZ: 16 rows read at one k on distinct banks) and
+//   the staged coefficients of the inverse (k-major, stride RC = RB + 2);
+//   then the twiddle table tq[t * RT + q] = W_h^{t q}, the split twiddles
+//   rt[k] = e^{-2 pi i k/n} (k < h), and the copy barrier.
+template <int N> struct RfLayout {
+    static constexpr int P = RfShape<N>::P, Q = RfShape<N>::Q, H = N / 2, RB = 256 / P;
+    static constexpr int RT = Q + 2;
+    static constexpr int RS = P * RT + ((8 - (P * RT) % 16) + 16) % 16;
+    static constexpr int RZ = H + 1;
+    static constexpr int RG = H + 8 + ((H + 8) % 16 == 8 ? 0 : 8);
+    static constexpr int RC = RB + 2;
+    static constexpr int R = RB * (RS > RZ ? (RS > RG ? RS : RG) : (RZ > RG ? RZ : RG));
+    static constexpr size_t OFF_TQ = (size_t)R * 8, OFF_RT = OFF_TQ + (size_t)P * RT * 8,
+                            OFF_BAR = OFF_RT + (size_t)H * 8, SMEM = OFF_BAR + 16;
+    static_assert(P == 8 && Q % P == 0 && Q % 4 == 0 && (RT / 2) % 2 == 1 && RS % 16 == 8 && RG % 16 == 8, "layout");
+    static_assert(H * RC <= R, "the staged coefficients fit region R");
+    static_assert(RB == 32, "warp 0 issues one row copy per lane");
+};
+
+// cos(2 pi a / 24) for an integer a (multiples of 15 degrees)
+__host__ __device__ constexpr double cos24(int a) {
+    a = ((a % 24) + 24) % 24;
+    if (a > 12) a = 24 - a;
+    switch (a) {
+        case 0: return 1.0;
+        case 1: return 0.96592582628906828675;
+        case 2: return 0.86602540378443864676;
+        case 3: return 0.70710678118654752440;
+        case 4: return 0.5;
+        case 5: return 0.25881904510252076235;
+        case 6: return 0.0;
+        case 7: return -0.25881904510252076235;
+        case 8: return -0.5;
+        case 9: return -0.70710678118654752440;
+        case 10: return -0.86602540378443864676;
+        case 11: return -0.96592582628906828675;
+        default: return -1.0;
+    }
+}
+// v * e^{S 2 pi i a / 24} for a constant a
+template <typename T, int S>
+__device__ __forceinline__ cpx<T> cmul_w24(cpx<T> v, int a) {
+    a %= 24;
+    if (a == 0) return v;
+    if (a == 6) return rot90<T, S>(v);
+    if (a == 12) return cpx<T>{-v.x, -v.y};
+    if (a == 18) return rot90<T, -S>(v);
+    const T c = (T)cos24(a), s = (T)(S * cos24(a - 6));   // sin(x) = cos(x - pi/2)
+    return cpx<T>{v.x * c - v.y * s, v.x * s + v.y * c};
+}
+// 24-point DFT in registers, V[k] = sum_n v[n] e^{S 2 pi i nk/24}:
+// n = 8 n1 + n2, k = k1 + 3 k2; 3-point DFTs over n1, twiddles W_24^{n2 k1},
+// 8-point DFTs over n2
+template <typename T, int S>
+__device__ __forceinline__ void dft24(cpx<T> *v) {
+    cpx<T> a[24];
+#pragma unroll
+    for (int n2 = 0; n2 < 8; n2++) {
+        cpx<T> t[3] = {v[n2], v[8 + n2], v[16 + n2]};
+        dft3<T, S>(t);
+#pragma unroll
+        for (int k1 = 0; k1 < 3; k1++) a[3 * n2 + k1] = cmul_w24<T, S>(t[k1], n2 * k1);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 3; k1++) {
+        cpx<T> t[8];
+#pragma unroll
+        for (int n2 = 0; n2 < 8; n2++) t[n2] = a[3 * n2 + k1];
+        dft8<T, S>(t);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++) v[k1 + 3 * k2] = t[k2];
+    }
+}
+template <typename T, int S, int Q>
+__device__ __forceinline__ void dftQ(cpx<T> *v) {
+    static_assert(Q == 24, "register DFT length");
+    dft24<T, S>(v);
+}
+
+// bulk copy shared -> global in this thread's bulk group (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void bulk_s2g(void *dst_gmem, const void *src_smem, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem),
+                 "r"(tc::smem_u32(src_smem)), "r"(bytes)
+                 : "memory");
+}
+// returns once this thread's bulk stores have read their shared-memory sources
+__device__ __forceinline__ void bulk_commit_wait_read() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+template <int N>
+struct RfSmem {
+    using Lay = RfLayout<N>;
+    cpx<float> *r, *tq, *rt;
+    uint64_t *bar;
+    __device__ explicit RfSmem(unsigned char *raw)
+        : r(reinterpret_cast<cpx<float> *>(raw)), tq(reinterpret_cast<cpx<float> *>(raw + Lay::OFF_TQ)),
+          rt(reinterpret_cast<cpx<float> *>(raw + Lay::OFF_RT)), bar(reinterpret_cast<uint64_t *>(raw + Lay::OFF_BAR)) {}
+};
+
+// Block set-up from constant data only (runs before the dependent-launch wait):
+// the copy barrier and the per-block twiddle tables.  Ends with a block barrier.
+template <int N>
+__device__ __forceinline__ void rf_setup(const RfSmem<N> &S, const cpx<float> *__restrict__ w,
+                                         const cpx<float> *__restrict__ rt) {
+    using Lay = RfLayout<N>;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(S.bar, 1);
+        tc::mbar_fence_init();
+    }
+    for (int i = threadIdx.x; i < Lay::P * Lay::Q; i += blockDim.x) {
+        const int t = i / Lay::Q, q = i - t * Lay::Q;
+        S.tq[t * Lay::RT + q] = w[t * q];   // t q < h
+    }
+    for (int k = threadIdx.x; k < Lay::H; k += blockDim.x) S.rt[k] = rt[k];
+    __syncthreads();
+}
+
+// Waits for the block's bulk loads; false (block-uniform, error word set) if the bounded wait gave up.
+__device__ __forceinline__ bool rf_wait_loads(uint64_t *bar) {
+    const bool ok = __syncthreads_and(tc::mbar_wait(bar, 0)) != 0;
+    if (!ok && threadIdx.x == 0) atomicExch(&g_fft_error, 1);
+    return ok;
+}
+
+// Forward complex transform of the block's RB rows; afterwards row r's Z[k]
+// sits at S.r[r * RZ + k] (visible to the block).  grow(r) is row r's index in
+// g (rows of n floats), or < 0 for a zero row.  False if the loads timed out.
+template <int N, typename RowOf>
+__device__ __forceinline__ bool rf_forward_rows(const float *__restrict__ g, RowOf grow, const RfSmem<N> &S) {
+    using Lay = RfLayout<N>;
+    constexpr int P = Lay::P, Q = Lay::Q, H = Lay::H, QP = Q / P;
+    const int t = threadIdx.x % P, r = threadIdx.x / P;
+    if (threadIdx.x < 32) {   // warp 0: one bulk copy per row
+        const long long gr = grow(threadIdx.x);
+        const unsigned valid = __ballot_sync(0xffffffffu, gr >= 0);
+        if (threadIdx.x == 0) tc::mbar_arrive_expect_tx(S.bar, (uint32_t)__popc(valid) * (uint32_t)(N * 4));
+        __syncwarp();
+        if (gr >= 0) tc::bulk_g2s(S.r + threadIdx.x * Lay::RG, g + gr * N, N * 4, S.bar);
+    }
+    if (grow(r) < 0) {   // zero rows: written here, never by a copy
+        for (int j = t; j < H; j += P) S.r[r * Lay::RG + j] = cpx<float>{0.f, 0.f};
+    }
+    if (!rf_wait_loads(S.bar)) return false;
+    cpx<float> v[Q];
+    const cpx<float> *s = S.r + r * Lay::RG + t;
+#pragma unroll
+    for (int j = 0; j < Q; j++) v[j] = s[P * j];
+    dftQ<float, -1, Q>(v);
+    const cpx<float> *tq = S.tq + t * Lay::RT;
+#pragma unroll
+    for (int q = 2; q < Q; q += 2) {
+        const float4 f = *reinterpret_cast<const float4 *>(tq + q);
+        v[q] = cmul(v[q], cpx<float>{f.x, f.y});
+        v[q + 1] = cmul(v[q + 1], cpx<float>{f.z, f.w});
+    }
+    v[1] = cmul(v[1], tq[1]);
+    __syncthreads();   // the staged rows are read; the transposition overwrites them
+    cpx<float> *x = S.r + r * Lay::RS;
+#pragma unroll
+    for (int q = 0; q < Q; q += 2)
+        *reinterpret_cast<float4 *>(x + t * Lay::RT + q) = make_float4(v[q].x, v[q].y, v[q + 1].x, v[q + 1].y);
+    __syncthreads();
+    cpx<float> z[QP][P];
+#pragma unroll
+    for (int i = 0; i < QP; i++) {
+#pragma unroll
+        for (int u = 0; u < P; u++) z[i][u] = x[u * Lay::RT + QP * t + i];
+        dft8<float, -1>(z[i]);
+    }
+    __syncthreads();   // the spectra overwrite the transposition buffer
+    cpx<float> *zs = S.r + r * Lay::RZ;
+#pragma unroll
+    for (int i = 0; i < QP; i++)
+#pragma unroll
+        for (int m = 0; m < P; m++) zs[QP * t + i + Q * m] = z[i][m];
+    __syncthreads();
+    return true;
+}
+
+// the Fourier coefficient X_k of a real row from Z_k and Z_{h-k} of its
+// half-length complex transform (k > 0), scaled by 1/n
+__device__ __forceinline__ cpx<float> rf_split(cpx<float> a, cpx<float> b, cpx<float> wk, float scale) {
+    const cpx<float> E{0.5f * (a.x + b.x), 0.5f * (a.y - b.y)};
+    const cpx<float> O{0.5f * (a.y + b.y), 0.5f * (b.x - a.x)};
+    const cpx<float> wo = cmul(wk, O);
+    return cpx<float>{(E.x + wo.x) * scale, (E.y + wo.y) * scale};
+}
+
+// rfft_fwd_ct_body for the register-resident lengths: RB rows per block
+template <int N>
+__device__ __forceinline__ void rfft_fwd_rf_body(const float *gp, float *fc, long long lot, int kf, long long f_rs,
+                                                 long long f_ms, const cpx<float> *__restrict__ w,
+                                                 const cpx<float> *__restrict__ rt, long long blk) {
+    using Lay = RfLayout<N>;
+    constexpr int H = Lay::H, RB = Lay::RB;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const RfSmem<N> S(smraw);
+    const long long row0 = blk * RB;
+    const int rows = (int)min((long long)RB, lot - row0);
+    pdl_trigger();
+    rf_setup<N>(S, w, rt);
+    pdl_wait();   // the grid rows may come from the previous kernel
+    if (!rf_forward_rows<N>(gp, [&](int r) { return r < rows ? row0 + r : -1ll; }, S)) return;
+    const float scale = 1.f / (float)N;
+    const int kh = min(H / 2, kf - 1);   // pairs (k, h-k) with k <= kh cover every k < kf
+    const bool kfast = f_ms == 1;        // row-major Fourier side: k fastest across threads
+    for (int it = threadIdx.x; it < RB * (kh + 1); it += blockDim.x) {
+        const int r = kfast ? it / (kh + 1) : it % RB, k = kfast ? it - r * (kh + 1) : it / RB, k2 = H - k;
+        if (r >= rows) continue;
+        const cpx<float> *z = S.r + r * Lay::RZ;
+        cpx<float> *fr = reinterpret_cast<cpx<float> *>(fc) + (row0 + r) * f_rs;
+        const cpx<float> a = z[k];
+        if (k == 0) {
+            fr[0] = cpx<float>{(a.x + a.y) * scale, 0.f};
+            continue;
+        }
+        const cpx<float> b = z[k2];
+        fr[(long long)k * f_ms] = rf_split(a, b, S.rt[k], scale);
+        if (k2 < kf && k2 != k) fr[(long long)k2 * f_ms] = rf_split(b, a, S.rt[k2], scale);
+    }
+}
+
+// rfft_fwd_fold_body for the register-resident lengths: a block takes RB/2
+// latitude pairs of one field, rows r and r + RB/2 being a pair's northern and
+// southern rows
+template <int N>
+__device__ __forceinline__ void rfft_fwd_fold_rf_body(const float *gp, float *fc, int nlat, long long lot, int kf,
+                                                      long long f_ms, const cpx<float> *__restrict__ w,
+                                                      const cpx<float> *__restrict__ rt, long long blk) {
+    using Lay = RfLayout<N>;
+    constexpr int H = Lay::H, RB = Lay::RB, PR = RB / 2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const RfSmem<N> S(smraw);
+    const int nlath = nlat / 2, nbpf = (nlath + PR - 1) / PR;
+    const long long field = blk / nbpf;
+    const int j0 = (int)(blk - field * nbpf) * PR;
+    const bool fin = field * nlat < lot;
+    pdl_trigger();
+    rf_setup<N>(S, w, rt);
+    pdl_wait();   // the grid rows may come from the previous kernel, which may still read the output
+    auto grow = [&](int r) {
+        const int j = j0 + (r % PR);
+        return (fin && j < nlath) ? field * nlat + (r < PR ? j : nlat - 1 - j) : -1ll;
+    };
+    if (!rf_forward_rows<N>(gp, grow, S)) return;
+    const float scale = 1.f / (float)N;
+    auto put = [&](long long row, int k, cpx<float> xn, cpx<float> xs) {
+        cpx<float> *fr = reinterpret_cast<cpx<float> *>(fc) + row + (long long)k * f_ms;
+        fr[0] = cpx<float>{xn.x + xs.x, xn.y + xs.y};
+        fr[nlath] = cpx<float>{xn.x - xs.x, xn.y - xs.y};
+    };
+    const int kh = min(H / 2, kf - 1);
+    for (int it = threadIdx.x; it < PR * (kh + 1); it += blockDim.x) {
+        const int pr = it % PR, k = it / PR, k2 = H - k, j = j0 + pr;
+        if (!fin || j >= nlath) continue;
+        const long long row = field * nlat + j;     // E row; O is nlath further
+        const cpx<float> *zn = S.r + pr * Lay::RZ, *zs = S.r + (pr + PR) * Lay::RZ;
+        const cpx<float> an = zn[k], as = zs[k];
+        if (k == 0) {
+            put(row, 0, cpx<float>{(an.x + an.y) * scale, 0.f}, cpx<float>{(as.x + as.y) * scale, 0.f});
+            continue;
+        }
+        const cpx<float> bn = zn[k2], bs = zs[k2], wk = S.rt[k];
+        put(row, k, rf_split(an, bn, wk, scale), rf_split(as, bs, wk, scale));
+        if (k2 < kf && k2 != k) {
+            const cpx<float> wk2 = S.rt[k2];
+            put(row, k2, rf_split(bn, an, wk2, scale), rf_split(bs, as, wk2, scale));
+        }
+    }
+}
+
+// rfft_inv_ct_body for the register-resident lengths: the block's
+// coefficients c_k (k < kf) are staged k-major in shared memory; each thread
+// forms the Z_k of its own q from c_k and c_{h-k}, takes their P-point DFTs,
+// and after the transposition the Q-point DFT of its column; the grid rows
+// leave through shared memory as one bulk store each
+template <int N>
+__device__ __forceinline__ void rfft_inv_rf_body(const float *fc, float *gp, long long lot, int kf, long long f_rs,
+                                                 long long f_ms, const cpx<float> *__restrict__ w,
+                                                 const cpx<float> *__restrict__ rt, long long blk) {
+    using Lay = RfLayout<N>;
+    constexpr int P = Lay::P, Q = Lay::Q, H = Lay::H, RB = Lay::RB, QP = Q / P;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const RfSmem<N> S(smraw);
+    const long long row0 = blk * RB;
+    const int rows = (int)min((long long)RB, lot - row0);
+    const int t = threadIdx.x % P, r = threadIdx.x / P;
+    pdl_trigger();
+    rf_setup<N>(S, w, rt);
+    pdl_wait();   // the coefficients come from the previous kernel
+    const cpx<float> *fcc = reinterpret_cast<const cpx<float> *>(fc);
+    cpx<float> *cs = S.r;   // c_k of row r at cs[k * RC + r]
+    // bulk copies when each k's rows are one 16-byte-aligned run of the m-major side
+    const bool bulk = f_rs == 1 && !(f_ms & 1) && !(rows & 1) && !(reinterpret_cast<uintptr_t>(fc) & 15);
+    if (bulk) {
+        if (threadIdx.x < 32) {
+            if (threadIdx.x == 0) tc::mbar_arrive_expect_tx(S.bar, (uint32_t)kf * (uint32_t)rows * 8u);
+            __syncwarp();
+            for (int k = threadIdx.x; k < kf; k += 32)
+                tc::bulk_g2s(cs + k * Lay::RC, fcc + row0 + (long long)k * f_ms, (uint32_t)rows * 8u, S.bar);
+        }
+        if (!rf_wait_loads(S.bar)) return;
+    } else {
+        for (int i = threadIdx.x; i < kf * RB; i += blockDim.x) {
+            const int k = i / RB, rr = i - k * RB;
+            if (rr < rows) cs[k * Lay::RC + rr] = fcc[(row0 + rr) * f_rs + (long long)k * f_ms];
+        }
+        __syncthreads();
+    }
+    cpx<float> z[QP][P];
+#pragma unroll
+    for (int i = 0; i < QP; i++) {
+        const int q = QP * t + i;
+#pragma unroll
+        for (int m = 0; m < P; m++) {
+            const int k = q + Q * m, k2 = H - k;
+            cpx<float> a{0.f, 0.f}, b{0.f, 0.f};
+            if (k < kf) {
+                a = cs[k * Lay::RC + r];
+                if (k == 0) a.y = 0.f;
+            }
+            if (k > 0 && k2 < kf) b = cs[k2 * Lay::RC + r];
+            // Z_k of the half-length complex sequence (c = 0 for k >= kf, the m = 0 imaginary part ignored)
+            const cpx<float> E{a.x + b.x, a.y - b.y}, D{a.x - b.x, a.y + b.y};
+            cpx<float> wk = S.rt[k];
+            wk.y = -wk.y;
+            const cpx<float> O = cmul(D, wk);
+            z[i][m] = cpx<float>{E.x - O.y, E.y + O.x};
+        }
+        dft8<float, +1>(z[i]);
+    }
+    __syncthreads();   // the staged coefficients are read; the transposition overwrites them
+    cpx<float> *x = S.r + r * Lay::RS;
+#pragma unroll
+    for (int i = 0; i < QP; i++)
+#pragma unroll
+        for (int u = 0; u < P; u++) x[u * Lay::RT + QP * t + i] = z[i][u];
+    __syncthreads();
+    cpx<float> v[Q];
+    const cpx<float> *tq = S.tq + t * Lay::RT;
+#pragma unroll
+    for (int q = 0; q < Q; q += 2) {
+        const float4 f = *reinterpret_cast<const float4 *>(x + t * Lay::RT + q);
+        const float4 wq = *reinterpret_cast<const float4 *>(tq + q);
+        v[q] = q ? cmul(cpx<float>{f.x, f.y}, cpx<float>{wq.x, -wq.y}) : cpx<float>{f.x, f.y};
+        v[q + 1] = cmul(cpx<float>{f.z, f.w}, cpx<float>{wq.z, -wq.w});
+    }
+    dftQ<float, +1, Q>(v);
+    __syncthreads();   // the transposition is read; the grid rows are staged over it
+    cpx<float> *gs = S.r + r * Lay::RG + t;
+#pragma unroll
+    for (int j = 0; j < Q; j++) gs[P * j] = v[j];
+    tc::fence_proxy_async();   // the staged rows feed the bulk stores
+    __syncthreads();
+    if (threadIdx.x < rows) {
+        bulk_s2g(gp + (row0 + threadIdx.x) * N, S.r + threadIdx.x * Lay::RG, N * 4);
+        bulk_commit_wait_read();
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_rfft_fwd_rf(const float *gp, float *fc, long long lot, int kf, long long f_rs,
+                                                      long long f_ms, const cpx<float> *__restrict__ w,
+                                                      const cpx<float> *__restrict__ rt) {
+    rfft_fwd_rf_body<N>(gp, fc, lot, kf, f_rs, f_ms, w, rt, blockIdx.x);
+}
+template <int N>
+__global__ void __launch_bounds__(256) k_rfft_inv_rf(const float *fc, float *gp, long long lot, int kf, long long f_rs,
+                                                      long long f_ms, const cpx<float> *__restrict__ w,
+                                                      const cpx<float> *__restrict__ rt) {
+    rfft_inv_rf_body<N>(fc, gp, lot, kf, f_rs, f_ms, w, rt, blockIdx.x);
+}
+template <int N>
+__global__ void __launch_bounds__(256) k_rfft_fwd_fold_rf(const float *gp, float *fc, int nlat, long long lot, int kf,
+                                                           long long f_ms, const cpx<float> *__restrict__ w,
+                                                           const cpx<float> *__restrict__ rt) {
+    rfft_fwd_fold_rf_body<N>(gp, fc, nlat, lot, kf, f_ms, w, rt, blockIdx.x);
+}
+
 // ---------------------------------------------------------------- ensembles
 // One launch transforms the rows of up to FFT_ENS_MAXSEG segments of different
 // lengths (an uneven ensemble); block b belongs to the last segment whose
@@ -598,36 +1001,48 @@ __global__ void __launch_bounds__(256) k_rfft_ens(const __grid_constant__ FftEns
         EXOTX_FFT_ENS_CASE(192)
         EXOTX_FFT_ENS_CASE(256)
         EXOTX_FFT_ENS_CASE(320)
-        EXOTX_FFT_ENS_CASE(384)
         EXOTX_FFT_ENS_CASE(512)
 #undef EXOTX_FFT_ENS_CASE
         default: break;
+    }
+}
+// the register-resident lengths (more registers per thread) in a launch of their own
+template <bool FWD>
+__global__ void __launch_bounds__(256) k_rfft_ens_rf(const __grid_constant__ FftEnsLaunch P) {
+    int s = 0;
+    while (s + 1 < P.nseg && P.seg[s + 1].block0 <= (int)blockIdx.x) s++;
+    const FftEnsArgs &S = P.seg[s];
+    const long long blk = (long long)blockIdx.x - S.block0;
+    if (S.n == 384) {
+        if (FWD && S.fold_nlat) rfft_fwd_fold_rf_body<384>(S.in, S.out, S.fold_nlat, S.lot, S.kf, S.f_ms, S.w, S.r, blk);
+        else if (FWD) rfft_fwd_rf_body<384>(S.in, S.out, S.lot, S.kf, S.f_rs, S.f_ms, S.w, S.r, blk);
+        else rfft_inv_rf_body<384>(S.in, S.out, S.lot, S.kf, S.f_rs, S.f_ms, S.w, S.r, blk);
     }
 }
 
 static bool ens_len(int n) {
     return n == 64 || n == 128 || n == 192 || n == 256 || n == 320 || n == 384 || n == 512;
 }
+static bool rf_len_host(int n) { return n == 384; }
 static bool aligned16_(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s) {
-    if (nseg < 1 || nseg > FFT_ENS_MAXSEG) return EXOTX_BAD_ARG;
+// one launch over the segments whose lengths have (rf) or have not (!rf) a
+// register-resident kernel
+static exotx_status fft_ens_group(bool fwd, bool rf, const FftEnsSeg *segs, int nseg, cudaStream_t s) {
     FftEnsLaunch P;
-    P.nseg = nseg;
+    P.nseg = 0;
     int blocks = 0;
     size_t smem = 0;
     for (int i = 0; i < nseg; i++) {
         const FftEnsSeg &g = segs[i];
-        if (!ens_len(g.n)) return EXOTX_NOT_BUILT;
-        if (!aligned16_(g.in) || !aligned16_(g.out)) return EXOTX_BAD_ARG;
+        if (rf_len_host(g.n) != rf) continue;
         exotx_status st;
         const FftTables *t = fft_tables(g.n, &st);
         if (!t) return st;
-        const int rows = ct_rows<float>(g.n);
-        FftEnsArgs &a = P.seg[i];
+        const int rows = rf ? RfLayout<384>::RB : ct_rows<float>(g.n);
+        FftEnsArgs &a = P.seg[P.nseg++];
         a.in = g.in; a.out = g.out; a.lot = g.lot; a.f_rs = g.f_rs; a.f_ms = g.f_ms; a.n = g.n; a.kf = g.kf;
         a.fold_nlat = fwd ? g.fold_nlat : 0;
-        if (a.fold_nlat && (g.n != 2 * g.fold_nlat || g.lot % g.fold_nlat || g.f_rs != 1)) return EXOTX_BAD_ARG;
         a.w = reinterpret_cast<const cpx<float> *>(t->w32);
         a.r = reinterpret_cast<const cpx<float> *>(t->r32);
         a.block0 = blocks;
@@ -638,22 +1053,31 @@ exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s) 
             blocks += (int)((g.lot + rows - 1) / rows);
         }
         const int hp = g.n / 2 + 2 * (g.n / 32);   // padded row, as fpad_row
-        smem = std::max(smem, 2 * (size_t)rows * hp * sizeof(cpx<float>));
+        smem = std::max(smem, rf ? RfLayout<384>::SMEM : 2 * (size_t)rows * hp * sizeof(cpx<float>));
     }
     if (blocks == 0) return EXOTX_OK;
     const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
-    if (fwd) {
-        if (smem > 48 * 1024)
-            EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_ens<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    } else if (smem > 48 * 1024) {
-        EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_ens<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
+    void (*k)(FftEnsLaunch) = rf ? (fwd ? k_rfft_ens_rf<true> : k_rfft_ens_rf<false>)
+                                 : (fwd ? k_rfft_ens<true> : k_rfft_ens<false>);
+    if (smem > 48 * 1024) EXOTX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cudaEvent_t ev = ktimer_start(kid, s);
-    if (fwd) k_rfft_ens<true><<<blocks, 256, smem, s>>>(P);
-    else k_rfft_ens<false><<<blocks, 256, smem, s>>>(P);
+    k<<<blocks, 256, smem, s>>>(P);
     EXOTX_CHECK_LAUNCH();
     ktimer_stop(kid, s, ev);
     return EXOTX_OK;
+}
+
+exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s) {
+    if (nseg < 1 || nseg > FFT_ENS_MAXSEG) return EXOTX_BAD_ARG;
+    for (int i = 0; i < nseg; i++) {
+        const FftEnsSeg &g = segs[i];
+        if (!ens_len(g.n)) return EXOTX_NOT_BUILT;
+        if (!aligned16_(g.in) || !aligned16_(g.out)) return EXOTX_BAD_ARG;
+        const int fold = fwd ? g.fold_nlat : 0;
+        if (fold && (g.n != 2 * fold || g.lot % fold || g.f_rs != 1)) return EXOTX_BAD_ARG;
+    }
+    EXOTX_TRY(fft_ens_group(fwd, false, segs, nseg, s));
+    return fft_ens_group(fwd, true, segs, nseg, s);
 }
 
 template <typename T, int N>
@@ -685,10 +1109,35 @@ static exotx_status launch_ct(bool fwd, const T *in, T *out, long long lot, int 
     return EXOTX_OK;
 }
 
+template <int N>
+static exotx_status launch_rf(bool fwd, const float *in, float *out, long long lot, int kf, long long f_rs,
+                              long long f_ms, const cpx<float> *w, const cpx<float> *r, cudaStream_t s) {
+    using Lay = RfLayout<N>;
+    const long long nb = (lot + Lay::RB - 1) / Lay::RB;
+    const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
+    if (fwd)
+        EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_rf<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM));
+    else
+        EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_inv_rf<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM));
+    cudaEvent_t ev = ktimer_start(kid, s);
+    if (fwd)
+        EXOTX_CUDA(launch_pdl(k_rfft_fwd_rf<N>, dim3((unsigned)nb), dim3(256), Lay::SMEM, s, in, out, lot, kf, f_rs,
+                              f_ms, w, r));
+    else
+        EXOTX_CUDA(launch_pdl(k_rfft_inv_rf<N>, dim3((unsigned)nb), dim3(256), Lay::SMEM, s, in, out, lot, kf, f_rs,
+                              f_ms, w, r));
+    EXOTX_CHECK_LAUNCH();
+    ktimer_stop(kid, s, ev);
+    return EXOTX_OK;
+}
+
 // returns EXOTX_NOT_BUILT when n has no specialised kernel
 template <typename T>
 static exotx_status dispatch_ct(bool fwd, int n, const T *in, T *out, long long lot, int kf, long long f_rs,
                                 long long f_ms, const cpx<T> *w, const cpx<T> *r, cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {   // single precision: register-resident kernels where built
+        if (n == 384) return launch_rf<384>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
+    }
     switch (n) {
         case 64: return launch_ct<T, 64>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
         case 128: return launch_ct<T, 128>(fwd, in, out, lot, kf, f_rs, f_ms, w, r, s);
@@ -847,6 +1296,19 @@ template exotx_status fft_forward_l<float>(const float *, float *, int, long lon
 template <int N>
 static exotx_status launch_fold(const float *in, float *out, int nlat, long long lot, int kf, long long f_ms,
                                 const cpx<float> *w, const cpx<float> *r, cudaStream_t s) {
+    if constexpr (rf_len<N>()) {
+        using Lay = RfLayout<N>;
+        const int nbpf = (nlat / 2 + Lay::RB / 2 - 1) / (Lay::RB / 2);
+        const long long nb = (lot / nlat) * nbpf;
+        EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_fold_rf<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)Lay::SMEM));
+        cudaEvent_t ev = ktimer_start(EXOTX_K_FFT_FORWARD, s);
+        EXOTX_CUDA(launch_pdl(k_rfft_fwd_fold_rf<N>, dim3((unsigned)nb), dim3(256), Lay::SMEM, s, in, out, nlat, lot,
+                              kf, f_ms, w, r));
+        EXOTX_CHECK_LAUNCH();
+        ktimer_stop(EXOTX_K_FFT_FORWARD, s, ev);
+        return EXOTX_OK;
+    }
     constexpr int ROWS = ct_rows<float>(N);
     const size_t smem = 2 * ROWS * fpad_row<N / 2>() * sizeof(cpx<float>);
     const int nbpf = (nlat / 2 + ROWS / 2 - 1) / (ROWS / 2);
@@ -889,6 +1351,17 @@ template exotx_status fft_inverse_l<double>(const double *, double *, int, long 
                                             cudaStream_t);
 template exotx_status fft_inverse_l<float>(const float *, float *, int, long long, int, long long, long long,
                                            cudaStream_t);
+
+exotx_status fft_error_reset(cudaStream_t s) {
+    int zero = 0;
+    EXOTX_CUDA(cudaMemcpyToSymbolAsync(g_fft_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+    return EXOTX_OK;
+}
+exotx_status fft_error_read(int *err, cudaStream_t s) {
+    EXOTX_CUDA(cudaMemcpyFromSymbolAsync(err, g_fft_error, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+    EXOTX_CUDA(cudaStreamSynchronize(s));
+    return EXOTX_OK;
+}
 
 // ----------------------------------------------- caller-supplied twiddle tables
 // The twiddle values the cached tables hold (same long-double evaluation, so

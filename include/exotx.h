@@ -205,8 +205,9 @@ typedef enum {
 exotx_status exotx_kernel_timing(int enable);
 exotx_status exotx_kernel_time(int kernel, double *ms, long long *launches);
 
-/* Error word of the tensor-core kernels (0 = none; nonzero = a bounded
- * device-side wait gave up), read after synchronising the stream, then reset. */
+/* Error word of the tensor-core and FFT kernels (0 = none; nonzero = a
+ * bounded device-side wait gave up), read after synchronising the stream,
+ * then reset. */
 exotx_status exotx_tc_error(int *code, exotx_stream s);
 
 /* ---- radiation column pass (radmod.f90 radstep :927-1110) ---- */
