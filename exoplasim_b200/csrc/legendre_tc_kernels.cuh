@@ -872,7 +872,8 @@ __host__ __device__ inline FpLayout fp_layout(int njmax) {
     L.bars = (L.bars + 15) & ~15u;
     return L;
 }
-static size_t fpipe_smem(int njmax) { return fp_layout(njmax).bars + 32 * 8; }
+constexpr int FP_JOBS = 512;             // jobs of a CTA kept in shared memory (later ones are read from global)
+static size_t fpipe_smem(int njmax) { return fp_layout(njmax).bars + 32 * 8 + FP_JOBS * 16; }
 
 // bounded wait that also gives up as soon as another role has aborted
 __device__ __forceinline__ bool fp_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
@@ -942,12 +943,19 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
     uint64_t *acc_full = bars + 8, *acc_empty = bars + 11, *ep_bar = bars + 14;
     uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 15);
     volatile int *abort = reinterpret_cast<volatile int *>(bars + 16);
+    int4 *jobs_s = reinterpret_cast<int4 *>(sm + LY.bars + 32 * 8);
     const int nprod = P.nprod;
     const int njobs = P.njobs;
     // tiles of this CTA: jobs blockIdx.x + k gridDim.x, four tables each
     const int mine = njobs > (int)blockIdx.x ? (njobs - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int ntile = 4 * mine;
     pdl_trigger();
+    // this CTA's job descriptors, read once (host-written, so before the dependent-launch wait)
+    for (int k = tid; k < mine && k < FP_JOBS; k += FP_THREADS) jobs_s[k] = P.jobs[blockIdx.x + k * gridDim.x];
+    auto job = [&](int i) {
+        const int k = i >> 2;
+        return k < FP_JOBS ? jobs_s[k] : P.jobs[blockIdx.x + k * gridDim.x];
+    };
     if (warp == 0) tc::tmem_alloc(slot, 512);
     if (tid == 0) {
         for (int i = 0; i < 2; i++) {
@@ -976,7 +984,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             for (int i = 0; i < ntile; i++) {
                 const int b = i & 1, u = i >> 1;
                 if (!fp_wait(tab_empty + b, (u & 1) ^ 1, abort)) break;
-                const int4 jb = P.jobs[blockIdx.x + (i >> 2) * gridDim.x];
+                const int4 jb = job(i);
                 const TcFwd3Args &A = P.seg[jb.y >> 16];
                 const int m = jb.x, p = jb.w >> 8, t = i & 3;
                 const uint32_t tbytes = 8u * (uint32_t)pad8(kpar(A.ntp1 - m, p)) * (uint32_t)A.njc;
@@ -999,7 +1007,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
                     !fp_wait(acc_empty + a, (ua & 1) ^ 1, abort))
                     break;
                 tc::fence_after_sync();
-                const int4 jb = P.jobs[blockIdx.x + (i >> 2) * gridDim.x];
+                const int4 jb = job(i);
                 const TcFwd3Args &A = P.seg[jb.y >> 16];
                 const int m = jb.x, p = jb.w >> 8, t = i & 3;
                 const int R = pad8(kpar(A.ntp1 - m, p)), njc = A.njc;
@@ -1034,11 +1042,13 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
         const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
         constexpr int NO = NLT * 8 + 2;
         float o[NLT][4][2], ov[2];
+        float fl = 0.f;   // the job's filter factor and output offset, loaded when the job starts
+        int wom = 0;
         bool ok = true;
         uint32_t ep_phase = 0;
         for (int i = 0; i < ntile && ok; i++) {
             const int a = i % 3, ua = i / 3, t = i & 3;
-            const int4 jb = P.jobs[blockIdx.x + (i >> 2) * gridDim.x];
+            const int4 jb = job(i);
             const TcFwd3Args &A = P.seg[jb.y >> 16];
             const int m = jb.x, inst = jb.y & 0xffff, l0 = jb.z, nl = jb.w & 0xff, p = jb.w >> 8;
             const int Kq = kpar(A.ntp1 - m, p), R = pad8(Kq);
@@ -1048,6 +1058,8 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
 #pragma unroll
                     for (int k = 0; k < 4; k++) o[li][k][0] = o[li][k][1] = 0.f;
                 ov[0] = ov[1] = 0.f;
+                if (r < Kq) fl = A.filt[m + 2 * r + p];
+                wom = A.woff[m];
             }
             ok = __all_sync(0xffffffffu, fp_wait(acc_full + a, ua & 1, abort));   // warp-uniform
             if (!ok) break;
@@ -1075,8 +1087,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             if (r < Kq) {
                 const float *e = E + (size_t)r * NO;
                 const int L = A.L, nfo = 4 * L + 1, k = 2 * r + p;   // k = n - m
-                const float fl = A.filt[m + k];
-                const size_t wo = (size_t)A.woff[m] + k;
+                const size_t wo = (size_t)wom + k;
 #pragma unroll
                 for (int li = 0; li < NLT; li++) {
                     if (li >= nl) break;
@@ -1113,7 +1124,6 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             if constexpr (FOLD) f3_store_fold<NLT>(t, sl, njc, bt, v);
             else f3_store<NLT>(t, p, sl, njc, bt, v);
         };
-        auto job = [&](int i) { return P.jobs[blockIdx.x + (i >> 2) * gridDim.x]; };
         if (ntile > 0) {
             const int4 jb = job(0);
 #pragma unroll
