@@ -135,9 +135,19 @@ exotx_status radstep_columns(const exotx_rad_params *p, int prec, const exotx_ra
     warps = warps < 1 ? 1 : (warps > RAD_WARPS ? RAD_WARPS : warps);
     size_t smem = elems * esz * warps;
     int blocks = (maxcols + warps - 1) / warps;
-    // a column list is usually short (often empty): a few resident blocks per SM
-    // stride over it instead of one block per possible entry
-    if (cols) blocks = std::min(blocks, 148 * 8);
+    // a column list is usually short (often empty): one wave of resident blocks
+    // strides over it instead of one block per possible entry
+    if (cols) {
+        static int nsm = 0;
+        if (!nsm) {
+            int dev = 0;
+            if (cudaGetDevice(&dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1)
+                nsm = 148;
+        }
+        const int per_sm = std::max(1, (int)((227 * 1024) / std::max<size_t>(smem, 1)));
+        blocks = std::min(blocks, nsm * per_sm);
+    }
     if (prec == EXOTX_FP64) return launch_radstep_fp64(D, blocks, warps, smem, st);
     return launch_radstep_fp32(D, blocks, warps, smem, st);
 }

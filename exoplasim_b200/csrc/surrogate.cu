@@ -190,7 +190,17 @@ __device__ __forceinline__ float silu_grad(float z) {
 }
 
 // inference activation: fast exponential and division (the result is rounded to BF16)
-__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(-z)); }
+// silu(z) = z sigmoid(z) = h + h tanh(h) with h = z/2: one MUFU operation (tanh.approx, max relative
+// error about 2^-11), half the special-function work of the exp + reciprocal form
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float silu_fast(float z) {
+    const float h = 0.5f * z;
+    return fmaf(h, tanh_approx(h), h);
+}
 
 __global__ void k_silu(const float *Z, float *H, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -300,7 +310,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
     const int row = quarter * 32 + lane;  // TMEM lane = column of the tile
     const int nhor = A.in.nhor, nl = A.nl;
     const int ntiles = (nhor + SURR_TILE - 1) / SURR_TILE;
-    if (warp == 0) tc::tmem_alloc(slot, 256);
+    if (warp == 0) tc::tmem_alloc(slot, 2 * SURR_WIDTH);   // two layer accumulators
     auto issue_weights = [&](int l) {
         const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l);
         const uint32_t cbytes = (uint32_t)N * KC * 2;
@@ -321,31 +331,101 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
     const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
     const float *xm = A.norm, *xs = A.norm + A.nin, *xlo = A.norm + 2 * A.nin, *xhi = A.norm + 3 * A.nin;
     const float *ym = A.norm + 4 * A.nin, *ys = ym + A.nout;
-    uint32_t phase = 0;
+    // per input feature: source array (read at the column, or at its latitude
+    // row for kind 5), transform kind (0 none, 1-3 log with floors 1e-12, 1,
+    // 1e-6, -1 a constant), the constant, and 1 / the normalisation scale
+    struct __align__(16) Feat {
+        const T *src;
+        int kind;
+        float cst, xr, xm, lo, hi;
+    };
+    __shared__ Feat ftab[SURR_KIN];
+    if (tid < SURR_KIN) {
+        const int L = A.in.L, n = A.in.nhor;
+        int f = tid, kd = -1;
+        const T *src = nullptr;
+        float cv = 0.f;
+        if (f < A.nin) {
+            if (f < L + 1) { src = A.in.dt + (size_t)f * n; kd = 0; }
+            else if (f < 2 * L + 2) { src = A.in.dq + (size_t)(f - L - 1) * n; kd = 1; }
+            else if (f < 3 * L + 2) { src = A.in.dcc + (size_t)(f - 2 * L - 2) * n; kd = 0; }
+            else {
+                switch (f - 3 * L - 2) {
+                    case 0: src = A.in.dp; kd = 2; break;
+                    case 1: src = A.in.dalb; kd = 0; break;
+                    case 2: src = A.in.gmu0; kd = 0; break;
+                    case 3: src = A.in.dqco2; kd = 3; break;
+                    case 4: if (A.in.zsol) { src = A.in.zsol; kd = 0; } else cv = (float)A.in.zsolar1; break;
+                    case 5: if (A.in.zsol) { src = A.in.zsol + 2 * (size_t)n; kd = 0; } else cv = (float)A.in.rcoeff; break;
+                    default: src = A.in.sid; kd = 5; break;
+                }
+            }
+            ftab[f].xr = 1.f / xs[f];
+            ftab[f].xm = xm[f]; ftab[f].lo = xlo[f]; ftab[f].hi = xhi[f];
+        } else {
+            ftab[f].xr = 0.f;
+            ftab[f].xm = 0.f; ftab[f].lo = -INFINITY; ftab[f].hi = INFINITY;
+        }
+        ftab[f].src = src; ftab[f].kind = kd; ftab[f].cst = cv;
+    }
+    __syncthreads();
+    uint32_t pw = 0, pm = 0;   // completed phases of the weight and MMA barriers
     bool ok = true;  // cleared on every thread when a wait gives up
+    // thread 0: MMAs of layer l over the 16-wide K steps [k0, k1) into the layer's
+    // accumulator (layers alternate between two 256-column TMEM regions); the
+    // first step waits for the layer's weights; commit arrives on bar_mma
+    auto issue_mma = [&](int l, int k0, int k1, bool commit) -> bool {
+        const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l);
+        if (k0 == 0) {
+            if (!tc::mbar_wait(bar_w, pw & 1)) {
+                atomicExch(&g_surr_error, 1);
+                return false;
+            }
+            pw++;
+            tc::fence_after_sync();
+        }
+        const uint32_t idesc = tc::idesc_bf16(SURR_TILE, N);
+        const uint64_t da = tc::smem_desc(abuf, 128, (uint32_t)(K / 8) * 128);
+        const uint64_t db = tc::smem_desc(wbuf, 128, (uint32_t)(KC / 8) * 128);
+        const uint32_t d = tmem + (uint32_t)((l & 1) * SURR_WIDTH);
+        for (int kc = k0; kc < k1; kc++) {
+            const int c = (kc * 16) / KC, kin = (kc * 16) % KC;
+            tc::mma_bf16(d, tc::desc_add(da, kc * 256), tc::desc_add(db, c * 65536 + (kin / 8) * 128), idesc, kc > 0);
+        }
+        if (commit) tc::mma_commit(bar_mma);
+        return true;
+    };
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const int col = tile * SURR_TILE + row;
         const bool live = col < nhor;
         if (grp == 0) flags[row] = 0;
         __syncthreads();
         // features: warp group g builds the 8-input blocks g, g+4, ... of its row,
-        // normalised, as BF16
+        // normalised, as BF16; the block's eight raw loads are issued together
         {
             int bad = 0;
+            const int crow = col / A.in.nlon;   // latitude row, for the kind-5 feature
 #pragma unroll 1
             for (int g = grp; g < SURR_KIN / 8; g += 4) {
-                float v[8];
                 const int f0 = 8 * g;
+                float raw[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const Feat &F = ftab[f0 + e];
+                    raw[e] = F.cst;
+                    if (live && F.kind >= 0) raw[e] = (float)F.src[F.kind == 5 ? crow : col];
+                }
+                float v[8];
 #pragma unroll
                 for (int e = 0; e < 8; e++) {
                     const int f = f0 + e;
-                    float x = 0.f;
-                    if (live && f < A.nin) {
-                        const float raw = surr_feature<T, true>(A.in, col, f);
-                        bad |= (raw < xlo[f]) | (raw > xhi[f]) | (raw != raw);
-                        x = (raw - xm[f]) / xs[f];
-                    }
-                    v[e] = x;
+                    const Feat &F = ftab[f];
+                    float x = raw[e];
+                    if (F.kind == 1) x = __logf(fmaxf(x, 1e-12f));
+                    else if (F.kind == 2) x = __logf(fmaxf(x, 1.f));
+                    else if (F.kind == 3) x = __logf(fmaxf(x, 1e-6f));
+                    if (live && f < A.nin) bad |= (x < F.lo) | (x > F.hi) | (x != x);
+                    v[e] = (live && f < A.nin) ? (x - F.xm) * F.xr : 0.f;
                 }
                 uint32_t w[4];
 #pragma unroll
@@ -361,28 +441,14 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
         tc::fence_before_sync();
         __syncthreads();
         tc::fence_after_sync();
+        // layer 0 (the input features) in one go; each hidden epilogue below
+        // issues the next layer's MMAs in two K halves, the first while the
+        // second half of the activations is still being written
+        if (tid == 0 && ok) ok = issue_mma(0, 0, SURR_KIN / 16, true);
         for (int l = 0; l < nl; l++) {
-            const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l);
-            if (tid == 0) {
-                ok = tc::mbar_wait(bar_w, phase & 1);
-                if (ok) {
-                    tc::fence_after_sync();
-                    const uint32_t idesc = tc::idesc_bf16(SURR_TILE, N);
-                    const uint64_t da = tc::smem_desc(abuf, 128, (uint32_t)(K / 8) * 128);
-                    const uint64_t db = tc::smem_desc(wbuf, 128, (uint32_t)(KC / 8) * 128);
-                    for (int kc = 0; kc < K / 16; kc++) {
-                        const int c = (kc * 16) / KC, kin = (kc * 16) % KC;
-                        tc::mma_bf16(tmem, tc::desc_add(da, kc * 256),
-                                     tc::desc_add(db, c * 65536 + (kin / 8) * 128), idesc, kc > 0);
-                    }
-                    tc::mma_commit(bar_mma);
-                } else {
-                    atomicExch(&g_surr_error, 1);
-                }
-            }
-            __syncthreads();
-            const bool mok = __all_sync(0xffffffffu, tc::mbar_wait(bar_mma, phase & 1));
-            phase++;
+            const uint32_t acc = tmem + (uint32_t)((l & 1) * SURR_WIDTH);
+            const bool mok = __all_sync(0xffffffffu, tc::mbar_wait(bar_mma, pm & 1));
+            pm++;
             if (!mok) { if (lane == 0) atomicExch(&g_surr_error, 2); ok = false; }
             tc::fence_after_sync();
             // the weight buffer is free: fetch the next layer (or the next tile's first)
@@ -393,12 +459,13 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
             if (!mok) break;
             if (l + 1 < nl) {
                 // hidden epilogue: bias + SiLU, BF16, into the next layer's A operand;
-                // warp group g takes columns [64g, 64g + 64)
+                // in half h warp group g takes columns [128h + 32g, 128h + 32g + 32)
                 const float *b = A.bias[l];
 #pragma unroll 1
-                for (int c0 = grp * 64; c0 < grp * 64 + 64; c0 += 32) {
+                for (int h = 0; h < 2; h++) {
+                    const int c0 = 128 * h + 32 * grp;
                     uint32_t r[32];
-                    tc::tmem_ld32_nw(tmem + lane_addr + (uint32_t)c0, r);
+                    tc::tmem_ld32_nw(acc + lane_addr + (uint32_t)c0, r);
                     tc::tmem_wait_ld();
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
@@ -414,42 +481,62 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
                         *reinterpret_cast<uint4 *>(abuf + tc::kmajor_off(row, c0 + 8 * q, SURR_WIDTH)) =
                             make_uint4(w[0], w[1], w[2], w[3]);
                     }
+                    tc::fence_proxy_async();
+                    tc::fence_before_sync();
+                    __syncthreads();
+                    tc::fence_after_sync();
+                    // K half h of the next layer's A operand is complete
+                    constexpr int KH = SURR_WIDTH / 32;   // 16-wide K steps per half
+                    if (tid == 0 && ok) ok = issue_mma(l + 1, KH * h, KH * h + KH, h == 1);
                 }
-                tc::fence_proxy_async();
-                tc::fence_before_sync();
-                __syncthreads();
-                tc::fence_after_sync();
             } else {
                 // output epilogue: de-normalise and write the in-range columns; warp
                 // group g writes the levels k = g (mod 4), group 0 the surface fluxes
                 uint32_t r[32];
-                tc::tmem_ld32_nw(tmem + lane_addr, r);
+                tc::tmem_ld32_nw(acc + lane_addr, r);
                 tc::tmem_wait_ld();
                 if (live && !flags[row]) {
                     const float *b = A.bias[l];
                     const int L = A.in.L;
                     const size_t n = (size_t)nhor;
                     const float ps = (float)A.in.dp[col] * 1e-5f, adv = (float)A.in.adv;
+                    // this group's levels k = grp (mod 4): their humidities and heating
+                    // rates are read together before the updates
+                    constexpr int KMAX = SURR_NOUT / 4;
+                    T qk[KMAX], hk[KMAX];
 #pragma unroll
-                    for (int o = 0; o < SURR_NOUT; o++) {
-                        if (o >= A.nout || (o < L && (o & 3) != grp) || (o >= L && grp != 0)) continue;
-                        const float y = (__uint_as_float(r[o]) + __ldg(b + o)) * ys[o] + ym[o];
-                        if (o < L) {
-                            const float q = (float)A.in.dq[(size_t)o * n + col];
-                            A.dtdt[(size_t)o * n + col] += (T)__fdividef(y, 86400.f * ps * (1.f + adv * q));
-                        } else if (o == L) {
-                            A.dfd[(size_t)L * n + col] = (T)y;
-                        } else if (o == L + 1) {
-                            A.dfu[(size_t)L * n + col] = (T)y;
-                        } else if (o == L + 2) {
-                            A.dftd[(size_t)L * n + col] = (T)y;
-                        } else {
-                            A.dftu[(size_t)L * n + col] = (T)y;
+                    for (int j = 0; j < KMAX; j++) {
+                        const int o = grp + 4 * j;
+                        if (o < L && o < A.nout) {
+                            qk[j] = A.in.dq[(size_t)o * n + col];
+                            hk[j] = A.dtdt[(size_t)o * n + col];
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < KMAX; j++) {
+                        const int o = grp + 4 * j;
+                        if (o < L && o < A.nout) {
+                            // r[4j + grp] with constant register indices
+                            const uint32_t rv = grp == 0 ? r[4 * j] : grp == 1 ? r[4 * j + 1] : grp == 2 ? r[4 * j + 2] : r[4 * j + 3];
+                            const float y = (__uint_as_float(rv) + __ldg(b + o)) * ys[o] + ym[o];
+                            A.dtdt[(size_t)o * n + col] = hk[j] + (T)__fdividef(y, 86400.f * ps * (1.f + adv * (float)qk[j]));
                         }
                     }
                     if (grp == 0) {
-                        A.dswfl[(size_t)L * n + col] = A.dfd[(size_t)L * n + col] + A.dfu[(size_t)L * n + col];
-                        A.dlwfl[(size_t)L * n + col] = A.dftd[(size_t)L * n + col] + A.dftu[(size_t)L * n + col];
+                        float f4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                        for (int o = 0; o < SURR_NOUT; o++) {
+                            const int i = o - L;
+                            if (i < 0 || i > 3 || o >= A.nout) continue;
+                            const float y = (__uint_as_float(r[o]) + __ldg(b + o)) * ys[o] + ym[o];
+                            if (i == 0) f4[0] = y; else if (i == 1) f4[1] = y; else if (i == 2) f4[2] = y; else f4[3] = y;
+                        }
+                        A.dfd[(size_t)L * n + col] = (T)f4[0];
+                        A.dfu[(size_t)L * n + col] = (T)f4[1];
+                        A.dftd[(size_t)L * n + col] = (T)f4[2];
+                        A.dftu[(size_t)L * n + col] = (T)f4[3];
+                        A.dswfl[(size_t)L * n + col] = (T)f4[0] + (T)f4[1];
+                        A.dlwfl[(size_t)L * n + col] = (T)f4[2] + (T)f4[3];
                     }
                 }
                 if (live && flags[row] && grp == 0) {
@@ -466,7 +553,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 256);
+    if (warp == 0) tc::tmem_dealloc(tmem, 2 * SURR_WIDTH);
 }
 
 }  // namespace exotx
