@@ -340,6 +340,12 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
         float cst, xr, xm, lo, hi;
     };
     __shared__ Feat ftab[SURR_KIN];
+    // every layer's biases (hidden layers: SURR_WIDTH each; output: SURR_NOUT)
+    __shared__ __align__(16) float bias_s[MLP_MAX_LAYERS][SURR_WIDTH];
+    for (int i = tid; i < MLP_MAX_LAYERS * SURR_WIDTH; i += SURR_THREADS) {
+        const int l = i / SURR_WIDTH, c = i - l * SURR_WIDTH;
+        bias_s[l][c] = (l < nl && c < surr_layer_N(l, nl) && c < (l == nl - 1 ? A.nout : SURR_WIDTH)) ? A.bias[l][c] : 0.f;
+    }
     if (tid < SURR_KIN) {
         const int L = A.in.L, n = A.in.nhor;
         int f = tid, kd = -1;
@@ -460,7 +466,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
             if (l + 1 < nl) {
                 // hidden epilogue: bias + SiLU, BF16, into the next layer's A operand;
                 // in half h warp group g takes columns [128h + 32g, 128h + 32g + 32)
-                const float *b = A.bias[l];
+                const float *b = bias_s[l];
 #pragma unroll 1
                 for (int h = 0; h < 2; h++) {
                     const int c0 = 128 * h + 32 * grp;
@@ -473,8 +479,9 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
 #pragma unroll
                         for (int i = 0; i < 4; i++) {
                             const int c = 8 * q + 2 * i;
-                            const float h0 = silu_fast(__uint_as_float(r[c]) + __ldg(b + c0 + c));
-                            const float h1 = silu_fast(__uint_as_float(r[c + 1]) + __ldg(b + c0 + c + 1));
+                            const float2 bb = *reinterpret_cast<const float2 *>(b + c0 + c);
+                            const float h0 = silu_fast(__uint_as_float(r[c]) + bb.x);
+                            const float h1 = silu_fast(__uint_as_float(r[c + 1]) + bb.y);
                             const __nv_bfloat162 b2 = __floats2bfloat162_rn(h0, h1);
                             w[i] = *reinterpret_cast<const uint32_t *>(&b2);
                         }
@@ -496,7 +503,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
                 tc::tmem_ld32_nw(acc + lane_addr, r);
                 tc::tmem_wait_ld();
                 if (live && !flags[row]) {
-                    const float *b = A.bias[l];
+                    const float *b = bias_s[l];
                     const int L = A.in.L;
                     const size_t n = (size_t)nhor;
                     const float ps = (float)A.in.dp[col] * 1e-5f, adv = (float)A.in.adv;
@@ -518,7 +525,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
                         if (o < L && o < A.nout) {
                             // r[4j + grp] with constant register indices
                             const uint32_t rv = grp == 0 ? r[4 * j] : grp == 1 ? r[4 * j + 1] : grp == 2 ? r[4 * j + 2] : r[4 * j + 3];
-                            const float y = (__uint_as_float(rv) + __ldg(b + o)) * ys[o] + ym[o];
+                            const float y = (__uint_as_float(rv) + b[o]) * ys[o] + ym[o];
                             A.dtdt[(size_t)o * n + col] = hk[j] + (T)__fdividef(y, 86400.f * ps * (1.f + adv * (float)qk[j]));
                         }
                     }
@@ -528,7 +535,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
                         for (int o = 0; o < SURR_NOUT; o++) {
                             const int i = o - L;
                             if (i < 0 || i > 3 || o >= A.nout) continue;
-                            const float y = (__uint_as_float(r[o]) + __ldg(b + o)) * ys[o] + ym[o];
+                            const float y = (__uint_as_float(r[o]) + b[o]) * ys[o] + ym[o];
                             if (i == 0) f4[0] = y; else if (i == 1) f4[1] = y; else if (i == 2) f4[2] = y; else f4[3] = y;
                         }
                         A.dfd[(size_t)L * n + col] = (T)f4[0];
