@@ -63,8 +63,9 @@ def fft_bytes(nlat, nlev, half, esz):
 # DRAM bytes per launch of the dominant kernel from one ncu capture (dram__bytes_read.sum
 # + dram__bytes_write.sum), keyed by (kernel, workload); the summary with its command is
 # in profiles/.
-# k_tc_forward_pipe on one T127 L20 instance, one cold-cache ncu capture: 63.8 MB read + 0.86 MB written
-NCU_TRAFFIC = {("tc_forward", WORKLOAD): 63.786752e6 + 0.864256e6}
+# k_tc_forward_pipe on two T127 L20 instances (one launch of the default step), one
+# cold-cache ncu capture: 99.2 MB read + 5.8 MB written
+NCU_TRAFFIC = {("tc_forward", WORKLOAD): 99.17056e6 + 5.818368e6}
 
 
 def args_():
