@@ -111,3 +111,26 @@ def test_autotuner_keeps_the_three_term_split(ens):
     torch.cuda.synchronize()
     assert torch.equal(gout, gout_ref) and torch.equal(spout, spout_ref)
     E.configure()
+
+
+def test_ensemble_with_a_t127_segment():
+    # a T127 segment runs the register-resident FFT bodies in a launch of their
+    # own (six launches per round trip); its instances still equal the
+    # single-resolution batched path bit for bit
+    E = Ensemble([192, 32, 64], [20, 10, 15])
+    spins, gins = _inputs(E, 40)
+    spin, gin = E.pack("spec", spins), E.pack("gin", gins)
+    _, gout, _, spout = E.buffers()
+    n0 = launch_count()
+    E.inverse(spin, gout)
+    E.forward(gin, spout)
+    torch.cuda.synchronize()
+    assert launch_count() - n0 == 6
+    gouts, spouts = E.unpack("gout", gout), E.unpack("spec", spout)
+    for i, (nlat, L) in enumerate(zip(E.nlat, E.nlev)):
+        P = Plan(nlat)
+        g = P.inverse_set_batch(spins[i].unsqueeze(0).contiguous(), L, precision="mixed")[0]
+        s = P.forward_set_batch(gins[i].unsqueeze(0).contiguous(), L, precision="mixed")[0]
+        torch.cuda.synchronize()
+        assert torch.equal(gouts[i], g), i
+        assert torch.equal(spouts[i], s), i

@@ -191,6 +191,23 @@ def test_fft_fp32(oracle, n):
     assert relerr(a.cpu().numpy(), ref) < 2e-6
 
 
+@pytest.mark.parametrize("rows", [1, 9, 32, 70])
+def test_fft_fp32_384_rows(oracle, rows):
+    # n = 384 runs the register-resident kernels: 32 rows per block, bulk copies
+    # of even row runs and a plain-load path otherwise; partial blocks, odd
+    # counts and the row-major Fourier side (k fastest across threads)
+    rng = np.random.default_rng(rows + 384)
+    x = rng.standard_normal((rows, 384))
+    a = _cuda(x, torch.float32)
+    gp2fc(a)
+    ref = oracle.gp2fc(x)
+    assert relerr(a.cpu().numpy(), ref) < 2e-6
+    f = rng.standard_normal((rows, 384))
+    b = _cuda(f, torch.float32)
+    fc2gp(b)
+    assert relerr(b.cpu().numpy(), oracle.fc2gp(f)) < 2e-6
+
+
 def test_fft_bad_lengths():
     for n in (14, 7, 5000, 2):
         a = torch.zeros((2, n), dtype=torch.float64, device="cuda")
