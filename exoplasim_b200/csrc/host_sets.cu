@@ -5,8 +5,11 @@
 // the instances stream through three device slots on three streams: while the
 // transforms of group k run, the inputs of group k+1 are copied in and the
 // outputs of group k-1 are copied out, so the PCIe link carries data in both
-// directions while the GPU computes.  Every slot is reused only after the
-// copy-out of its previous group has finished (events order the streams).
+// directions while the GPU computes.  Within a group the inverse half goes
+// first: its spectral input is small and its grid output large, so the grid
+// output of the inverse set leaves while the forward set's grid input is still
+// arriving.  Every slot is reused only after the copy-out of its previous group
+// has finished (events order the streams).
 #include <algorithm>
 #include "exotx_internal.cuh"
 
@@ -17,7 +20,9 @@ struct HostPipe {
     int prec = -1, nlev = 0, group = 0;
     void *d_spin[NSLOT] = {}, *d_gout[NSLOT] = {}, *d_gin[NSLOT] = {}, *d_sout[NSLOT] = {};
     cudaStream_t s_in = nullptr, s_run = nullptr, s_out = nullptr;
-    cudaEvent_t ev_in[NSLOT] = {}, ev_run[NSLOT] = {}, ev_out[NSLOT] = {}, ev_edge = nullptr;
+    // per slot: inverse inputs in, forward inputs in, inverse done, forward done, outputs out
+    cudaEvent_t ev_in[NSLOT] = {}, ev_in2[NSLOT] = {}, ev_run[NSLOT] = {}, ev_run2[NSLOT] = {}, ev_out[NSLOT] = {};
+    cudaEvent_t ev_edge = nullptr;
 
     void free_buffers() {
         for (int i = 0; i < NSLOT; i++) {
@@ -33,7 +38,9 @@ struct HostPipe {
         free_buffers();
         for (int i = 0; i < NSLOT; i++) {
             if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+            if (ev_in2[i]) cudaEventDestroy(ev_in2[i]);
             if (ev_run[i]) cudaEventDestroy(ev_run[i]);
+            if (ev_run2[i]) cudaEventDestroy(ev_run2[i]);
             if (ev_out[i]) cudaEventDestroy(ev_out[i]);
         }
         if (ev_edge) cudaEventDestroy(ev_edge);
@@ -66,18 +73,20 @@ static exotx_status pipe_setup(exotx_plan p, int prec, int L, int ninst, HostPip
         EXOTX_CUDA(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
         for (int i = 0; i < HostPipe::NSLOT; i++) {
             EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_in[i], cudaEventDisableTiming));
+            EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_in2[i], cudaEventDisableTiming));
             EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_run[i], cudaEventDisableTiming));
+            EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_run2[i], cudaEventDisableTiming));
             EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_out[i], cudaEventDisableTiming));
         }
         EXOTX_CUDA(cudaEventCreateWithFlags(&h->ev_edge, cudaEventDisableTiming));
     }
     size_t sp, go, gi;
     inst_bytes(p, prec, L, &sp, &go, &gi);
-    // instances per slot: about 256 MB of arrays, so the transform launches
+    // instances per slot: about 128 MB of arrays, so the transform launches
     // still cover several instances at small resolutions while the first
     // copy in and the last copy out (which nothing overlaps) stay short
     const size_t per = 2 * sp + go + gi;
-    int g = (int)std::max<size_t>(1, (256u << 20) / per);
+    int g = (int)std::max<size_t>(1, (128u << 20) / per);
     g = std::min(g, std::max(ninst, 1));
     if (h->prec != prec || h->nlev != L || h->group < g) {
         EXOTX_CUDA(cudaStreamSynchronize(h->s_in));
@@ -124,20 +133,24 @@ EXOTX_API exotx_status exotx_sets_host(exotx_plan p, int prec, const void *h_spi
         if (inv)
             EXOTX_CUDA(cudaMemcpyAsync(h->d_spin[b], (const char *)h_spin + sp * i0, sp * ni,
                                        cudaMemcpyHostToDevice, h->s_in));
+        EXOTX_CUDA(cudaEventRecord(h->ev_in[b], h->s_in));
         if (fwd)
             EXOTX_CUDA(cudaMemcpyAsync(h->d_gin[b], (const char *)h_gpin + gi * i0, gi * ni, cudaMemcpyHostToDevice,
                                        h->s_in));
-        EXOTX_CUDA(cudaEventRecord(h->ev_in[b], h->s_in));
-        // transforms
+        EXOTX_CUDA(cudaEventRecord(h->ev_in2[b], h->s_in));
+        // transforms: the inverse set as soon as its spectral input is in
         EXOTX_CUDA(cudaStreamWaitEvent(h->s_run, h->ev_in[b], 0));
         if (inv) EXOTX_TRY(exotx_inverse_set_batch(p, prec, h->d_spin[b], h->d_gout[b], nlev, ni, h->s_run));
-        if (fwd) EXOTX_TRY(exotx_forward_set_batch(p, prec, h->d_gin[b], h->d_sout[b], nlev, ni, h->s_run));
         EXOTX_CUDA(cudaEventRecord(h->ev_run[b], h->s_run));
-        // copy out
+        EXOTX_CUDA(cudaStreamWaitEvent(h->s_run, h->ev_in2[b], 0));
+        if (fwd) EXOTX_TRY(exotx_forward_set_batch(p, prec, h->d_gin[b], h->d_sout[b], nlev, ni, h->s_run));
+        EXOTX_CUDA(cudaEventRecord(h->ev_run2[b], h->s_run));
+        // copy out: the inverse set's grid rows while the forward input may still be arriving
         EXOTX_CUDA(cudaStreamWaitEvent(h->s_out, h->ev_run[b], 0));
         if (inv)
             EXOTX_CUDA(cudaMemcpyAsync((char *)h_gpout + go * i0, h->d_gout[b], go * ni, cudaMemcpyDeviceToHost,
                                        h->s_out));
+        EXOTX_CUDA(cudaStreamWaitEvent(h->s_out, h->ev_run2[b], 0));
         if (fwd)
             EXOTX_CUDA(cudaMemcpyAsync((char *)h_spout + sp * i0, h->d_sout[b], sp * ni, cudaMemcpyDeviceToHost,
                                        h->s_out));
