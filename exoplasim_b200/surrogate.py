@@ -9,7 +9,10 @@ inference (exotx_rad_surrogate) runs the network in BF16 on the tensor cores
 and computes every column whose inputs leave the training ranges with the
 plain radstep kernel.
 
-    python -m exoplasim_b200.surrogate --train OUT.npz [--columns 2000000] [--epochs 16]
+    python -m exoplasim_b200.surrogate --train OUT.npz [--columns 2000000] [--epochs 400]
+
+The packaged network (data/rad_surrogate_L20.npz) was trained this way with
+the defaults: 2M columns, 400 epochs of Adam with cosine decay from 1e-3.
 """
 import argparse
 import ctypes as C
@@ -298,7 +301,7 @@ def main():
     a = argparse.ArgumentParser()
     a.add_argument("--train", required=True, help="output .npz")
     a.add_argument("--columns", type=int, default=2_000_000)
-    a.add_argument("--epochs", type=int, default=16)
+    a.add_argument("--epochs", type=int, default=400)
     a.add_argument("--batch", type=int, default=4096)
     a.add_argument("--lr", type=float, default=1e-3)
     a.add_argument("--nlev", type=int, default=20)
