@@ -570,15 +570,15 @@ __global__ void __launch_bounds__(256) k_rfft_fwd_fold(const T *gp, T *fc, int n
 // Thread t takes the Q-point DFT of its column z[t + P j] in registers and
 // applies W_h^{t q}; one transposition through shared memory then hands it the
 // Q/P whole P-point DFTs q = (Q/P) t + i.  The inverse runs the same steps in
-// the other order.  A block of 256 threads works RB = 256/P rows.  The grid
+// the other order.  A block of NT threads works RB = NT/P rows.  The grid
 // rows and the block's Fourier coefficients move between global and shared
 // memory as bulk (TMA) copies, so the load/store unit only serves
 // bank-conflict-free shared-memory accesses; the twiddles W_h^{t q} sit in a
 // per-block table, Q contiguous values per t.
 __device__ int g_fft_error;   // nonzero: a bounded wait in an FFT kernel gave up
 
-template <int N> struct RfShape { static constexpr int P = 0, Q = 0; };
-template <> struct RfShape<384> { static constexpr int P = 8, Q = 24; };
+template <int N> struct RfShape { static constexpr int P = 0, Q = 0, NT = 256; };
+template <> struct RfShape<384> { static constexpr int P = 8, Q = 24, NT = 128; };
 template <int N> constexpr bool rf_len() { return RfShape<N>::P > 0; }
 // Shared memory (complex units unless noted), P = 8:
 //   region R, reused in turn for the staged grid rows (row stride RG = 8 mod 16:
@@ -590,7 +590,7 @@ template <int N> constexpr bool rf_len() { return RfShape<N>::P > 0; }
 //   then the twiddle table tq[t * RT + q] = W_h^{t q}, the split twiddles
 //   rt[k] = e^{-2 pi i k/n} (k < h), and the copy barrier.
 template <int N> struct RfLayout {
-    static constexpr int P = RfShape<N>::P, Q = RfShape<N>::Q, H = N / 2, RB = 256 / P;
+    static constexpr int P = RfShape<N>::P, Q = RfShape<N>::Q, H = N / 2, NT = RfShape<N>::NT, RB = NT / P;
     static constexpr int RT = Q + 2;
     static constexpr int RS = P * RT + ((8 - (P * RT) % 16) + 16) % 16;
     static constexpr int RZ = H + 1;
@@ -601,7 +601,7 @@ template <int N> struct RfLayout {
                             OFF_BAR = OFF_RT + (size_t)H * 8, SMEM = OFF_BAR + 16;
     static_assert(P == 8 && Q % P == 0 && Q % 4 == 0 && (RT / 2) % 2 == 1 && RS % 16 == 8 && RG % 16 == 8, "layout");
     static_assert(H * RC <= R, "the staged coefficients fit region R");
-    static_assert(RB == 32, "warp 0 issues one row copy per lane");
+    static_assert(RB <= 32 && RB % 4 == 0, "warp 0 issues one row copy per lane");
 };
 
 // cos(2 pi a / 24) for an integer a (multiples of 15 degrees)
@@ -717,10 +717,10 @@ __device__ __forceinline__ bool rf_wait_loads(uint64_t *bar) {
 template <int N, typename RowOf>
 __device__ __forceinline__ bool rf_forward_rows(const float *__restrict__ g, RowOf grow, const RfSmem<N> &S) {
     using Lay = RfLayout<N>;
-    constexpr int P = Lay::P, Q = Lay::Q, H = Lay::H, QP = Q / P;
+    constexpr int P = Lay::P, Q = Lay::Q, H = Lay::H, QP = Q / P, RB = Lay::RB;
     const int t = threadIdx.x % P, r = threadIdx.x / P;
     if (threadIdx.x < 32) {   // warp 0: one bulk copy per row
-        const long long gr = grow(threadIdx.x);
+        const long long gr = threadIdx.x < RB ? grow(threadIdx.x) : -1ll;
         const unsigned valid = __ballot_sync(0xffffffffu, gr >= 0);
         if (threadIdx.x == 0) tc::mbar_arrive_expect_tx(S.bar, (uint32_t)__popc(valid) * (uint32_t)(N * 4));
         __syncwarp();
@@ -1061,7 +1061,7 @@ static exotx_status fft_ens_group(bool fwd, bool rf, const FftEnsSeg *segs, int 
                                  : (fwd ? k_rfft_ens<true> : k_rfft_ens<false>);
     if (smem > 48 * 1024) EXOTX_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cudaEvent_t ev = ktimer_start(kid, s);
-    k<<<blocks, 256, smem, s>>>(P);
+    k<<<blocks, rf ? RfLayout<384>::NT : 256, smem, s>>>(P);
     EXOTX_CHECK_LAUNCH();
     ktimer_stop(kid, s, ev);
     return EXOTX_OK;
@@ -1121,10 +1121,10 @@ static exotx_status launch_rf(bool fwd, const float *in, float *out, long long l
         EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_inv_rf<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM));
     cudaEvent_t ev = ktimer_start(kid, s);
     if (fwd)
-        EXOTX_CUDA(launch_pdl(k_rfft_fwd_rf<N>, dim3((unsigned)nb), dim3(256), Lay::SMEM, s, in, out, lot, kf, f_rs,
+        EXOTX_CUDA(launch_pdl(k_rfft_fwd_rf<N>, dim3((unsigned)nb), dim3(Lay::NT), Lay::SMEM, s, in, out, lot, kf, f_rs,
                               f_ms, w, r));
     else
-        EXOTX_CUDA(launch_pdl(k_rfft_inv_rf<N>, dim3((unsigned)nb), dim3(256), Lay::SMEM, s, in, out, lot, kf, f_rs,
+        EXOTX_CUDA(launch_pdl(k_rfft_inv_rf<N>, dim3((unsigned)nb), dim3(Lay::NT), Lay::SMEM, s, in, out, lot, kf, f_rs,
                               f_ms, w, r));
     EXOTX_CHECK_LAUNCH();
     ktimer_stop(kid, s, ev);
@@ -1303,7 +1303,7 @@ static exotx_status launch_fold(const float *in, float *out, int nlat, long long
         EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_fold_rf<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)Lay::SMEM));
         cudaEvent_t ev = ktimer_start(EXOTX_K_FFT_FORWARD, s);
-        EXOTX_CUDA(launch_pdl(k_rfft_fwd_fold_rf<N>, dim3((unsigned)nb), dim3(256), Lay::SMEM, s, in, out, nlat, lot,
+        EXOTX_CUDA(launch_pdl(k_rfft_fwd_fold_rf<N>, dim3((unsigned)nb), dim3(Lay::NT), Lay::SMEM, s, in, out, nlat, lot,
                               kf, f_ms, w, r));
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_FFT_FORWARD, s, ev);
