@@ -571,10 +571,10 @@ __global__ void __launch_bounds__(256) k_rfft_fwd_fold(const T *gp, T *fc, int n
 // applies W_h^{t q}; one transposition through shared memory then hands it the
 // Q/P whole P-point DFTs q = (Q/P) t + i.  The inverse runs the same steps in
 // the other order.  A block of NT threads works RB = NT/P rows.  The grid
-// rows and the block's Fourier coefficients move between global and shared
-// memory as bulk (TMA) copies, so the load/store unit only serves
-// bank-conflict-free shared-memory accesses; the twiddles W_h^{t q} sit in a
-// per-block table, Q contiguous values per t.
+// rows (contiguous 4n-byte runs) move between global and shared memory as bulk
+// (TMA) copies, one per row; the inverse's Fourier coefficients, runs of only
+// RB complex values per wavenumber, arrive by plain coalesced loads.  The
+// twiddles W_h^{t q} sit in a per-block table, Q contiguous values per t.
 __device__ int g_fft_error;   // nonzero: a bounded wait in an FFT kernel gave up
 
 template <int N> struct RfShape { static constexpr int P = 0, Q = 0, NT = 256; };
@@ -859,7 +859,8 @@ __device__ __forceinline__ void rfft_fwd_fold_rf_body(const float *gp, float *fc
 }
 
 // rfft_inv_ct_body for the register-resident lengths: the block's
-// coefficients c_k (k < kf) are staged k-major in shared memory; each thread
+// coefficients c_k (k < kf) are staged k-major in shared memory by plain
+// coalesced loads (a k's RB rows are one run of the m-major side); each thread
 // forms the Z_k of its own q from c_k and c_{h-k}, takes their P-point DFTs,
 // and after the transposition the Q-point DFT of its column; the grid rows
 // leave through shared memory as one bulk store each
@@ -879,20 +880,22 @@ __device__ __forceinline__ void rfft_inv_rf_body(const float *fc, float *gp, lon
     pdl_wait();   // the coefficients come from the previous kernel
     const cpx<float> *fcc = reinterpret_cast<const cpx<float> *>(fc);
     cpx<float> *cs = S.r;   // c_k of row r at cs[k * RC + r]
-    // bulk copies when each k's rows are one 16-byte-aligned run of the m-major side
-    const bool bulk = f_rs == 1 && !(f_ms & 1) && !(rows & 1) && !(reinterpret_cast<uintptr_t>(fc) & 15);
-    if (bulk) {
-        if (threadIdx.x < 32) {
-            if (threadIdx.x == 0) tc::mbar_arrive_expect_tx(S.bar, (uint32_t)kf * (uint32_t)rows * 8u);
-            __syncwarp();
-            for (int k = threadIdx.x; k < kf; k += 32)
-                tc::bulk_g2s(cs + k * Lay::RC, fcc + row0 + (long long)k * f_ms, (uint32_t)rows * 8u, S.bar);
-        }
-        if (!rf_wait_loads(S.bar)) return;
-    } else {
-        for (int i = threadIdx.x; i < kf * RB; i += blockDim.x) {
-            const int k = i / RB, rr = i - k * RB;
-            if (rr < rows) cs[k * Lay::RC + rr] = fcc[(row0 + rr) * f_rs + (long long)k * f_ms];
+    // the block's coefficients, k-major: plain loads, eight per thread in flight
+    // (one k's rows are only RB x 8 bytes: bulk copies of that size were slower)
+    {
+        constexpr int U = 8;
+        for (int i0 = threadIdx.x; i0 < kf * RB; i0 += U * (int)blockDim.x) {
+            cpx<float> v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int i = i0 + u * (int)blockDim.x, k = i / RB, rr = i - k * RB;
+                v[u] = (i < kf * RB && rr < rows) ? fcc[(row0 + rr) * f_rs + (long long)k * f_ms] : cpx<float>{0.f, 0.f};
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int i = i0 + u * (int)blockDim.x, k = i / RB, rr = i - k * RB;
+                if (i < kf * RB) cs[k * Lay::RC + rr] = v[u];
+            }
         }
         __syncthreads();
     }
