@@ -705,9 +705,16 @@ __device__ __forceinline__ void rf_setup(const RfSmem<N> &S, const cpx<float> *_
 }
 
 // Waits for the block's bulk loads; false (block-uniform, error word set) if the bounded wait gave up.
+// After a timeout every thread waits once more (bounded) for copies still in
+// flight, so none lands in shared memory after the block has left (out of
+// line: the error path takes no registers from the transform).
+__device__ __noinline__ void rf_loads_timed_out(uint64_t *bar) {
+    if (threadIdx.x == 0) atomicExch(&g_fft_error, 1);
+    tc::mbar_wait(bar, 0);
+}
 __device__ __forceinline__ bool rf_wait_loads(uint64_t *bar) {
     const bool ok = __syncthreads_and(tc::mbar_wait(bar, 0)) != 0;
-    if (!ok && threadIdx.x == 0) atomicExch(&g_fft_error, 1);
+    if (!ok) rf_loads_timed_out(bar);
     return ok;
 }
 

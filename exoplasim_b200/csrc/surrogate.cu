@@ -311,9 +311,11 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
     const int nhor = A.in.nhor, nl = A.nl;
     const int ntiles = (nhor + SURR_TILE - 1) / SURR_TILE;
     if (warp == 0) tc::tmem_alloc(slot, 2 * SURR_WIDTH);   // two layer accumulators
+    uint32_t wissued = 0;   // weight loads issued (thread 0)
     auto issue_weights = [&](int l) {
         const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l);
         const uint32_t cbytes = (uint32_t)N * KC * 2;
+        wissued++;
         tc::mbar_arrive_expect_tx(bar_w, cbytes * (K / KC));
         for (int c = 0; c < K / KC; c++)
             tc::bulk_g2s(wbuf + c * 65536, A.tw + A.twoff[l] + (size_t)c * cbytes, cbytes, bar_w);
@@ -558,6 +560,8 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
             }
         }
     }
+    // after a timeout, a weight load still in flight lands before the block leaves
+    if (tid == 0 && !ok && wissued > pw) tc::mbar_wait(bar_w, pw & 1);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, 2 * SURR_WIDTH);
