@@ -7,14 +7,18 @@
 // synchronise the device), cannot let exotx_forward_set grow the plan's
 // Fourier work buffer or build its FFT twiddle tables on first use.  This
 // variant keeps both in one fixed array of device memory that is part of the
-// library: EXOTX_STATIC_WORK_BYTES bytes, held by every GPU that loads the
-// library until the process exits.
+// library: EXOTX_STATIC_WORK_BYTES bytes on each GPU, held from the library's
+// first use on that GPU (module loading is lazy) until the process exits.
 //
 // The array is shared by every call on a device and keeps the last call's
-// contents.  Each call writes every byte it later reads (twiddles by a
-// stream-ordered copy, the Fourier intermediate by the FFT kernel), so nothing
-// has to start at zero.  Calls whose work overlaps on the GPU (other streams,
-// other host threads, without synchronisation between them) race on the array.
+// contents.  Each call reads only bytes that it, or an earlier call with the
+// same grid length and precision, wrote: the twiddles are copied in by the
+// first call on a device and again only when the grid length or precision
+// changes (a per-device record says which twiddles the array holds), and the
+// Fourier intermediate is written by the FFT kernel before the Legendre
+// kernels read it, so nothing has to start at zero.  Calls whose work overlaps
+// on the GPU (other streams, other host threads, without synchronisation
+// between them) race on the array.
 #include <cstring>
 #include <mutex>
 #include "exotx_internal.cuh"
@@ -28,6 +32,10 @@ static __device__ __align__(256) unsigned char g_static_work[EXOTX_STATIC_WORK_B
 constexpr int kMaxDevices = 64;
 static std::mutex g_static_mu;
 static void *g_static_addr[kMaxDevices];  // device address of the array, per device ordinal
+// which twiddles the array of each device holds: grid length and element size
+// (0 = none yet)
+static int g_tw_nlon[kMaxDevices];
+static int g_tw_esz[kMaxDevices];
 
 // Set-up, once per device, with that device current.
 static exotx_status static_work_addr(unsigned char **out) {
@@ -80,13 +88,21 @@ static exotx_status forward_set_static(exotx_plan p, const T *gpin, T *spout, in
     T *W = reinterpret_cast<T *>(base + W_off);
     const int h = p->nlon / 2;
     {
-        // the pageable source is staged before cudaMemcpyAsync returns, so the
-        // host buffer may be refilled by the next call
+        // rewrite the twiddles only when the array holds another length's or
+        // precision's; the pageable source is staged before cudaMemcpyAsync
+        // returns, so the host buffer may be refilled by the next call
+        int dev = -1;
+        EXOTX_CUDA(cudaGetDevice(&dev));
         std::lock_guard<std::mutex> lk(g_static_mu);
-        T *hw = tw_host<T>(), *hr = hw + 2 * h;
-        fft_twiddles_host<T>(p->nlon, hw, hr);
-        EXOTX_CUDA(cudaMemcpyAsync(dw, hw, sizeof(T) * 2 * (size_t)h, cudaMemcpyHostToDevice, s));
-        EXOTX_CUDA(cudaMemcpyAsync(dr, hr, sizeof(T) * 2 * (size_t)(h + 1), cudaMemcpyHostToDevice, s));
+        if (g_tw_nlon[dev] != p->nlon || g_tw_esz[dev] != (int)sizeof(T)) {
+            T *hw = tw_host<T>(), *hr = hw + 2 * h;
+            fft_twiddles_host<T>(p->nlon, hw, hr);
+            g_tw_nlon[dev] = 0;  // unknown contents if a copy fails
+            EXOTX_CUDA(cudaMemcpyAsync(dw, hw, sizeof(T) * 2 * (size_t)h, cudaMemcpyHostToDevice, s));
+            EXOTX_CUDA(cudaMemcpyAsync(dr, hr, sizeof(T) * 2 * (size_t)(h + 1), cudaMemcpyHostToDevice, s));
+            g_tw_nlon[dev] = p->nlon;
+            g_tw_esz[dev] = (int)sizeof(T);
+        }
     }
     const long long nrsp = 2LL * p->ncsp;
     const long long nrows = (9LL * L + 1) * p->nlat;

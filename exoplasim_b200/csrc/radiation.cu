@@ -107,14 +107,14 @@ exotx_status radstep_columns(const exotx_rad_params *p, int prec, const exotx_ra
     if (!p || !io) return EXOTX_BAD_ARG;
     if (p->nlev < 2 || p->nlev > RAD_MAXLEV || p->nhor < 1 || p->nlon < 1) return EXOTX_BAD_DIM;
     if (prec != EXOTX_FP64 && prec != EXOTX_FP32) return EXOTX_BAD_ARG;
-    if (p->ndcycle == 0) return EXOTX_NOT_BUILT;  // zonal-mean insolation: not in this build
     const void *req[] = {io->dt, io->dq, io->dcc, io->dql, io->dqco2, io->dp, io->dls, io->dicec, io->dqo3,
                          io->gmu0, io->dalb, io->dsalb, io->dfu, io->dfd, io->dftu, io->dftd, io->dswfl,
                          io->dlwfl, io->dflux, io->dtdt, io->dtdtswr, io->dtdtlwr, io->dconv};
     for (const void *q : req) if (!q) return EXOTX_BAD_ARG;
     if ((p->nsol == 1 || p->no3 == 1) && (!io->sid || !io->cola)) return EXOTX_BAD_ARG;
-    // sid/cola are indexed by latitude row col/nlon: columns must fill whole rows
-    if ((p->nsol == 1 || p->no3 == 1) && (p->nhor % p->nlon) != 0) return EXOTX_BAD_DIM;
+    // sid/cola are indexed by latitude row col/nlon, and ndcycle = 0 averages
+    // over rows: columns must fill whole rows
+    if ((p->nsol == 1 || p->no3 == 1 || p->ndcycle == 0) && (p->nhor % p->nlon) != 0) return EXOTX_BAD_DIM;
     if ((cols == nullptr) != (ncols == nullptr)) return EXOTX_BAD_ARG;
     if (maxcols <= 0) return EXOTX_OK;
     RadDev D;

@@ -426,6 +426,30 @@ __device__ void lwr_warp(const exotx_rad_params &P, ColScratch<T> &s, int L, T d
     __syncwarp();
 }
 
+// cos zenith of column (jlat, jlon) clipped at dawn (solang, radmod.f90:1380-1436)
+template <typename T>
+__device__ __forceinline__ T solang_mu(const exotx_rad_params &P, const T *sid, const T *cola, int jlat, int jlon,
+                                       int nlon) {
+    const T PI = (T)3.14159265359, TWOPI = PI + PI;
+    T zdawn = sin((T)P.dawn * PI / (T)180.0), zmuz;
+    if (P.ncstsol == 0) {
+        T zrlon = TWOPI / nlon;
+        T zhangle = (T)P.zmins * (T)P.zrtim + jlon * zrlon - PI;
+        if (P.ngenkeplerian == 1) zhangle = zhangle - (T)P.rasc;
+        if (zhangle < -PI) zhangle = zhangle + TWOPI;
+        if (zhangle > PI) zhangle = zhangle - TWOPI;
+        if (P.nfixed == 1) zhangle = zhangle + PI;
+        zmuz = sin((T)P.zdecl) * sid[jlat] + cola[jlat] * cos((T)P.zdecl) * cos(zhangle);
+    } else {
+        T solclatcdec = (T)P.solclat * (T)P.solcdec;
+        T solslat = sqrt((T)1 - (T)P.solclat * (T)P.solclat);
+        T solsdec = sqrt((T)1 - (T)P.solcdec * (T)P.solcdec);
+        if (P.ndcycle == 1) zmuz = solslat * solsdec + solclatcdec * cos((T)P.zmins * (T)P.zrtim - PI);
+        else zmuz = solslat * solsdec + solclatcdec / PI;
+    }
+    return (zmuz > zdawn) ? zmuz : (T)0.0;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(RAD_WARPS * 32) k_radstep(RadDev D) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -466,26 +490,32 @@ __global__ void __launch_bounds__(RAD_WARPS * 32) k_radstep(RadDev D) {
         // solang (radmod.f90:1380-1436)
         T mu0;
         if (P.nsol == 1) {
-            T zdawn = sin((T)P.dawn * PI / (T)180.0), zmuz;
-            if (P.ncstsol == 0) {
-                T zrlon = TWOPI / nlon;
-                T zhangle = (T)P.zmins * (T)P.zrtim + jlon * zrlon - PI;
-                if (P.ngenkeplerian == 1) zhangle = zhangle - (T)P.rasc;
-                if (zhangle < -PI) zhangle = zhangle + TWOPI;
-                if (zhangle > PI) zhangle = zhangle - TWOPI;
-                if (P.nfixed == 1) zhangle = zhangle + PI;
-                zmuz = sin((T)P.zdecl) * sid[jlat] + cola[jlat] * cos((T)P.zdecl) * cos(zhangle);
-            } else {
-                T solclatcdec = (T)P.solclat * (T)P.solcdec;
-                T solslat = sqrt((T)1 - (T)P.solclat * (T)P.solclat);
-                T solsdec = sqrt((T)1 - (T)P.solcdec * (T)P.solcdec);
-                if (P.ndcycle == 1) zmuz = solslat * solsdec + solclatcdec * cos((T)P.zmins * (T)P.zrtim - PI);
-                else zmuz = solslat * solsdec + solclatcdec / PI;
-            }
-            mu0 = (zmuz > zdawn) ? zmuz : (T)0.0;
+            mu0 = solang_mu<T>(P, sid, cola, jlat, jlon, nlon);
             if (lane == 0) gmu0[col] = mu0;
         } else {
             mu0 = gmu0[col];
+        }
+        // insolation and cloud zenith factors (radmod.f90:1650-1669): the
+        // column's own cos zenith, or with ndcycle = 0 the means over its
+        // latitude row -- over the sunlit columns (clouds) and over all
+        // (insolation).  Every warp of the row forms the same sums, reading the
+        // row's gmu0 or, when this launch computes gmu0, evaluating solang for
+        // each column of the row itself.
+        T mu1 = mu0;
+        if (P.ndcycle == 0) {
+            T zsum = 0;
+            int icnt = 0;
+            for (int j = lane; j < nlon; j += 32) {
+                T g = P.nsol == 1 ? solang_mu<T>(P, sid, cola, jlat, j, nlon) : gmu0[(size_t)jlat * nlon + j];
+                zsum += g;
+                icnt += g > (T)0.0 ? 1 : 0;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                zsum += __shfl_xor_sync(0xffffffffu, zsum, o);
+                icnt += __shfl_xor_sync(0xffffffffu, icnt, o);
+            }
+            mu0 = icnt > 0 ? zsum / (T)icnt : (T)0.0;
+            mu1 = icnt > 0 ? zsum / (T)nlon : (T)0.0;
         }
         // mko3 (radmod.f90:1489-1522): serial in height on lane 0
         if (P.no3 == 1) {
@@ -512,7 +542,7 @@ __global__ void __launch_bounds__(RAD_WARPS * 32) k_radstep(RadDev D) {
         T dalb = dalbv[col];
         T dsalb[2] = {dsalbv[2 * col], dsalbv[2 * col + 1]};
         if (P.nswr == 1) {
-            swr_warp<T>(P, s, L, mu0, mu0, dp, dalb, dsalb, dls, dicec, csol1, csol2, crco, lane);
+            swr_warp<T>(P, s, L, mu0, mu1, dp, dalb, dsalb, dls, dicec, csol1, csol2, crco, lane);
         } else {
             for (int k = lane; k < E; k += 32) { s.fu[k] = 0; s.fd[k] = 0; s.sw[k] = 0; }
         }

@@ -814,6 +814,9 @@ EXOTX_API exotx_status exotx_rad_surrogate(exotx_mlp net, const exotx_rad_params
     if (!net->prepared || !net->has_norm) return EXOTX_BAD_ARG;
     if (net->nin != surr_nin(p->nlev) || net->nout != surr_nout(p->nlev)) return EXOTX_BAD_DIM;
     if (p->nsol != 0) return EXOTX_NOT_BUILT;  // the cosine of the zenith angle is an input (gmu0)
+    // the network was trained on each column's own cos zenith; zonal-mean
+    // insolation (ndcycle = 0) is a different input
+    if (p->ndcycle != 1) return EXOTX_NOT_BUILT;
     cudaStream_t s = (cudaStream_t)sv;
     if (net->fb_cap < p->nhor) {
         cudaFree(net->fb);

@@ -179,9 +179,12 @@ exotx_status exotx_ensemble_tune(exotx_ensemble e, const float *spin, float *gpo
  * and returns EXOTX_BAD_DIM, before any work, for sets that need more.
  * prec is EXOTX_FP64 or EXOTX_FP32 (EXOTX_MIXED -> EXOTX_BAD_ARG).  Results
  * equal exotx_forward_set's.  The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture.  All calls on a device share the array: calls
- * that overlap on the GPU (different streams or threads without
+ * array's device address (cudaGetSymbolAddress) and copies the FFT twiddles
+ * into the array, so make that first call before any stream capture.  A later
+ * call whose NLON or precision differs from the twiddles the array holds
+ * copies them in again from host memory, which may wait for the stream; do
+ * that one outside stream capture too.  All calls on a device share the
+ * array: calls that overlap on the GPU (different streams or threads without
  * synchronisation between them) race. */
 #define EXOTX_STATIC_WORK_BYTES (16u << 20)
 exotx_status exotx_forward_set_noalloc(exotx_plan p, int prec, const void *gpin, void *spout,

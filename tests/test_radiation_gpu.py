@@ -20,11 +20,12 @@ RATES = ("dtdt", "dtdtswr", "dtdtlwr", "dconv")
 def _run(oracle, nlat, nlev, precision, seed=2, **over):
     cols, g = S.radiation_columns(nlat, nlev, seed=seed)
     nhor, nlon = g["nhor"], g["nlon"]
-    params = R.default_params(nlev, nhor, nlon, nsol=0, **over)
+    over.setdefault("nsol", 0)
+    params = R.default_params(nlev, nhor, nlon, **over)
     # identical sigma levels on both sides: the synthetic columns clip T at
     # 150 K, which makes some of radmod's branch tests exact ties
     sig = [np.array(getattr(params, k)[:nlev]) for k in ("sigma", "sigmah", "dsigma")]
-    p_ref = oracle.radpar(nlev, nhor, nlon, *sig, nsol=0, **over)
+    p_ref = oracle.radpar(nlev, nhor, nlon, *sig, **over)
     ref = oracle.radstep(p_ref, cols["sid"], cols["cola"], cols)
     dt = torch.float64 if precision == "fp64" else torch.float32
     dev = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=dt, device="cuda") for k, v in cols.items()}
@@ -84,3 +85,46 @@ def test_energy_closure(oracle):
     heat = np.sum(got["dtdt"] * ds * cols["dp"][None, :] * cp / p.ga, axis=0)
     net = got["dflux"][0] - got["dflux"][10]
     assert relerr(heat, net) < 1e-12
+
+
+# solang (radmod.f90:1336-1444) computed on the GPU: the daily cycle, a dawn
+# angle, the tidally locked fixed substellar point (nfixed = 1 sets zrtim =
+# 2 pi, zmins = 1 - fixedlon/360 and zdecl = obliquity, :1395-1401), a
+# constant solar angle (ncstsol) and the generalised Keplerian orbit's right
+# ascension (ngenkeplerian); then the zonal-mean insolation of ndcycle = 0
+# (:1650-1669) on the GPU's own gmu0 and on given gmu0
+TWOPI = 2.0 * 3.14159265359
+SOLANG = {
+    "daily": dict(nsol=1, zdecl=0.3, zmins=400.0),
+    "dawn": dict(nsol=1, zdecl=-0.35, zmins=1130.0, dawn=4.0),
+    "nfixed": dict(nsol=1, nfixed=1, zrtim=TWOPI, zmins=1.0 - 47.0 / 360.0, zdecl=0.41),
+    "ncstsol": dict(nsol=1, ncstsol=1, solclat=0.8, solcdec=0.93, zmins=300.0),
+    "genkeplerian": dict(nsol=1, ngenkeplerian=1, rasc=0.7, zdecl=0.1, zmins=700.0),
+    "zonal_mean_solang": dict(nsol=1, ndcycle=0, zdecl=0.3, zmins=100.0),
+    "zonal_mean_cstsol": dict(nsol=1, ncstsol=1, ndcycle=0, solclat=0.6, solcdec=0.9),
+    "zonal_mean_given_mu0": dict(nsol=0, ndcycle=0),
+}
+
+
+@pytest.mark.parametrize("case", list(SOLANG))
+def test_radstep_solang_fp64(oracle, case):
+    got, ref = _run(oracle, 32, 10, "fp64", seed=11, **SOLANG[case])
+    if SOLANG[case]["nsol"] == 1:
+        # the on-GPU cos zenith itself, then everything downstream of it
+        assert np.max(np.abs(got["gmu0"] - ref["gmu0"])) < 1e-14
+        assert (got["gmu0"] > 0).any() and (got["gmu0"] == 0).any()
+    for k in FLUXES + RATES + ("dqo3", "dalb", "dsalb"):
+        assert relerr(got[k], ref[k]) < 1e-11, (case, k)
+
+
+def test_radstep_zonal_mean_is_zonally_uniform(oracle):
+    # with ndcycle = 0 every column of a latitude row gets the same insolation
+    got, _ = _run(oracle, 32, 10, "fp64", seed=11, nsol=1, ndcycle=0, zdecl=0.3, zmins=100.0)
+    nlon = 64
+    top = got["dfd"][0].reshape(-1, nlon)
+    assert np.all(np.abs(top - top[:, :1]) <= 1e-12 * np.abs(top).max())
+
+
+def test_radstep_solang_fp32(oracle):
+    got, ref = _run(oracle, 32, 10, "fp32", seed=11, **SOLANG["daily"])
+    assert np.max(np.abs(got["gmu0"] - ref["gmu0"])) < 1e-5

@@ -86,3 +86,7 @@ def test_bench_reference_arm_prints_on_rank_zero_only():
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     for k in ("metric", "unit", "steps", "warmup", "ms_per_step", "higher_is_better", "config", "cpu_baseline", "e2e"):
         assert k in line, k
+    # both arms print one metric string and state the batch alike, so their lines compare
+    import bench
+    assert line["metric"] == bench.METRIC and line["unit"] == "round-trips/s"
+    assert line["config"]["workload"] == bench.WORKLOAD and line["config"]["batch"] == bench.BATCH

@@ -243,7 +243,7 @@ def test_smallest_resolution(plans, oracle):
     assert relerr(out[0], L.sp2fc(sp[0])) < FP64_TOL
 
 
-@pytest.mark.parametrize("nlat,nlev", [(32, 10), (64, 20), (96, 10), (256, 25)])
+@pytest.mark.parametrize("nlat,nlev", [(32, 10), (64, 20), (96, 10), (192, 20), (256, 25)])
 def test_transform_sets_fp64(plans, oracle, nlat, nlev):
     P = plans[nlat]
     L = oracle.Leg(nlat)
@@ -289,3 +289,47 @@ def test_roundtrip_identity_t127(plans):
     gp2fc(g)
     back = P.fc2sp(g).cpu().numpy()
     assert relerr(back, sp) < 1e-10
+
+
+# the model's spectral filters (legmod.f90:124-155): Cesaro, exponential,
+# Lander-Hoskins and Riesz-2, applied grid->spectral (ngptfilter) and
+# spectral->grid (nspvfilter), through the plan the GPU builds
+FILTERS = [dict(nfilter=1, ngptfilter=1, nspvfilter=1),
+           dict(nfilter=2, ngptfilter=1, nspvfilter=1, filterkappa=6.0, nfilterexp=6),
+           dict(nfilter=3, ngptfilter=1, nspvfilter=1, landhoskn0=12.0),
+           dict(nfilter=4, ngptfilter=1, nspvfilter=0),
+           dict(nfilter=2, ngptfilter=0, nspvfilter=1)]
+
+
+@pytest.mark.parametrize("filt", range(len(FILTERS)))
+def test_model_filters(oracle, filt):
+    kw = FILTERS[filt]
+    nlat, nlev = 64, 4
+    P = Plan(nlat, **kw)
+    L = oracle.Leg(nlat, **kw)
+    for t in TABLES:
+        assert relerr(P.table(t), L.table(t).reshape(nlat, L.ncsp)) < 1e-12, t
+    sp = _spec(P.ntru, 2, seed=17)
+    fc = P.sp2fc(_cuda(sp)).cpu().numpy()
+    for v in range(2):
+        assert relerr(fc[v], L.sp2fc(sp[v])) < FP64_TOL
+    gin = np.random.default_rng(18).standard_normal((2, nlat, 2 * nlat))
+    fsp = P.fc2sp(_cuda(gin)).cpu().numpy()
+    for v in range(2):
+        assert relerr(fsp[v], L.fc2sp(gin[v])) < FP64_TOL
+    # whole sets in FP64 and on the tensor cores (the filter is folded into
+    # the split tables there)
+    spin = S.transform_state(P.ntru, nlev, seed=19)
+    ref = L.inverse_set(spin, nlev, plavor=S.EZ)
+    gp = P.inverse_set(_cuda(spin), nlev).cpu().numpy().reshape(6 * nlev + 3, -1)
+    gpm = P.inverse_set(_cuda(spin, torch.float32), nlev, precision="mixed").cpu().numpy().reshape(6 * nlev + 3, -1)
+    g4 = S.grid_tendencies(nlat, nlev, seed=20)
+    refs = L.forward_set(g4.reshape(9 * nlev + 1, -1), nlev)
+    spo = P.forward_set(_cuda(g4), nlev).cpu().numpy()
+    spm = P.forward_set(_cuda(g4, torch.float32), nlev, precision="mixed").cpu().numpy()
+    for f in range(6 * nlev + 3):
+        assert relerr(gp[f], ref[f]) < FP64_TOL, f
+        assert relerr(gpm[f], ref[f]) < 5e-6, f
+    for f in range(4 * nlev + 1):
+        assert relerr(spo[f], refs[f]) < FP64_TOL, f
+        assert relerr(spm[f], refs[f]) < 5e-6, f

@@ -58,6 +58,21 @@ def test_noalloc_matches_forward_set(nlat, nlev, prec):
         _fields_close(o, ref, TOL[prec])
 
 
+def test_noalloc_alternating_grids_and_precisions():
+    # the array keeps one set of twiddles; calls that switch grid length or
+    # precision back and forth must each see their own
+    runs = [(32, 10, "fp64"), (64, 10, "fp64"), (32, 10, "fp32"), (32, 10, "fp64"), (64, 10, "fp64")]
+    plans = {n: Plan(n) for n in (32, 64)}
+    for nlat, nlev, prec in runs:
+        P = plans[nlat]
+        g = torch.as_tensor(S.grid_tendencies(nlat, nlev, seed=nlat + nlev), device="cuda").to(DT[prec])
+        o = torch.full((4 * nlev + 1, P.nrsp), float("nan"), dtype=DT[prec], device="cuda")
+        assert _noalloc(P, prec, g, o, nlev) == 0
+        ref = P.forward_set(g, nlev, precision=prec)
+        torch.cuda.synchronize()
+        _fields_close(o, ref, TOL[prec])
+
+
 def test_noalloc_rejects_oversized_and_mixed():
     nlev = 20
     P = Plan(96)  # T63 L20 FP64 needs ~17.8 MB of scratch, above the 16 MiB array
