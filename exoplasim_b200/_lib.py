@@ -82,6 +82,7 @@ SIGNATURES = {
     "exotx_inverse_set_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_forward_set_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_sets_host": [_P, _I, _P, _P, _P, _P, _I, _I, _S],
+    "exotx_sets_host_f64": [_P, _I, _P, _P, _P, _P, _I, _I, _S],
     "exotx_forward_set_noalloc": [_P, _I, _P, _P, _I, _S],
     "exotx_kernel_timing": [_I],
     "exotx_ensemble_create": [_I, _P, _P, C.POINTER(C.c_void_p)],

@@ -165,6 +165,9 @@ exotx_status fft_forward_fold(const float *in, float *out, int n, int nlat, long
                               cudaStream_t s);
 exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s);
 
+// element-wise FP64 <-> FP32 conversion of n device reals (fortran_abi.cu)
+exotx_status convert_reals(const void *in, size_t in_esz, void *out, size_t out_esz, size_t n, cudaStream_t s);
+
 // radstep over all columns or a device-side column list (radiation.cu)
 exotx_status radstep_columns(const exotx_rad_params *p, int prec, const exotx_rad_io *io, const int *cols,
                              const int *ncols, int maxcols, cudaStream_t st);

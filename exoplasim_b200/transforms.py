@@ -248,15 +248,17 @@ class Plan:
         call("exotx_forward_set_batch", self._h, p, _ptr(gpin), _ptr(out), nlev, ninst, _stream())
         return out
 
-    def sets_host(self, nlev, spin=None, gpout=None, gpin=None, spout=None, precision="mixed"):
+    def sets_host(self, nlev, spin=None, gpout=None, gpin=None, spout=None, precision="mixed", host_fp64=False):
         """Both transform sets for states held in HOST tensors (page-locked for
         overlap): spin (ninst, 4L+1, NRSP) -> gpout (ninst, 6L+3, NLAT, NLON) and
         gpin (ninst, 9L+1, NLAT, NLON) -> spout (ninst, 4L+1, NRSP); leave out a
         half by passing None for both of its tensors.  The copies and transforms
         of neighbouring states overlap; the current stream waits for the last
-        copy out, so synchronise it before reading the outputs."""
+        copy out, so synchronise it before reading the outputs.  host_fp64: the
+        host tensors are float64 whatever the precision (an 8-byte model's
+        arrays), converted on the device (exotx_sets_host_f64)."""
         p = _prec(precision)
-        dt = _dtype(p)
+        dt = torch.float64 if host_fp64 else _dtype(p)
         ninst = (spin if spin is not None else gpin).shape[0]
         shapes = {"spin": (ninst, 4 * nlev + 1, self.nrsp), "gpout": (ninst, 6 * nlev + 3, self.nlat, self.nlon),
                   "gpin": (ninst, 9 * nlev + 1, self.nlat, self.nlon), "spout": (ninst, 4 * nlev + 1, self.nrsp)}
@@ -270,7 +272,7 @@ class Plan:
             if t.dtype != dt or tuple(t.shape) != shapes[name] or not t.is_contiguous():
                 raise ValueError(f"{name} must be a contiguous {dt} tensor of shape {shapes[name]}")
             ptrs.append(_ptr(t))
-        call("exotx_sets_host", self._h, p, *ptrs, nlev, ninst, _stream())
+        call("exotx_sets_host_f64" if host_fp64 else "exotx_sets_host", self._h, p, *ptrs, nlev, ninst, _stream())
 
 
 def tc_error():

@@ -138,6 +138,15 @@ exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const void *gpin, v
 exotx_status exotx_sets_host(exotx_plan p, int prec, const void *h_spin, void *h_gpout,
                              const void *h_gpin, void *h_spout, int nlev, int ninst,
                              exotx_stream s);
+/* exotx_sets_host for FP64 host arrays whatever prec is: the array kind of a
+ * model built with -fdefault-real-8 (the reference's recommended build).
+ * With EXOTX_FP32 or EXOTX_MIXED the FP64 arrays are copied to the device as
+ * they are and converted there (round to nearest) before the transforms, and
+ * the results converted back to FP64 before the copy out, so an 8-byte model
+ * runs the tensor-core sets without converting on the host. */
+exotx_status exotx_sets_host_f64(exotx_plan p, int prec, const double *h_spin, double *h_gpout,
+                                 const double *h_gpin, double *h_spout, int nlev, int ninst,
+                                 exotx_stream s);
 /* Uneven ensembles (no counterpart in the reference, which runs one model
  * state per process): ninst instances with their own nlat (NLON = 2 NLAT) and
  * level count, MIXED precision (float arrays).  Instances of one resolution

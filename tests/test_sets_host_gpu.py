@@ -57,3 +57,22 @@ def test_one_half_and_bad_arguments():
     P.sets_host(nlev, spin, gout)       # inverse half alone
     torch.cuda.current_stream().synchronize()
     assert torch.equal(gout, P.inverse_set_batch(spin.cuda(), nlev).cpu())
+
+
+@pytest.mark.parametrize("nlat,nlev,ninst,prec", [(32, 10, 5, "mixed"), (64, 20, 3, "fp32"), (32, 10, 2, "fp64")])
+def test_fp64_host_arrays(nlat, nlev, ninst, prec):
+    # an 8-byte model's arrays: FP64 on the host whatever the transforms'
+    # precision; the conversion on the device rounds to nearest, as torch does
+    P = Plan(nlat)
+    spin, gin = _host_states(P, nlev, ninst, torch.float64, seed=nlat + 7)
+    gout = torch.full((ninst, 6 * nlev + 3, P.nlat, P.nlon), float("nan"), dtype=torch.float64).pin_memory()
+    sout = torch.full((ninst, 4 * nlev + 1, P.nrsp), float("nan"), dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        P.sets_host(nlev, spin, gout, gin, sout, precision=prec, host_fp64=True)
+        torch.cuda.current_stream().synchronize()
+        dt = DT[prec]
+        ref_g = P.inverse_set_batch(spin.cuda().to(dt), nlev, precision=prec).double()
+        ref_s = P.forward_set_batch(gin.cuda().to(dt), nlev, precision=prec).double()
+        torch.cuda.synchronize()
+        assert torch.equal(gout, ref_g.cpu())
+        assert torch.equal(sout, ref_s.cpu())
