@@ -2,8 +2,10 @@
 
 The reference ships no golden vectors for these routines and no Fortran
 compiler exists here, so the oracle is pinned by (a) mathematical identities
-the reference's algorithms must satisfy and (b) fixtures from numpy/scipy
-(tests/golden/, made by tests/golden/make_golden.py).
+the reference's algorithms must satisfy, (b) fixtures from numpy/scipy
+(tests/golden/, made by tests/golden/make_golden.py) and (c) for the
+longwave scheme, a second restatement written separately in numpy
+(oracle/lwr_numpy.py).
 """
 import math
 import os
@@ -11,6 +13,7 @@ import os
 import numpy as np
 import pytest
 
+from exoplasim_b200 import synthetic as S
 from tests._util import relerr
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_v1.npz")
@@ -195,3 +198,73 @@ def test_pyfft_compositions(oracle):
     assert relerr(c[2::2], X.real[1:32]) < 1e-14 and relerr(c[3::2], X.imag[1:32]) < 1e-14
     # the FFT991 variant (pyfft991 for NLAT 192 and 320) agrees with fftmod
     assert relerr(PO.gp3fc(a, use991=True), c) < 1e-14
+
+
+# ---- an independent second restatement of lwr pins the C oracle's fits ----
+def _lwr_pair(O, nlat, nlev, seed, **over):
+    from oracle import lwr_numpy as LN
+    cols, g = S.radiation_columns(nlat, nlev, seed=seed)
+    sig = O.default_sigma(nlev)
+    p = O.radpar(nlev, g["nhor"], g["nlon"], *sig, nsol=0, nswr=0, **over)
+    ref = O.radstep(p, cols["sid"], cols["cola"], cols)
+    pd = dict(nlev=nlev, sigma=sig[0], sigmah=sig[1], dsigma=sig[2], ga=p.ga, acllwr=p.acllwr, clgray=p.clgray,
+              th2oc=p.th2oc, tpofmt=p.tpofmt, npbroaden=p.npbroaden)
+    got = LN.lwr(pd, cols["dt"], cols["dq"], cols["dcc"], cols["dql"], ref["dqo3"], cols["dqco2"], cols["dp"],
+                 cols["dls"])
+    return got, ref
+
+
+@pytest.mark.parametrize("over", [{}, {"clgray": 0.5}, {"npbroaden": 0}, {"th2oc": 0.0}, {"tpofmt": 0.9}])
+def test_lwr_matches_independent_numpy_restatement(oracle, over):
+    # lwr_numpy.py restates radmod.f90:2122-2456 in numpy from the Fortran, apart
+    # from exo_oracle_rad.c: the two agree to rounding on every flux
+    (u, d, l), ref = _lwr_pair(oracle, 16, 20, seed=31, **over)
+    for k, v in (("dftu", u), ("dftd", d), ("dlwfl", l)):
+        assert relerr(v, ref[k]) < 1e-12, k
+
+
+def test_lwr_fits_branches_and_continuity():
+    # the synthetic columns reach both sides of every absorptivity fit's switch,
+    # and the printed continuity constants make each fit continuous there
+    # (radmod.f90:2207-2218); a slipped coefficient breaks one of the two
+    from oracle import lwr_numpy as LN
+    eps = 1e-9
+    for name, x0 in (("h2o", 0.01), ("co2", 1.0), ("o3", 0.01), ("th2o", 2.0)):
+        lo = np.array([x0 - eps]); hi = np.array([x0 + eps]); z = np.array([1e-3])
+        args = {"h2o": (lo, z, z), "co2": (z, z, lo), "o3": (z, lo, z), "th2o": (lo, z, z)}[name]
+        argh = {"h2o": (hi, z, z), "co2": (z, z, hi), "o3": (z, hi, z), "th2o": (hi, z, z)}[name]
+        a = LN.absorptivities(*args, th2oc=0.0)
+        b = LN.absorptivities(*argh, th2oc=0.0)
+        idx = {"h2o": 0, "co2": 1, "th2o": 2, "o3": 3}[name]
+        assert abs(a[idx][0] - b[idx][0]) < 1e-6, name
+    # absorber paths of the test columns straddle the switches
+    from oracle import oracle as O
+    nlev = 20
+    cols, g = S.radiation_columns(16, nlev, seed=31)
+    sig = O.default_sigma(nlev)
+    zps2 = cols["dp"] ** 2
+    uwv = np.cumsum([0.1 * sig[0][j] * sig[2][j] / 9.80665 / 1e5 * zps2 * cols["dq"][j] for j in range(nlev)], axis=0)
+    assert (uwv <= 0.01).any() and (uwv > 2.0).any()
+
+
+@pytest.mark.parametrize("over", [{}, {"nswrcl": 0}, {"necham": 0, "necham6": 1}, {"newrsc": 1}, {"nrscat": 0},
+                                  {"nclouds": 0}, {"rcoeff": 2.5, "zsolar1": 0.6, "zsolar2": 0.4}])
+def test_swr_matches_independent_numpy_restatement(oracle, over):
+    # swr_numpy.py restates radmod.f90:1530-2116 in numpy from the Fortran, apart
+    # from exo_oracle_rad.c: fluxes and updated albedos agree to rounding
+    from oracle import swr_numpy as SN
+    nlev = 20
+    cols, g = S.radiation_columns(16, nlev, seed=37)
+    sig = oracle.default_sigma(nlev)
+    p = oracle.radpar(nlev, g["nhor"], g["nlon"], *sig, nsol=0, nlwr=0, **over)
+    ref = oracle.radstep(p, cols["sid"], cols["cola"], cols)
+    pd = {f[0]: getattr(p, f[0]) for f in oracle.RadPar._fields_}
+    pd.update(sigma=sig[0], sigmah=sig[1], dsigma=sig[2], rcl1=list(p.rcl1), rcl2=list(p.rcl2),
+              acl2=list(p.acl2))
+    mu = cols["gmu0"]
+    got = SN.swr(pd, mu, mu, cols["dt"], cols["dq"], cols["dcc"], cols["dql"], ref["dqo3"], cols["dp"],
+                 cols["dalb"], cols["dsalb"], cols["dls"], cols["dicec"])
+    for k, v in zip(("dfu", "dfd", "dswfl", "dalb", "dsalb"), got):
+        assert np.all(np.isfinite(v)), k
+        assert relerr(v, ref[k]) < 1e-12, k
+    assert (mu > 0).any() and (mu == 0).any()
