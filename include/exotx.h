@@ -198,6 +198,27 @@ exotx_status exotx_ensemble_tune(exotx_ensemble e, const float *spin, float *gpo
 #define EXOTX_STATIC_WORK_BYTES (16u << 20)
 exotx_status exotx_forward_set_noalloc(exotx_plan p, int prec, const void *gpin, void *spout,
                                        int nlev, exotx_stream s);
+/* ---- raw output records (outmod.f90 writegp :97-134, writesp :140-169) ----
+ * One output field = an 8-word int32 header record and a float32 data record,
+ * each framed by 4-byte length markers (Fortran unformatted sequential, as
+ * gfortran writes it): 48 + 4n bytes for n values.  kind 0 (writegp) converts
+ * n grid values to float32; kind 1 (writesp) multiplies spectral real i by
+ * spnorm(i) = (-1)^m / sqrt(2) (plasim.f90:1637-1650) and pscale, adds poff to
+ * the first, and converts.  head holds the header words as the model sets
+ * them (code, level, date, time, dimensions, step, days per year). */
+typedef struct {
+    int head[8];
+    const void *src;      /* DEVICE array of n values of precision prec (FP64 or FP32) */
+    long long n;
+    int prec, kind, ntru; /* ntru: truncation of a spectral field */
+    double pscale, poff;
+} exotx_raw_rec;
+/* bytes of the records' image (HOST array of nrec descriptors) */
+exotx_status exotx_raw_size(const exotx_raw_rec *recs, int nrec, size_t *nbytes);
+/* the byte image of the records, in order, into the DEVICE buffer out
+ * (exotx_raw_size bytes); copy it to the host and append it to the file */
+exotx_status exotx_raw_pack(const exotx_raw_rec *recs, int nrec, void *out, exotx_stream s);
+
 /* Per-kernel device time (diagnostics; no counterpart in the reference).
  * While enabled, launches of these kernels outside stream capture are
  * bracketed by CUDA events on the launching stream.  exotx_kernel_time
