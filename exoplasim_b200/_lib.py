@@ -81,6 +81,12 @@ SIGNATURES = {
     "exotx_tc_selftest": [_P, _P, _P, _I, _I, _I, _S],
     "exotx_inverse_set_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_forward_set_batch": [_P, _I, _P, _P, _I, _I, _S],
+    "exotx_inverse_set_d": [_P, _I, _P, _P, _I, _S],
+    "exotx_forward_set_d": [_P, _I, _P, _P, _I, _S],
+    "exotx_inverse_set_d_batch": [_P, _I, _P, _P, _I, _I, _S],
+    "exotx_forward_set_d_batch": [_P, _I, _P, _P, _I, _I, _S],
+    "exotx_raw_size": [_P, _I, C.POINTER(C.c_size_t)],
+    "exotx_raw_pack": [_P, _I, _P, _S],
     "exotx_sets_host": [_P, _I, _P, _P, _P, _P, _I, _I, _S],
     "exotx_sets_host_f64": [_P, _I, _P, _P, _P, _P, _I, _I, _S],
     "exotx_forward_set_noalloc": [_P, _I, _P, _P, _I, _S],

@@ -72,6 +72,56 @@ static exotx_status forward_set_simt(exotx_plan p, const T *gpin, T *spout, int 
     return EXOTX_OK;
 }
 
+// gridpointd (plasim.f90:3142-3149): invlegd (legmod.f90:661-677) and fc2gp.
+// spin (4L+1 fields) sd, st, sz, sq, sp -> gpout (4L+1) gu, gv, gt, gq, gp
+template <typename T>
+static exotx_status inverse_set_d_simt(exotx_plan p, const T *spin, T *gpout, int L, cudaStream_t s) {
+    const long long nrsp = 2LL * p->ncsp;
+    const long long nfld = 4LL * L + 1, nrows = nfld * p->nlat;
+    EXOTX_TRY(ensure_work(p, sizeof(T) * 2 * (size_t)nrows * p->ntp1));
+    T *w = (T *)p->d_work;
+    FourierLayout F = mmajor_layout(p, nrows);
+    const T *sd = spin, *st = spin + L * nrsp, *sz = spin + 2 * L * nrsp, *sq = spin + 3 * L * nrsp,
+            *sp = spin + 4 * L * nrsp;
+    auto fld = [&](long long f) { return w + 2 * f * p->nlat; };
+    EXOTX_TRY(leg_inverse_l<T>(p, OP_DV2UV, sd, sz, fld(0), fld(L), L, nrsp, nrsp, F, s));
+    EXOTX_TRY(leg_inverse_l<T>(p, OP_SP2FC, st, nullptr, fld(2 * L), nullptr, L, nrsp, 0, F, s));
+    EXOTX_TRY(leg_inverse_l<T>(p, OP_SP2FC, sq, nullptr, fld(3 * L), nullptr, L, nrsp, 0, F, s));
+    EXOTX_TRY(leg_inverse_l<T>(p, OP_SP2FC, sp, nullptr, fld(4 * L), nullptr, 1, nrsp, 0, F, s));
+    return fft_inverse_l<T>(w, gpout, p->nlon, nrows, p->ntp1, 1, nrows, s);
+}
+
+// gridpointd (plasim.f90:3415-3428): gp2fc, fc2sp of the temperature and
+// humidity tendencies, uv2dv.  gpin (4L) gtdt, gudt, gvdt, gqdt -> spout (4L) sdf, stf, szf, sqf
+template <typename T>
+static exotx_status forward_set_d_simt(exotx_plan p, const T *gpin, T *spout, int L, cudaStream_t s) {
+    const long long nrsp = 2LL * p->ncsp;
+    const long long nfld = 4LL * L, nrows = nfld * p->nlat;
+    EXOTX_TRY(ensure_work(p, sizeof(T) * 2 * (size_t)nrows * p->ntp1));
+    T *w = (T *)p->d_work;
+    EXOTX_TRY(fft_forward_l<T>(gpin, w, p->nlon, nrows, p->ntp1, 1, nrows, s));
+    FourierLayout F = mmajor_layout(p, nrows);
+    auto fld = [&](long long f) -> const T * { return w + 2 * f * p->nlat; };
+    const T *gtdt = fld(0), *gudt = fld(L), *gvdt = fld(2 * L), *gqdt = fld(3 * L);
+    T *sdf = spout, *stf = spout + L * nrsp, *szf = spout + 2 * L * nrsp, *sqf = spout + 3 * L * nrsp;
+    {
+        const T *in[1] = {gtdt};
+        T *out[1] = {stf};
+        EXOTX_TRY(leg_forward_l<T>(p, OP_FC2SP, in, out, L, F, nrsp, s));
+    }
+    {
+        const T *in[1] = {gqdt};
+        T *out[1] = {sqf};
+        EXOTX_TRY(leg_forward_l<T>(p, OP_FC2SP, in, out, L, F, nrsp, s));
+    }
+    {
+        const T *in[2] = {gudt, gvdt};
+        T *out[2] = {sdf, szf};
+        EXOTX_TRY(leg_forward_l<T>(p, OP_UV2DV, in, out, L, F, nrsp, s));
+    }
+    return EXOTX_OK;
+}
+
 }  // namespace exotx
 
 using namespace exotx;
@@ -236,4 +286,57 @@ EXOTX_API exotx_status exotx_forward_set(exotx_plan p, int prec, const void *gpi
     if (prec == EXOTX_FP32)
         return forward_set_simt<float>(p, (const float *)gpin, (float *)spout, nlev, (cudaStream_t)s);
     return tc_forward_set(p, (const float *)gpin, (float *)spout, nlev, (cudaStream_t)s);
+}
+
+// ---- gridpointd sets ----
+EXOTX_API exotx_status exotx_inverse_set_d(exotx_plan p, int prec, const void *spin, void *gpout, int nlev,
+                                           exotx_stream s) {
+    PLAN_PREC_CHECK(p, prec);
+    if (!spin || !gpout || nlev < 1) return EXOTX_BAD_ARG;
+    if (prec == EXOTX_FP64)
+        return inverse_set_d_simt<double>(p, (const double *)spin, (double *)gpout, nlev, (cudaStream_t)s);
+    if (prec == EXOTX_FP32)
+        return inverse_set_d_simt<float>(p, (const float *)spin, (float *)gpout, nlev, (cudaStream_t)s);
+    return tc_inverse_batch_d(p, (const float *)spin, (float *)gpout, nlev, 1, (cudaStream_t)s);
+}
+
+EXOTX_API exotx_status exotx_forward_set_d(exotx_plan p, int prec, const void *gpin, void *spout, int nlev,
+                                           exotx_stream s) {
+    PLAN_PREC_CHECK(p, prec);
+    if (!gpin || !spout || nlev < 1) return EXOTX_BAD_ARG;
+    if (prec == EXOTX_FP64)
+        return forward_set_d_simt<double>(p, (const double *)gpin, (double *)spout, nlev, (cudaStream_t)s);
+    if (prec == EXOTX_FP32)
+        return forward_set_d_simt<float>(p, (const float *)gpin, (float *)spout, nlev, (cudaStream_t)s);
+    return tc_forward_batch_d(p, (const float *)gpin, (float *)spout, nlev, 1, (cudaStream_t)s);
+}
+
+EXOTX_API exotx_status exotx_inverse_set_d_batch(exotx_plan p, int prec, const void *spin, void *gpout, int nlev,
+                                                 int ninst, exotx_stream s) {
+    PLAN_PREC_CHECK(p, prec);
+    if (ninst == 0) return EXOTX_OK;
+    if (!spin || !gpout || nlev < 1 || ninst < 0) return EXOTX_BAD_ARG;
+    if (prec == EXOTX_MIXED)
+        return tc_inverse_batch_d(p, (const float *)spin, (float *)gpout, nlev, ninst, (cudaStream_t)s);
+    const size_t esz = prec == EXOTX_FP64 ? 8 : 4;
+    const size_t in_b = (size_t)(4 * nlev + 1) * 2 * p->ncsp * esz;
+    const size_t out_b = (size_t)(4 * nlev + 1) * p->nlat * p->nlon * esz;
+    for (int i = 0; i < ninst; i++)
+        EXOTX_TRY(exotx_inverse_set_d(p, prec, (const char *)spin + i * in_b, (char *)gpout + i * out_b, nlev, s));
+    return EXOTX_OK;
+}
+
+EXOTX_API exotx_status exotx_forward_set_d_batch(exotx_plan p, int prec, const void *gpin, void *spout, int nlev,
+                                                 int ninst, exotx_stream s) {
+    PLAN_PREC_CHECK(p, prec);
+    if (ninst == 0) return EXOTX_OK;
+    if (!gpin || !spout || nlev < 1 || ninst < 0) return EXOTX_BAD_ARG;
+    if (prec == EXOTX_MIXED)
+        return tc_forward_batch_d(p, (const float *)gpin, (float *)spout, nlev, ninst, (cudaStream_t)s);
+    const size_t esz = prec == EXOTX_FP64 ? 8 : 4;
+    const size_t in_b = (size_t)(4 * nlev) * p->nlat * p->nlon * esz;
+    const size_t out_b = (size_t)(4 * nlev) * 2 * p->ncsp * esz;
+    for (int i = 0; i < ninst; i++)
+        EXOTX_TRY(exotx_forward_set_d(p, prec, (const char *)gpin + i * in_b, (char *)spout + i * out_b, nlev, s));
+    return EXOTX_OK;
 }

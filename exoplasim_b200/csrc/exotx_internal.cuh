@@ -182,6 +182,9 @@ exotx_status tc_inverse_set(exotx_plan p, const float *spin, float *four, int nl
 exotx_status tc_forward_set(exotx_plan p, const float *four, float *spout, int nlev, cudaStream_t s);
 exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int L, int ninst, cudaStream_t s);
 exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int L, int ninst, cudaStream_t s);
+// the gridpointd sets (plasim.f90:3142-3149, :3415-3428) on the same kernels
+exotx_status tc_inverse_batch_d(exotx_plan p, const float *spin, float *gpout, int L, int ninst, cudaStream_t s);
+exotx_status tc_forward_batch_d(exotx_plan p, const float *gpin, float *spout, int L, int ninst, cudaStream_t s);
 // uneven ensembles: a segment is a run of instances of one resolution and level count
 constexpr int TC_MAXSEG = 12;  // segments per tensor-core launch
 struct EnsSeg {

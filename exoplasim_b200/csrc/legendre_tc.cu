@@ -119,7 +119,7 @@ struct TcTables {
     unsigned char *fwd3 = nullptr;
     long long *d_fwd3_off = nullptr;
     // cached job lists, keyed by (direction, nlev, ninst)
-    struct Jobs { int dir, nlev, ninst, njobs; int4 *d = nullptr; };
+    struct Jobs { int dir, nlev, ninst, njobs, dset; int4 *d = nullptr; };
     std::vector<Jobs> jobs;
     ~TcTables() {
         cudaFree(inv); cudaFree(fwd); cudaFree(d_inv_off); cudaFree(d_fwd_off);
@@ -397,15 +397,21 @@ static exotx_status launch_fwd(const TcFwdLaunch &P, int level, int njobs, size_
     return EXOTX_OK;
 }
 
-static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst, const int4 **d, int *njobs) {
+// dset = 1: the gridpointd inverse set (qi on st, sq, sp; no qj job), whose
+// forward jobs are the gridpointa ones
+static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst, const int4 **d, int *njobs,
+                            int dset = 0) {
+    if (dir == 1) dset = 0;
     for (auto &j : T->jobs)
-        if (j.dir == dir && j.nlev == L && j.ninst == ninst) { *d = j.d; *njobs = j.njobs; return EXOTX_OK; }
+        if (j.dir == dir && j.nlev == L && j.ninst == ninst && j.dset == dset) {
+            *d = j.d; *njobs = j.njobs; return EXOTX_OK;
+        }
     std::vector<int4> v;
     int INV_NC_QI, INV_NC_UV;
     inv_tiles(T->nj8, p->ntp1, &INV_NC_QI, &INV_NC_UV);
     for (int m = 0; m < p->ntp1; m++) {
         if (dir == 0) {
-            const int n0 = ninst * (4 * L + 1) * 2, n1 = ninst * 2, n2 = ninst * L * 4;
+            const int n0 = ninst * (dset ? 2 * L + 1 : 4 * L + 1) * 2, n1 = dset ? 0 : ninst * 2, n2 = ninst * L * 4;
             for (int c = 0; c < n0; c += INV_NC_QI) v.push_back(make_int4(m, 0, c, std::min(INV_NC_QI, n0 - c)));
             for (int c = 0; c < n1; c += INV_NC_QI) v.push_back(make_int4(m, 1, c, std::min(INV_NC_QI, n1 - c)));
             for (int c = 0; c < n2; c += INV_NC_UV) v.push_back(make_int4(m, 2, c, std::min(INV_NC_UV, n2 - c)));
@@ -430,7 +436,7 @@ static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst
         }
     }
     TcTables::Jobs J;
-    J.dir = dir; J.nlev = L; J.ninst = ninst; J.njobs = (int)v.size();
+    J.dir = dir; J.nlev = L; J.ninst = ninst; J.njobs = (int)v.size(); J.dset = dset;
     if (cudaMalloc(&J.d, sizeof(int4) * v.size()) != cudaSuccess) return EXOTX_NO_MEM;
     if (cudaMemcpy(J.d, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess) return EXOTX_CUDA_ERR;
     T->jobs.push_back(J);
@@ -440,11 +446,12 @@ static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst
 }
 
 // ---------------------------------------------------------- set drivers
-exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int L, int ninst, cudaStream_t s) {
+static exotx_status tc_inverse_run(exotx_plan p, const float *spin, float *gpout, int L, int ninst, int dset,
+                                   cudaStream_t s) {
     TcTables *T;
     EXOTX_TRY(tc_tables(p, &T));
     const long long nrsp = 2LL * p->ncsp, nhor = (long long)p->nlat * p->nlon;
-    const int nfo = 6 * L + 3;
+    const int nfo = dset ? 4 * L + 1 : 6 * L + 3;
     // chunk instances so the m-major Fourier intermediate stays L2-resident (<= 80 MB of the 126 MB L2)
     const size_t per_inst = (size_t)nfo * p->nlat * p->ntp1 * sizeof(float2);
     int chunk = (int)std::max<size_t>(1, (80u << 20) / per_inst);
@@ -452,7 +459,7 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
     EXOTX_TRY(ensure_work(p, per_inst * chunk));
     const int4 *jobs;
     int njobs;
-    EXOTX_TRY(tc_jobs(p, T, 0, L, chunk, &jobs, &njobs));
+    EXOTX_TRY(tc_jobs(p, T, 0, L, chunk, &jobs, &njobs, dset));
     int nc_qi, nc_uv;
     inv_tiles(T->nj8, p->ntp1, &nc_qi, &nc_uv);
     size_t smem = std::max(inv_smem(T->nj8, p->ntp1, nc_qi), inv_smem(T->nj8, p->ntp1, nc_uv));
@@ -462,7 +469,7 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
         const int ni = std::min(chunk, ninst - i0);
         const int4 *jl = jobs;
         int nj = njobs;
-        if (ni != chunk) EXOTX_TRY(tc_jobs(p, T, 0, L, ni, &jl, &nj));
+        if (ni != chunk) EXOTX_TRY(tc_jobs(p, T, 0, L, ni, &jl, &nj, dset));
         TcInvLaunch P;
         P.jobs = jl;
         P.nprod = 6;
@@ -474,6 +481,7 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
         A.nrows = (long long)ni * nfo * p->nlat;
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.nj8 = T->nj8; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
         A.plavor = (float)p->desc.plavor;
+        A.dset = dset;
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
         EXOTX_CUDA(launch_pdl(k_tc_inverse, dim3(nj), dim3(TCI), smem, s, P));   // set-up overlaps the last tail
         EXOTX_CHECK_LAUNCH();
@@ -484,11 +492,19 @@ exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int
     return EXOTX_OK;
 }
 
-exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int L, int ninst, cudaStream_t s) {
+exotx_status tc_inverse_batch(exotx_plan p, const float *spin, float *gpout, int L, int ninst, cudaStream_t s) {
+    return tc_inverse_run(p, spin, gpout, L, ninst, 0, s);
+}
+exotx_status tc_inverse_batch_d(exotx_plan p, const float *spin, float *gpout, int L, int ninst, cudaStream_t s) {
+    return tc_inverse_run(p, spin, gpout, L, ninst, 1, s);
+}
+
+static exotx_status tc_forward_run(exotx_plan p, const float *gpin, float *spout, int L, int ninst, int dset,
+                                   cudaStream_t s) {
     TcTables *T;
     EXOTX_TRY(tc_tables(p, &T));
     const long long nrsp = 2LL * p->ncsp, nhor = (long long)p->nlat * p->nlon;
-    const int nfi = 9 * L + 1;
+    const int nfi = dset ? 4 * L : 9 * L + 1, nfo = dset ? 4 * L : 4 * L + 1;
     const size_t per_inst = (size_t)nfi * p->nlat * p->ntp1 * sizeof(float2);
     int chunk = (int)std::max<size_t>(1, (80u << 20) / per_inst);
     chunk = std::min(chunk, ninst);
@@ -522,7 +538,8 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
             TcFwd3Launch P3;
             P3.jobs = jl;
             P3.nprod = 6;
-            fwd3_args(P3.seg[0], p, T, L, (const float2 *)p->d_work, nrows, spout + (size_t)i0 * (4 * L + 1) * nrsp);
+            fwd3_args(P3.seg[0], p, T, L, (const float2 *)p->d_work, nrows, spout + (size_t)i0 * nfo * nrsp);
+            P3.seg[0].dset = dset;
             EXOTX_TRY(launch_fwd_pipe(P3, nj, T->njc, folded, s));
             continue;
         }
@@ -535,11 +552,18 @@ exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int
         A.W = (const float2 *)p->d_work;
         A.nrows = nrows;
         A.filt = p->d_fg32;
-        A.spout = spout + (size_t)i0 * (4 * L + 1) * nrsp;
+        A.spout = spout + (size_t)i0 * nfo * nrsp;
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.njc = T->njc; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
+        A.dset = dset;
         EXOTX_TRY(launch_fwd(P, lv, nj, smem, s));
     }
     return EXOTX_OK;
+}
+exotx_status tc_forward_batch(exotx_plan p, const float *gpin, float *spout, int L, int ninst, cudaStream_t s) {
+    return tc_forward_run(p, gpin, spout, L, ninst, 0, s);
+}
+exotx_status tc_forward_batch_d(exotx_plan p, const float *gpin, float *spout, int L, int ninst, cudaStream_t s) {
+    return tc_forward_run(p, gpin, spout, L, ninst, 1, s);
 }
 
 // ---------------------------------------------------------- ensembles

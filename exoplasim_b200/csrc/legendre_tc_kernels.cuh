@@ -22,6 +22,7 @@ struct TcInvArgs {
     long long nrows;
     int L, nlat, nlath, nj8, ntp1, nrsp;
     float plavor;
+    int dset = 0;           // 0: gridpointa set (invlega), 1: gridpointd set (invlegd)
 };
 
 // One launch covers up to TC_MAXSEG segments (a resolution, a level count and
@@ -34,12 +35,21 @@ struct TcInvLaunch {
 };
 
 // spectral row (complex, filter not applied) feeding column pair gq, and
-// whether it is the vorticity of a dv2uv pair (planetary vorticity removed)
+// whether it is the vorticity of a dv2uv pair (planetary vorticity removed).
+// Group 0 takes every field of an instance in the gridpointa set (sd, st, sz,
+// sq, sp) and, in the gridpointd set, st, sq and sp only (invlegd,
+// legmod.f90:661-677): column pair j of an instance reads st (j < L), sq
+// (j < 2L) or sp (j = 2L), fields L + j for j < L and 2L + j after.
 __device__ __forceinline__ const float2 *inv_row(const TcInvArgs &A, int group, int gq, bool *zvort) {
     const int L = A.L, nf = 4 * L + 1;
     int inst, f;
     *zvort = false;
-    if (group == 0) { inst = gq / nf; f = gq % nf; }
+    if (group == 0 && A.dset) {
+        const int nf0 = 2 * L + 1;
+        inst = gq / nf0;
+        const int j = gq - inst * nf0;
+        f = j < L ? L + j : 2 * L + j;
+    } else if (group == 0) { inst = gq / nf; f = gq % nf; }
     else if (group == 1) { inst = gq; f = 4 * L; }
     else {
         // columns per level: Dr, Di, Zr, Zi -> pairs 2l (D), 2l+1 (Z)
@@ -197,7 +207,9 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
     if (ok && quarter * 32 < A.nlath) {
         const int j = quarter * 32 + lane;
         const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
-        const int L = A.L, nfo = 6 * L + 3, nf = 4 * L + 1;
+        // gridpointa writes gu gv gt gd gz gq gpj gpmt gp (6L+3 fields),
+        // gridpointd gu gv gt gq gp (4L+1)
+        const int L = A.L, nfo = A.dset ? 4 * L + 1 : 6 * L + 3, nf = A.dset ? 2 * L + 1 : 4 * L + 1;
         const bool has1 = Kq[1] > 0;
         const bool row_ok = j < A.nlath;
         const int latN = j, latS = A.nlat - 1 - j;
@@ -228,14 +240,15 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
                     int inst = inst0, f = f0;
                     if (group == 0) {
                         f += i >> 1;
-                        if (f >= nf) { f -= nf; inst++; }
+                        while (f >= nf) { f -= nf; inst++; }
                     } else {
                         inst += i >> 1;
                     }
                     const float2 vn = make_float2(d0r + d1r, d0i + d1i);
                     const float2 vs = make_float2(ss * (d0r - d1r), ss * (d0i - d1i));
                     int F;
-                    if (group == 1) F = 6 * L;                    // gpj
+                    if (A.dset) F = 2 * L + f;                    // st -> gt, sq -> gq, sp -> gp
+                    else if (group == 1) F = 6 * L;               // gpj
                     else if (f < L) F = 3 * L + f;                // sd -> gd
                     else if (f < 2 * L) F = f + L;                // st -> gt
                     else if (f < 4 * L) F = f + 2 * L;            // sz -> gz, sq -> gq
@@ -243,7 +256,7 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
                     float2 *wr = Wm + (size_t)(inst * nfo + F) * A.nlat;
                     wr[latN] = vn;
                     wr[latS] = vs;
-                    if (group == 0 && f == 4 * L) {               // gpmt = i*m*gp
+                    if (group == 0 && !A.dset && f == 4 * L) {    // gpmt = i*m*gp
                         const float fm = (float)m;
                         float2 *wt = Wm + (size_t)(inst * nfo + 6 * L + 1) * A.nlat;
                         wt[latN] = make_float2(-fm * vn.y, fm * vn.x);
@@ -311,8 +324,9 @@ struct TcFwdArgs {
     const float2 *W;        // [m][row], row = (inst*(9L+1) + field)*nlat + lat
     long long nrows;
     const float *filt;      // skgpsp
-    float *spout;           // [inst][4L+1][NRSP]
+    float *spout;           // [inst][4L+1][NRSP] (gridpointd: [inst][4L][NRSP])
     int L, nlat, nlath, njc, ntp1, nrsp;
+    int dset = 0;           // 0: gridpointa forward set, 1: gridpointd
 };
 
 struct TcFwdLaunch {
@@ -343,7 +357,23 @@ template <int NC> __device__ __forceinline__ void tmem_ld_nw(uint32_t taddr, uin
     else tc::tmem_ld16_nw(taddr, r);
 }
 
-__device__ __forceinline__ long long fwd_row(int L, int inst, int kind, int l) {
+// Fourier row of field kind `kind`, level l of an instance, or -1 for a kind
+// the set does not have.  gridpointa (9L+1 fields) has every kind; gridpointd
+// (4L fields gtdt, gudt, gvdt, gqdt, plasim.f90:3415-3428) feeds fc2sp of
+// gtdt and gqdt through the tn and qn columns and uv2dv(gudt, gvdt) through
+// the fu and fv columns: mktend's d and z with ke = 0 are uv2dv's
+// (legmod.f90:356-426, :555-602), its t with vt = ut = 0 and qtend's q with
+// vq = uq = 0 are fc2sp's.
+__device__ __forceinline__ long long fwd_row(int L, int inst, int kind, int l, int dset = 0) {
+    if (dset) {
+        int F;
+        if (kind == 0) F = l;               // tn <- gtdt
+        else if (kind == 5) F = L + l;      // fu <- gudt
+        else if (kind == 4) F = 2 * L + l;  // fv <- gvdt
+        else if (kind == 1) F = 3 * L + l;  // qn <- gqdt
+        else return -1;
+        return (long long)inst * (4 * L) + F;
+    }
     const int nfi = 9 * L + 1;
     int F;
     if (kind == 7) F = 7 * L;
@@ -364,7 +394,7 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
     const int Kq[2] = {kpar(K, 0), kpar(K, 1)};
     const int R[2] = {pad8(Kq[0]), pad8(Kq[1])};
     const int njc = A.njc, L = A.L, nlat = A.nlat;
-    const bool with_vpp = (l0 == 0);
+    const bool with_vpp = (l0 == 0) && !A.dset;
     const bool onebuf = P.onebuf != 0;
     // a table block is [parity 0: 3 splits x R0 rows][parity 1: 3 splits x R1 rows];
     // the halves travel separately, into two buffers so the next table's half 0
@@ -414,7 +444,7 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
                 if (t == 0 && q == nf * NLT) { if (with_vpp) rb = fwd_row(L, inst, 7, 0); }
                 else {
                     const int fi = q / NLT, li = q - fi * NLT;
-                    if (li < nl) rb = fwd_row(L, inst, c_fwd_fields[t][fi], l0 + li);
+                    if (li < nl) rb = fwd_row(L, inst, c_fwd_fields[t][fi], l0 + li, A.dset);
                 }
             }
             const int j0 = 8 * g;
@@ -606,7 +636,7 @@ __global__ void __launch_bounds__(TCT2) k_tc_forward(const __grid_constant__ TcF
             const int k = 2 * kk + p;  // n - m
             const float fl = A.filt[m + k];
             const size_t wo = 2 * (size_t)(A.woff[m] + k);
-            const int nfo = 4 * L + 1;
+            const int nfo = A.dset ? 4 * L : 4 * L + 1;
 #pragma unroll
             for (int li = 0; li < NLT; li++) {
                 if (li >= nl) break;
@@ -669,6 +699,7 @@ struct TcFwd3Args {
     const float *filt;
     float *spout;
     int L, nlat, nlath, njc, ntp1, nrsp;
+    int dset = 0;           // 0: gridpointa forward set, 1: gridpointd (no gvpp; 4L outputs)
 };
 struct TcFwd3Launch {
     TcFwd3Args seg[TC_MAXSEG];
@@ -715,9 +746,9 @@ __device__ __forceinline__ long long f3_row(const TcFwd3Args &A, int inst, int l
                                             int q) {
     const int nf = c_fwd_nf[t];
     if (q >= nf * NLT + ((t == 0) ? 1 : 0)) return -1;
-    if (t == 0 && q == nf * NLT) return with_vpp ? fwd_row(A.L, inst, 7, 0) : -1;
+    if (t == 0 && q == nf * NLT) return (with_vpp && !A.dset) ? fwd_row(A.L, inst, 7, 0) : -1;
     const int fi = q / NLT, li = q - fi * NLT;
-    return li < nl ? fwd_row(A.L, inst, c_fwd_fields[t][fi], l0 + li) : -1;
+    return li < nl ? fwd_row(A.L, inst, c_fwd_fields[t][fi], l0 + li, A.dset) : -1;
 }
 
 // Operand staging works on slots: a slot is one column pair q (a field level,
@@ -1086,7 +1117,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             if (!ok) break;
             if (r < Kq) {
                 const float *e = E + (size_t)r * NO;
-                const int L = A.L, nfo = 4 * L + 1, k = 2 * r + p;   // k = n - m
+                const int L = A.L, nfo = A.dset ? 4 * L : 4 * L + 1, k = 2 * r + p;   // k = n - m
                 const size_t wo = (size_t)wom + k;
 #pragma unroll
                 for (int li = 0; li < NLT; li++) {
@@ -1098,7 +1129,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
                                               (o[li][kk][1] + e[(li * 4 + kk) * 2 + 1]) * fl);
                     }
                 }
-                if (l0 == 0) {
+                if (l0 == 0 && !A.dset) {
                     float2 *dst = reinterpret_cast<float2 *>(A.spout + ((size_t)inst * nfo + 4 * L) * A.nrsp);
                     dst[wo] = make_float2((ov[0] + e[NLT * 8]) * fl, (ov[1] + e[NLT * 8 + 1]) * fl);
                 }

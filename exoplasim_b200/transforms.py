@@ -248,6 +248,45 @@ class Plan:
         call("exotx_forward_set_batch", self._h, p, _ptr(gpin), _ptr(out), nlev, ninst, _stream())
         return out
 
+    # ---------------------------------------------- gridpointd transform sets
+    def inverse_set_d_batch(self, spin, nlev, precision="mixed", out=None):
+        """gridpointd inverse half (invlegd + fc2gp, plasim.f90:3142-3149) for ninst
+        states: (ninst, 4L+1, NRSP) sd, st, sz, sq, sp -> (ninst, 4L+1, NLAT, NLON)
+        gu, gv, gt, gq, gp."""
+        p = _prec(precision)
+        dt = _dtype(p)
+        ninst = spin.shape[0]
+        _check(spin, dt, (ninst, 4 * nlev + 1, self.nrsp), "spin")
+        if out is None:
+            out = torch.zeros((ninst, 4 * nlev + 1, self.nlat, self.nlon), dtype=dt, device=spin.device)
+        _check(out, dt, (ninst, 4 * nlev + 1, self.nlat, self.nlon), "gpout")
+        call("exotx_inverse_set_d_batch", self._h, p, _ptr(spin), _ptr(out), nlev, ninst, _stream())
+        return out
+
+    def forward_set_d_batch(self, gpin, nlev, precision="mixed", out=None):
+        """gridpointd forward half (gp2fc, fc2sp, uv2dv, plasim.f90:3415-3428) for
+        ninst states: (ninst, 4L, NLAT, NLON) gtdt, gudt, gvdt, gqdt -> (ninst, 4L, NRSP)
+        sdf, stf, szf, sqf; gpin is not modified."""
+        p = _prec(precision)
+        dt = _dtype(p)
+        ninst = gpin.shape[0]
+        _check(gpin, dt, (ninst, 4 * nlev, self.nlat, self.nlon), "gpin")
+        if out is None:
+            out = torch.zeros((ninst, 4 * nlev, self.nrsp), dtype=dt, device=gpin.device)
+        _check(out, dt, (ninst, 4 * nlev, self.nrsp), "spout")
+        call("exotx_forward_set_d_batch", self._h, p, _ptr(gpin), _ptr(out), nlev, ninst, _stream())
+        return out
+
+    def inverse_set_d(self, spin, nlev, precision="fp64", out=None):
+        """inverse_set_d_batch of one state: (4L+1, NRSP) -> (4L+1, NLAT, NLON)."""
+        o = None if out is None else out.unsqueeze(0)
+        return self.inverse_set_d_batch(spin.unsqueeze(0), nlev, precision, o)[0]
+
+    def forward_set_d(self, gpin, nlev, precision="fp64", out=None):
+        """forward_set_d_batch of one state: (4L, NLAT, NLON) -> (4L, NRSP)."""
+        o = None if out is None else out.unsqueeze(0)
+        return self.forward_set_d_batch(gpin.unsqueeze(0), nlev, precision, o)[0]
+
     def sets_host(self, nlev, spin=None, gpout=None, gpin=None, spout=None, precision="mixed", host_fp64=False):
         """Both transform sets for states held in HOST tensors (page-locked for
         overlap): spin (ninst, 4L+1, NRSP) -> gpout (ninst, 6L+3, NLAT, NLON) and

@@ -126,6 +126,23 @@ exotx_status exotx_inverse_set_batch(exotx_plan p, int prec, const void *spin, v
                                      int nlev, int ninst, exotx_stream s);
 exotx_status exotx_forward_set_batch(exotx_plan p, int prec, const void *gpin, void *spout,
                                      int nlev, int ninst, exotx_stream s);
+/* ---- gridpointd transform sets (plasim.f90 gridpointd :3142-3149, :3415-3428) ----
+ * inverse_set_d: spin(2*NCSP, 4L+1) = sd[L], st[L], sz[L], sq[L], sp (as inverse_set)
+ *   -> gpout(NHOR, 4L+1) = gu[L], gv[L], gt[L], gq[L], gp
+ *   (invlegd, legmod.f90:661-677: dv2uv, sp2fc of st, sq and sp; fc2gp of every field)
+ * forward_set_d: gpin(NHOR, 4L) = gtdt[L], gudt[L], gvdt[L], gqdt[L]
+ *   -> spout(2*NCSP, 4L) = sdf[L], stf[L], szf[L], sqf[L]
+ *   (gp2fc of every field, fc2sp of gtdt and gqdt, uv2dv(gudt, gvdt)); gpin is not modified.
+ * EXOTX_MIXED runs the tensor-core kernels of the gridpointa sets with these
+ * field maps (uv2dv as mktend's d and z with no kinetic-energy term). */
+exotx_status exotx_inverse_set_d(exotx_plan p, int prec, const void *spin, void *gpout,
+                                 int nlev, exotx_stream s);
+exotx_status exotx_forward_set_d(exotx_plan p, int prec, const void *gpin, void *spout,
+                                 int nlev, exotx_stream s);
+exotx_status exotx_inverse_set_d_batch(exotx_plan p, int prec, const void *spin, void *gpout,
+                                       int nlev, int ninst, exotx_stream s);
+exotx_status exotx_forward_set_d_batch(exotx_plan p, int prec, const void *gpin, void *spout,
+                                       int nlev, int ninst, exotx_stream s);
 /* Both sets for ninst states whose arrays are in HOST memory, laid out as for
  * the _batch calls (h_spin -> h_gpout by the inverse set, h_gpin -> h_spout by
  * the forward set; pass both pointers of a half as NULL to skip it).  The

@@ -130,6 +130,9 @@ int  oracle_num_threads(void);
 void oracle_inverse_set(const oracle_leg *L, int nlev, const double *spin, double *gpout,
                         double plavor, int use991);
 void oracle_forward_set(const oracle_leg *L, int nlev, double *gpin, double *spout, int use991);
+void oracle_inverse_set_d(const oracle_leg *L, int nlev, const double *spin, double *gpout,
+                          double plavor, int use991);
+void oracle_forward_set_d(const oracle_leg *L, int nlev, double *gpin, double *spout, int use991);
 void oracle_radstep_par(const oracle_radpar *p, oracle_radio *io);
 
 #ifdef __cplusplus

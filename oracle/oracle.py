@@ -95,6 +95,8 @@ def _declare(L):
     L.oracle_num_threads.restype = C.c_int
     L.oracle_inverse_set.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_double, C.c_int]
     L.oracle_forward_set.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_int]
+    L.oracle_inverse_set_d.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_double, C.c_int]
+    L.oracle_forward_set_d.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_int]
 
 
 def _ptr(a):
@@ -184,6 +186,20 @@ class Leg:
         lib().oracle_inverse_set(C.byref(self.t), nlev, _ptr(np.ascontiguousarray(spin)), _ptr(gpout),
                                  plavor, int(use991))
         return gpout
+
+    def inverse_set_d(self, spin, nlev, plavor, use991=False):
+        """gridpointd inverse half: (4L+1, NRSP) -> (4L+1, NHOR) gu, gv, gt, gq, gp."""
+        gpout = np.zeros(((4 * nlev + 1), self.nlat * self.nlon))
+        lib().oracle_inverse_set_d(C.byref(self.t), nlev, _ptr(np.ascontiguousarray(spin)), _ptr(gpout),
+                                   plavor, int(use991))
+        return gpout
+
+    def forward_set_d(self, gpin, nlev, use991=False):
+        """gridpointd forward half: (4L, NHOR) gtdt, gudt, gvdt, gqdt -> (4L, NRSP) sdf, stf, szf, sqf."""
+        work = np.array(gpin, dtype=np.float64, order="C", copy=True).reshape(4 * nlev, -1)
+        spout = np.zeros((4 * nlev, self.nrsp))
+        lib().oracle_forward_set_d(C.byref(self.t), nlev, _ptr(work), _ptr(spout), int(use991))
+        return spout
 
     def forward_set(self, gpin, nlev, use991=False):
         work = np.array(gpin, dtype=np.float64, order="C", copy=True)

@@ -86,6 +86,61 @@ void oracle_forward_set(const oracle_leg *L, int nlev, double *gpin, double *spo
     }
 }
 
+/* inverse half of gridpointd: invlegd (legmod.f90:661-677) and the fc2gp
+ * calls (plasim.f90:3142-3149).  spin as above;
+ * gpout [4L+1][NLAT*NLON] gu[L], gv[L], gt[L], gq[L], gp */
+void oracle_inverse_set_d(const oracle_leg *L, int nlev, const double *spin, double *gpout,
+                          double plavor, int use991) {
+    int nlat = L->nlat, nlon = L->nlon, nrsp = 2 * L->ncsp;
+    size_t nhor = (size_t)nlat * nlon;
+    const double *sd = spin, *st = spin + (size_t)nlev * nrsp, *sz = spin + (size_t)2 * nlev * nrsp,
+                 *sq = spin + (size_t)3 * nlev * nrsp, *sp = spin + (size_t)4 * nlev * nrsp;
+    double *gu = gpout, *gv = gpout + nlev * nhor, *gt = gpout + 2 * nlev * nhor, *gq = gpout + 3 * nlev * nhor,
+           *gp = gpout + 4 * nlev * nhor;
+#pragma omp parallel for schedule(dynamic)
+    for (int v = 0; v < nlev; v++) {
+        double *pz = malloc(sizeof(double) * nrsp);
+        memcpy(pz, sz + (size_t)v * nrsp, sizeof(double) * nrsp);
+        oracle_dv2uv(L, sd + (size_t)v * nrsp, pz, gu + v * nhor, gv + v * nhor, 1, plavor);
+        free(pz);
+        oracle_sp2fc(L, sq + (size_t)v * nrsp, gq + v * nhor);
+        oracle_sp2fc(L, st + (size_t)v * nrsp, gt + v * nhor);
+    }
+    oracle_sp2fc(L, sp, gp);
+    int nrows = (int)((4 * nlev + 1) * (size_t)nlat);
+    int chunk = nlat;
+#pragma omp parallel for schedule(dynamic)
+    for (int r = 0; r < nrows; r += chunk) {
+        if (use991) oracle_fc2gp_991(gpout + (size_t)r * nlon, nlon, chunk);
+        else oracle_fc2gp(gpout + (size_t)r * nlon, nlon, chunk);
+    }
+}
+
+/* forward half of gridpointd: the gp2fc calls (plasim.f90:3415-3418), fc2sp
+ * of the temperature and humidity tendencies and uv2dv (:3423-3428); gpin
+ * [4L][NLAT*NLON] gtdt[L], gudt[L], gvdt[L], gqdt[L] is transformed in place;
+ * spout [4L][2*NCSP] sdf[L], stf[L], szf[L], sqf[L] */
+void oracle_forward_set_d(const oracle_leg *L, int nlev, double *gpin, double *spout, int use991) {
+    int nlat = L->nlat, nlon = L->nlon, nrsp = 2 * L->ncsp;
+    size_t nhor = (size_t)nlat * nlon;
+    int nrows = (int)((4 * nlev) * (size_t)nlat);
+    int chunk = nlat;
+#pragma omp parallel for schedule(dynamic)
+    for (int r = 0; r < nrows; r += chunk) {
+        if (use991) oracle_gp2fc_991(gpin + (size_t)r * nlon, nlon, chunk);
+        else oracle_gp2fc(gpin + (size_t)r * nlon, nlon, chunk);
+    }
+    double *gtdt = gpin, *gudt = gpin + nlev * nhor, *gvdt = gpin + 2 * nlev * nhor, *gqdt = gpin + 3 * nlev * nhor;
+    double *sdf = spout, *stf = spout + (size_t)nlev * nrsp, *szf = spout + (size_t)2 * nlev * nrsp,
+           *sqf = spout + (size_t)3 * nlev * nrsp;
+#pragma omp parallel for schedule(dynamic)
+    for (int v = 0; v < nlev; v++) {
+        oracle_fc2sp(L, gtdt + v * nhor, stf + (size_t)v * nrsp, 1);
+        oracle_fc2sp(L, gqdt + v * nhor, sqf + (size_t)v * nrsp, 1);
+        oracle_uv2dv(L, gudt + v * nhor, gvdt + v * nhor, sdf + (size_t)v * nrsp, szf + (size_t)v * nrsp, 1, 1);
+    }
+}
+
 /* radstep over all columns in blocks of whole latitude rows */
 void oracle_radstep_par(const oracle_radpar *p, oracle_radio *io) {
     int nlat = p->nhor / p->nlon;
