@@ -302,6 +302,28 @@ def run_ours(a, rank, world, local_rank):
     clk = clocks.stop()
     primary = precisions[0]
 
+    # a whole dynamics timestep's transforms: the gridpointa round trip above
+    # plus the gridpointd one (invlegd + fc2gp, then gp2fc + fc2sp + uv2dv,
+    # plasim.f90:3142-3149, :3415-3428), same states, same precision
+    timestep = None
+    if primary != "fp64":
+        sd_in = spin64.float().unsqueeze(0).repeat(B, 1, 1).contiguous()
+        gd_in = gin64[:4 * NLEV].float().unsqueeze(0).repeat(B, 1, 1, 1).contiguous()
+        gd_out = torch.zeros((B, 4 * NLEV + 1, NLAT, 2 * NLAT), device=dev)
+        sd_out = torch.zeros((B, 4 * NLEV, plan.nrsp), device=dev)
+        ba = make(torch.float32)
+
+        def full_step():
+            step_fn(primary, ba)()
+            plan.inverse_set_d_batch(sd_in, NLEV, primary, out=gd_out)
+            plan.forward_set_d_batch(gd_in, NLEV, primary, out=sd_out)
+        ms_t, nl_t, st_t = time_graph(full_step, a.steps, a.warmup, with_steps=True)
+        med_t = max_over_ranks(statistics.median(st_t))
+        timestep = {"sets": "gridpointa + gridpointd round trips", "precision": primary,
+                    "ms_per_step": med_t, "timesteps_per_s": world * B / (med_t / 1000.0),
+                    "launches_per_step": nl_t}
+        del ba, sd_in, gd_in, gd_out, sd_out
+
     # per-stage timing of the primary precision
     bufs = make(torch.float32) if primary != "fp64" else make(torch.float64)
     inv_ms, _ = time_graph(lambda: plan.inverse_set_batch(bufs[0], NLEV, primary, out=bufs[2]), a.steps, a.warmup)
@@ -509,6 +531,7 @@ def run_ours(a, rank, world, local_rank):
         "roofline": roof,
         "kernels": kernels,
         "stages_ms_per_instance": {"inverse_set": inv_ms / (a.steps * B), "forward_set": fwd_ms / (a.steps * B)},
+        "full_timestep": timestep,
         "e2e": e2e,
         "e2e_fp64_host": e2e64,
         "radiation": {"metric": "radiation cols/s (T42 grid, 8192 columns, L20, plain radmod kernel)", **rad},

@@ -123,9 +123,9 @@ def test_fortran_legendre_and_fft(oracle, real_bytes, prec):
         assert relerr(got, ref) < tol
     # FFTs in place on lot rows of length n
     rows = _fields(nlat, 1, 8)[0]
-    a = h(rows)
-    lib.gp2fc_(_p(a), _ip(2 * nlat), _ip(nlat))
     ref = oracle.gp2fc(rows)
+    a = np.array(rows, dtype=hdt)   # a copy: the routine works in place
+    lib.gp2fc_(_p(a), _ip(2 * nlat), _ip(nlat))
     assert relerr(a, ref) < (1e-13 if prec == FP64 else 2e-6)
     lib.fc2gp_(_p(a), _ip(2 * nlat), _ip(nlat))
     assert relerr(a, oracle.fc2gp(ref)) < (1e-13 if prec == FP64 else 2e-6)

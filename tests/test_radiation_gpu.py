@@ -110,9 +110,12 @@ SOLANG = {
 def test_radstep_solang_fp64(oracle, case):
     got, ref = _run(oracle, 32, 10, "fp64", seed=11, **SOLANG[case])
     if SOLANG[case]["nsol"] == 1:
-        # the on-GPU cos zenith itself, then everything downstream of it
+        # the on-GPU cos zenith itself, then everything downstream of it; a
+        # constant solar angle (ncstsol) lights every column alike
         assert np.max(np.abs(got["gmu0"] - ref["gmu0"])) < 1e-14
-        assert (got["gmu0"] > 0).any() and (got["gmu0"] == 0).any()
+        assert (got["gmu0"] > 0).any()
+        if not SOLANG[case].get("ncstsol"):
+            assert (got["gmu0"] == 0).any()
     for k in FLUXES + RATES + ("dqo3", "dalb", "dsalb"):
         assert relerr(got[k], ref[k]) < 1e-11, (case, k)
 
