@@ -86,6 +86,11 @@ SIGNATURES = {
     "exotx_inverse_set_d_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_forward_set_d_batch": [_P, _I, _P, _P, _I, _I, _S],
     "exotx_raw_size": [_P, _I, C.POINTER(C.c_size_t)],
+    "exotx_gp_params_default": [_I, _P],
+    "exotx_gp_params_derive": [_P],
+    "exotx_gpconst_create": [_P, C.POINTER(C.c_void_p)],
+    "exotx_gpconst_destroy": [_P],
+    "exotx_gridpoint": [_P, _P, _I, _P, _P, _P, _P, _I, _S],
     "exotx_raw_pack": [_P, _I, _P, _S],
     "exotx_sets_host": [_P, _I, _P, _P, _P, _P, _I, _I, _S],
     "exotx_sets_host_f64": [_P, _I, _P, _P, _P, _P, _I, _I, _S],

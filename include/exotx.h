@@ -260,6 +260,38 @@ exotx_status exotx_kernel_time(int kernel, double *ms, long long *launches);
  * then reset. */
 exotx_status exotx_tc_error(int *code, exotx_stream s);
 
+/* ---- grid-point step of gridpointa (plasim.f90:2441-2455) ----
+ * Between the inverse and the forward set: gp = exp(gp), calcgp (:2587-2755:
+ * sigma-dot, adiabatic and vertical-advection tendencies, vorticity and
+ * divergence flux terms, non-linear geopotential) and the flux products
+ * gut = gu gt, gvt = gv gt, gke = gu^2 + gv^2 + gphi, guq = gu gq, gvq = gv gq.
+ * The constants are those calcgp reads from pumamod: levels, the reference
+ * profile t0 (dimensionless, T0/ct), the semi-implicit matrices of initsi
+ * (:1709-1745; g and c column-major, g[i + nlev*j] = g(i+1,j+1)), rdsig
+ * (:1564) and the scalings of :1316-1322. */
+typedef struct {
+    int nlev, nqspec;
+    double akap, rdbrv, adv, psurf, ww;
+    double dsigma[64], sigmah[64], rdsig[64], t0[64], t01s2[64], tkp[64];
+    double g[64 * 64], c[64 * 64];
+} exotx_gp_params;
+/* Earth defaults for nlev levels (default sigma levels, a 288 K / 6.5 K/km
+ * reference profile) with the derived arrays filled */
+exotx_status exotx_gp_params_default(int nlev, exotx_gp_params *p);
+/* recompute tkp, t01s2, g, c, rdsig from sigmah, dsigma, t0, akap (initsi) */
+exotx_status exotx_gp_params_derive(exotx_gp_params *p);
+typedef struct exotx_gpconst_s *exotx_gpconst;   /* the constants on the device */
+exotx_status exotx_gpconst_create(const exotx_gp_params *p, exotx_gpconst *out);
+exotx_status exotx_gpconst_destroy(exotx_gpconst c);
+/* ninst states back to back: gin (ninst x (6L+3) x NHOR, the inverse set's
+ * output, gp = ln ps) -> gout (ninst x (9L+1) x NHOR, the forward set's
+ * input).  dw (ninst x L x NHOR, may be NULL) receives calcgp's vertical
+ * velocity diagnostic.  dq (ninst x L x NHOR) is the grid humidity, read only
+ * when nqspec = 0.  FP64 or FP32 (EXOTX_MIXED: FP32) arrays; NHOR and the
+ * latitudes come from the plan. */
+exotx_status exotx_gridpoint(exotx_plan p, exotx_gpconst c, int prec, const void *gin, void *gout,
+                             void *dw, const void *dq, int ninst, exotx_stream s);
+
 /* ---- radiation column pass (radmod.f90 radstep :927-1110) ---- */
 typedef struct {
     int nlev, nhor, nlon;                 /* nlon: longitudes per latitude row */

@@ -125,6 +125,18 @@ void oracle_mko3_range(const oracle_radpar *p, const double *sid, const double *
                        const double *dp, double *dqo3, int j0, int j1);
 void oracle_radstep_range(const oracle_radpar *p, oracle_radio *io, int j0, int j1);
 
+/* ---------------- grid-point step of gridpointa (exo_oracle_gp.c) ---------------- */
+typedef struct {
+    int nlev, nhor, nlon, nqspec;
+    const double *dsigma, *sigmah, *rdsig, *t0, *t01s2, *tkp;  /* [nlev] */
+    const double *g, *c;                                       /* [nlev*nlev], column major */
+    double akap, rdbrv, adv, psurf, ww;
+    const double *dq;                                          /* [nlev][nhor] when nqspec == 0 */
+} oracle_gppar;
+void oracle_initsi(int nlev, const double *sigmah, const double *dsigma, const double *t0, double akap,
+                   double *g, double *c, double *tkp, double *t01s2, double *rdsig);
+void oracle_gridpoint(const oracle_gppar *P, const double *gin, double *gout, double *dw, const double *rcsq);
+
 /* ---------------- OpenMP drivers (timed CPU baseline) ---------------- */
 int  oracle_num_threads(void);
 void oracle_inverse_set(const oracle_leg *L, int nlev, const double *spin, double *gpout,

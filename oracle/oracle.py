@@ -95,6 +95,8 @@ def _declare(L):
     L.oracle_num_threads.restype = C.c_int
     L.oracle_inverse_set.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_double, C.c_int]
     L.oracle_forward_set.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_int]
+    L.oracle_gridpoint.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+    L.oracle_initsi.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp, _dp]
     L.oracle_inverse_set_d.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_double, C.c_int]
     L.oracle_forward_set_d.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_int]
 
@@ -291,3 +293,43 @@ def radstep(p, sid, cola, cols, parallel=False):
         setattr(io, k, _ptr(v))
     (lib().oracle_radstep_par if parallel else lib().oracle_radstep)(C.byref(p), C.byref(io))
     return arr
+
+
+class GpPar(C.Structure):
+    _fields_ = [("nlev", C.c_int), ("nhor", C.c_int), ("nlon", C.c_int), ("nqspec", C.c_int)] + \
+               [(n, _dp) for n in ("dsigma", "sigmah", "rdsig", "t0", "t01s2", "tkp", "g", "c")] + \
+               [(n, C.c_double) for n in ("akap", "rdbrv", "adv", "psurf", "ww")] + [("dq", _dp)]
+
+
+def initsi(sigmah, dsigma, t0, akap):
+    """g, c (nlev x nlev, [i, j] = g(i+1, j+1)), tkp, t01s2, rdsig (plasim.f90:1709-1745, :1564)."""
+    L = len(sigmah)
+    g, c = np.zeros(L * L), np.zeros(L * L)
+    tkp, t01s2, rdsig = np.zeros(L), np.zeros(L), np.zeros(L)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (sigmah, dsigma, t0)]
+    lib().oracle_initsi(L, *[_ptr(x) for x in a], akap, _ptr(g), _ptr(c), _ptr(tkp), _ptr(t01s2), _ptr(rdsig))
+    return g.reshape(L, L, order="F"), c.reshape(L, L, order="F"), tkp, t01s2, rdsig
+
+
+def gridpoint(gin, nlev, nlon, sigmah, dsigma, t0, akap, rdbrv, adv, psurf, ww, rcsq, nqspec=1, dq=None):
+    """The grid-point step of gridpointa (plasim.f90:2441-2455) on gin
+    ((6L+3, nhor): gu gv gt gd gz gq gpj gpmt gp); returns (gout (9L+1, nhor), dw (L, nhor))."""
+    L = nlev
+    gin = np.ascontiguousarray(gin, dtype=np.float64).reshape(6 * L + 3, -1)
+    nhor = gin.shape[1]
+    g, c, tkp, t01s2, rdsig = initsi(sigmah, dsigma, t0, akap)
+    keep = [np.ascontiguousarray(x, dtype=np.float64) for x in (dsigma, sigmah, rdsig, t0, t01s2, tkp)]
+    gF, cF = np.ascontiguousarray(g.ravel(order="F")), np.ascontiguousarray(c.ravel(order="F"))
+    p = GpPar()
+    p.nlev, p.nhor, p.nlon, p.nqspec = L, nhor, nlon, nqspec
+    for name, arr in zip(("dsigma", "sigmah", "rdsig", "t0", "t01s2", "tkp"), keep):
+        setattr(p, name, _ptr(arr))
+    p.g, p.c = _ptr(gF), _ptr(cF)
+    p.akap, p.rdbrv, p.adv, p.psurf, p.ww = akap, rdbrv, adv, psurf, ww
+    dqa = None if dq is None else np.ascontiguousarray(dq, dtype=np.float64)
+    p.dq = _ptr(dqa) if dqa is not None else None
+    gout = np.zeros((9 * L + 1, nhor))
+    dw = np.zeros((L, nhor))
+    rc = np.ascontiguousarray(rcsq, dtype=np.float64)
+    lib().oracle_gridpoint(C.byref(p), _ptr(gin), _ptr(gout), _ptr(dw), _ptr(rc))
+    return gout, dw
