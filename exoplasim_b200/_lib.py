@@ -91,6 +91,11 @@ SIGNATURES = {
     "exotx_gpconst_create": [_P, C.POINTER(C.c_void_p)],
     "exotx_gpconst_destroy": [_P],
     "exotx_gridpoint": [_P, _P, _I, _P, _P, _P, _P, _I, _S],
+    "exotx_spec_params_default": [_I, _P],
+    "exotx_specconst_create": [_P, _P, C.POINTER(C.c_void_p)],
+    "exotx_specconst_destroy": [_P],
+    "exotx_spectrala": [_P, _I, _P, _S],
+    "exotx_spectrald": [_P, _I, _P, _S],
     "exotx_raw_pack": [_P, _I, _P, _S],
     "exotx_sets_host": [_P, _I, _P, _P, _P, _P, _I, _I, _S],
     "exotx_sets_host_f64": [_P, _I, _P, _P, _P, _P, _I, _I, _S],

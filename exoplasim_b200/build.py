@@ -23,7 +23,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
 # per-file extra flags: the plan builder keeps every FP64 product and sum
 # separately rounded, in the reference's evaluation order
-EXTRA = {"plan.cu": ["-fmad=false"], "radiation_fp64.cu": ["-fmad=false"], "rawout.cu": ["-fmad=false"], "gridpoint_fp64.cu": ["-fmad=false"]}
+EXTRA = {"plan.cu": ["-fmad=false"], "radiation_fp64.cu": ["-fmad=false"], "rawout.cu": ["-fmad=false"], "gridpoint_fp64.cu": ["-fmad=false"], "spectral_fp64.cu": ["-fmad=false"]}
 
 
 def nvcc():

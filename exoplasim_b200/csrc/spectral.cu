@@ -1,0 +1,246 @@
+// Semi-implicit spectral time step on the device (plasim.f90 spectrala
+// :2757-2918 and spectrald :3645-3999, one model state, without their
+// diagnostic branches): host set-up of the level matrices (initsi
+// :1709-1760, makebm :1683-1704) and the diffusion coefficients (:1617-1633),
+// and the launchers.  The kernels are in spectral_kernel.cuh.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "spectral_kernel.cuh"
+
+struct exotx_specconst_s {
+    exotx_spec_params h;
+    int ntru = 0, nrsp = 0;
+    double *d = nullptr;    // constants block (see SpecArgs::k)
+    double *sak = nullptr;  // [L][NRSP]
+    int *nidx = nullptr;    // [NRSP]
+};
+
+namespace exotx {
+exotx_status launch_spectral_fp64(const SpecArgs<double> &A, bool d_part, cudaStream_t s);
+
+static int spec_threads(int L, size_t esz) {
+    int t = 128;
+    while (t > 32 && 4 * (size_t)L * t * esz > 160 * 1024) t -= 32;
+    return t;
+}
+
+static exotx_status launch_spectral_fp32(const SpecArgs<float> &A, bool d_part, cudaStream_t s) {
+    if (d_part) {
+        k_spectrald<float><<<(A.nrsp + 127) / 128, 128, 0, s>>>(A);
+    } else {
+        const int nt = spec_threads(A.L, 4);
+        const size_t smem = 4 * (size_t)A.L * nt * sizeof(float);
+        if (smem > 48 * 1024)
+            EXOTX_CUDA(cudaFuncSetAttribute(k_spectrala<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_spectrala<float><<<(A.nrsp + nt - 1) / nt, nt, smem, s>>>(A);
+    }
+    EXOTX_CHECK_LAUNCH();
+    return EXOTX_OK;
+}
+}  // namespace exotx
+
+using namespace exotx;
+
+// the inverse of a small matrix (column major), Gauss-Jordan with partial pivoting
+static bool invert(std::vector<double> &a, int n) {
+    std::vector<double> inv((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) inv[i + (size_t)n * i] = 1.0;
+    for (int c = 0; c < n; c++) {
+        int piv = c;
+        for (int r = c + 1; r < n; r++)
+            if (fabs(a[r + (size_t)n * c]) > fabs(a[piv + (size_t)n * c])) piv = r;
+        if (a[piv + (size_t)n * c] == 0.0) return false;
+        if (piv != c)
+            for (int k = 0; k < n; k++) {
+                std::swap(a[c + (size_t)n * k], a[piv + (size_t)n * k]);
+                std::swap(inv[c + (size_t)n * k], inv[piv + (size_t)n * k]);
+            }
+        const double d = a[c + (size_t)n * c];
+        for (int k = 0; k < n; k++) { a[c + (size_t)n * k] /= d; inv[c + (size_t)n * k] /= d; }
+        for (int r = 0; r < n; r++) {
+            if (r == c) continue;
+            const double f = a[r + (size_t)n * c];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; k++) {
+                a[r + (size_t)n * k] -= f * a[c + (size_t)n * k];
+                inv[r + (size_t)n * k] -= f * inv[c + (size_t)n * k];
+            }
+        }
+    }
+    a.swap(inv);
+    return true;
+}
+
+EXOTX_API exotx_status exotx_spec_params_default(int nlev, exotx_spec_params *p) {
+    if (!p || nlev < 2 || nlev > 64) return EXOTX_BAD_ARG;
+    memset(p, 0, sizeof(*p));
+    p->nlev = nlev;
+    p->nqspec = 1;
+    p->nhdiff = 15;                                      // plasimmod.f90:199
+    const double twopi = 2.0 * 3.14159265359, day = 86400.0, gascon = 287.0, plarad = 6371220.0,
+                 sidereal_day = 86164.0;
+    p->delt = twopi / 32.0;                              // 32 steps per rotation (plasim.f90:588)
+    p->delt2 = p->delt + p->delt;
+    p->pnu = 0.1;
+    p->pnu21 = 1.0 - 2.0 * p->pnu;
+    p->plavor = 1.63299310207;                           // EZ (plasimmod.f90:227)
+    p->akap = 0.286;
+    const double ww = twopi / sidereal_day, cv = plarad * ww, ct = cv * cv / gascon;
+    for (int j = 0; j < nlev; j++) {
+        const double z = (double)(j + 1) / nlev;
+        p->sigmah[j] = 0.75 * z + 1.75 * z * z * z - 1.5 * z * z * z * z;   // plasim.f90:1554-1564
+    }
+    p->dsigma[0] = p->sigmah[0];
+    for (int j = 1; j < nlev; j++) p->dsigma[j] = p->sigmah[j] - p->sigmah[j - 1];
+    for (int j = 0; j < nlev; j++) {
+        const double sig = j == 0 ? 0.5 * p->sigmah[0] : 0.5 * (p->sigmah[j - 1] + p->sigmah[j]);
+        const double t = 288.0 * pow(sig, 0.0065 * gascon / 9.80665);
+        p->t0[j] = (t < 216.65 ? 216.65 : t) / ct;
+        // rates in units of 1/(time unit 1/ww): day / (2 pi timescale) (plasim.f90:1583-1615)
+        p->tdissq[j] = day / (twopi * 0.1 * day);
+        p->tdisst[j] = day / (twopi * 0.76 * day);
+        p->tdissz[j] = day / (twopi * 0.3 * day);
+        p->tdissd[j] = day / (twopi * 0.06 * day);
+        p->ndel[j] = 2;
+    }
+    p->tfrc[0] = day / (twopi * 20.0 * day);
+    p->tfrc[1] = day / (twopi * 100.0 * day);
+    return EXOTX_OK;
+}
+
+EXOTX_API exotx_status exotx_specconst_create(exotx_plan pl, const exotx_spec_params *p, exotx_specconst *out) {
+    if (!pl || !p || !out || p->nlev < 2 || p->nlev > 64) return EXOTX_BAD_ARG;
+    const int L = p->nlev, ntru = pl->ntru, nrsp = 2 * pl->ncsp;
+    if (p->nhdiff < 0 || p->nhdiff >= ntru) return EXOTX_BAD_ARG;
+    // initsi (plasim.f90:1709-1760): g, c, tkp, t01s2, tau; rdsig (:1564)
+    std::vector<double> g((size_t)L * L, 0.0), c((size_t)L * L), tau((size_t)L * L), zalp(L, 0.0), tkp(L),
+        t01s2(L), rdsig(L);
+    for (int j = 0; j < L; j++) tkp[j] = p->akap * p->t0[j];
+    for (int j = 0; j < L - 1; j++) t01s2[j] = p->t0[j + 1] - p->t0[j];
+    t01s2[L - 1] = 0.0;
+    for (int j = 1; j < L; j++) zalp[j] = log(p->sigmah[j]) - log(p->sigmah[j - 1]);
+    g[0] = 1.0;
+    for (int jl = 1; jl < L; jl++) {
+        g[jl + (size_t)L * jl] = 1.0 - zalp[jl] * p->sigmah[jl - 1] / p->dsigma[jl];
+        for (int k = 0; k < jl; k++) g[jl + (size_t)L * k] = zalp[jl];
+    }
+    for (int jl = 0; jl < L; jl++)
+        for (int k = 0; k < L; k++) c[jl + (size_t)L * k] = g[k + (size_t)L * jl] * (p->dsigma[jl] / p->dsigma[k]);
+    for (int j = 0; j < L; j++) rdsig[j] = 0.5 / p->dsigma[j];
+    {
+        double zt01s2 = t01s2[0], zsig = p->sigmah[0];
+        tau[0] = 0.5 * zt01s2 * (zsig - 1.0) + tkp[0];
+        for (int j = 1; j < L; j++) tau[j] = 0.5 * zt01s2 * p->dsigma[j];
+        for (int jl = 1; jl < L; jl++) {
+            const double zttm = zt01s2, zsigm = zsig;
+            zt01s2 = t01s2[jl];
+            zsig = p->sigmah[jl];
+            for (int j2 = 0; j2 < L; j2++) {
+                const double ztm = j2 <= jl ? 1. : 0., ztmm = j2 < jl ? 1. : 0.;
+                double z = zttm * (zsigm - ztmm);
+                if (jl < L - 1) z = z + zt01s2 * (zsig - ztm);
+                z = z * rdsig[jl] * p->dsigma[j2];
+                if (j2 <= jl) z = z + tkp[jl] * c[j2 + (size_t)L * jl];
+                tau[j2 + (size_t)L * jl] = z;
+            }
+        }
+    }
+    // makebm (plasim.f90:1683-1704): bm1(n) = (delt^2 (t0 dsigma^T + g^T tau^T) + I/(n(n+1)))^-1
+    std::vector<double> base((size_t)L * L), bm1((size_t)(ntru + 1) * L * L, 0.0);
+    const double zdeltsq = p->delt * p->delt;
+    for (int j1 = 0; j1 < L; j1++)
+        for (int j2 = 0; j2 < L; j2++) {
+            double dot = 0.0;
+            for (int i = 0; i < L; i++) dot += g[i + (size_t)L * j1] * tau[j2 + (size_t)L * i];
+            base[j2 + (size_t)L * j1] = zdeltsq * (p->t0[j1] * p->dsigma[j2] + dot);
+        }
+    for (int jn = 1; jn <= ntru; jn++) {
+        std::vector<double> b = base;
+        for (int j = 0; j < L; j++) b[j + (size_t)L * j] += 1.0 / (jn * (jn + 1));
+        if (!invert(b, L)) return EXOTX_BAD_ARG;
+        memcpy(bm1.data() + (size_t)jn * L * L, b.data(), sizeof(double) * L * L);
+    }
+    // diffusion coefficients sak (plasim.f90:1617-1633) and the n of every real
+    std::vector<double> sak((size_t)L * nrsp);
+    std::vector<int> nidx(nrsp);
+    for (int jl = 0; jl < L; jl++) {
+        const int jdel = p->ndel[jl];
+        const double zakk = 1. / pow((double)(ntru - p->nhdiff), jdel);
+        int jr = 0;
+        for (int jm = 0; jm <= ntru; jm++)
+            for (int jn = jm; jn <= ntru; jn++) {
+                const double v = jn >= p->nhdiff ? zakk * pow((double)(jn - p->nhdiff), jdel) : 0.;
+                sak[(size_t)jl * nrsp + jr] = v;
+                sak[(size_t)jl * nrsp + jr + 1] = v;
+                nidx[jr] = nidx[jr + 1] = jn;
+                jr += 2;
+            }
+    }
+    std::vector<double> k((size_t)8 * L + 2 * (size_t)L * L + bm1.size());
+    for (int j = 0; j < L; j++) {
+        k[j] = p->t0[j]; k[L + j] = p->dsigma[j]; k[2 * L + j] = p->damp[j]; k[3 * L + j] = p->tdisst[j];
+        k[4 * L + j] = p->tdissq[j]; k[5 * L + j] = p->tdissd[j]; k[6 * L + j] = p->tdissz[j];
+        k[7 * L + j] = p->tfrc[j];
+    }
+    memcpy(k.data() + 8 * L, g.data(), sizeof(double) * L * L);
+    memcpy(k.data() + 8 * L + L * L, tau.data(), sizeof(double) * L * L);
+    memcpy(k.data() + 8 * L + 2 * L * L, bm1.data(), sizeof(double) * bm1.size());
+    exotx_specconst sc = new exotx_specconst_s();
+    sc->h = *p;
+    sc->ntru = ntru;
+    sc->nrsp = nrsp;
+    bool ok = cudaMalloc(&sc->d, sizeof(double) * k.size()) == cudaSuccess &&
+              cudaMalloc(&sc->sak, sizeof(double) * sak.size()) == cudaSuccess &&
+              cudaMalloc(&sc->nidx, sizeof(int) * nidx.size()) == cudaSuccess &&
+              cudaMemcpy(sc->d, k.data(), sizeof(double) * k.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(sc->sak, sak.data(), sizeof(double) * sak.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(sc->nidx, nidx.data(), sizeof(int) * nidx.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+        cudaFree(sc->d); cudaFree(sc->sak); cudaFree(sc->nidx);
+        delete sc;
+        return EXOTX_NO_MEM;
+    }
+    *out = sc;
+    return EXOTX_OK;
+}
+
+EXOTX_API exotx_status exotx_specconst_destroy(exotx_specconst c) {
+    if (!c) return EXOTX_BAD_ARG;
+    cudaFree(c->d); cudaFree(c->sak); cudaFree(c->nidx);
+    delete c;
+    return EXOTX_OK;
+}
+
+template <typename T>
+static SpecArgs<T> spec_args(exotx_specconst c, const exotx_spec_state *s) {
+    SpecArgs<T> A;
+    A.sdp = (T *)s->sdp; A.szp = (T *)s->szp; A.stp = (T *)s->stp; A.sqp = (T *)s->sqp; A.spp = (T *)s->spp;
+    A.sdm = (T *)s->sdm; A.szm = (T *)s->szm; A.stm = (T *)s->stm; A.sqm = (T *)s->sqm; A.spm = (T *)s->spm;
+    A.sdt = (T *)s->sdt; A.szt = (T *)s->szt; A.stt = (T *)s->stt; A.sqt = (T *)s->sqt; A.spt = (T *)s->spt;
+    A.sop = (const T *)s->sop; A.srp = (const T *)s->srp;
+    A.k = c->d; A.sak = c->sak; A.nidx = c->nidx;
+    A.L = c->h.nlev; A.nrsp = c->nrsp; A.ntru = c->ntru; A.nqspec = c->h.nqspec; A.nsponge = c->h.nsponge;
+    A.delt = c->h.delt; A.delt2 = c->h.delt2; A.pnu = c->h.pnu; A.pnu21 = c->h.pnu21; A.plavor = c->h.plavor;
+    A.dampsp = c->h.dampsp;
+    return A;
+}
+
+static exotx_status spec_run(exotx_specconst c, int prec, const exotx_spec_state *s, bool d_part, exotx_stream st) {
+    if (!c || !s || (prec != EXOTX_FP64 && prec != EXOTX_FP32)) return EXOTX_BAD_ARG;
+    const void *need[] = {s->sdp, s->szp, s->stp, s->spp, s->sdm, s->szm, s->stm, s->spm,
+                          s->sdt, s->szt, s->stt, s->spt};
+    for (const void *q : need) if (!q) return EXOTX_BAD_ARG;
+    if (c->h.nqspec == 1 && (!s->sqp || !s->sqm || !s->sqt)) return EXOTX_BAD_ARG;
+    if (!d_part && !s->sop) return EXOTX_BAD_ARG;
+    if (d_part && !s->srp) return EXOTX_BAD_ARG;
+    if (prec == EXOTX_FP64) return launch_spectral_fp64(spec_args<double>(c, s), d_part, (cudaStream_t)st);
+    return launch_spectral_fp32(spec_args<float>(c, s), d_part, (cudaStream_t)st);
+}
+
+EXOTX_API exotx_status exotx_spectrala(exotx_specconst c, int prec, const exotx_spec_state *s, exotx_stream st) {
+    return spec_run(c, prec, s, false, st);
+}
+EXOTX_API exotx_status exotx_spectrald(exotx_specconst c, int prec, const exotx_spec_state *s, exotx_stream st) {
+    return spec_run(c, prec, s, true, st);
+}

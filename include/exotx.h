@@ -292,6 +292,44 @@ exotx_status exotx_gpconst_destroy(exotx_gpconst c);
 exotx_status exotx_gridpoint(exotx_plan p, exotx_gpconst c, int prec, const void *gin, void *gout,
                              void *dw, const void *dq, int ninst, exotx_stream s);
 
+/* ---- semi-implicit spectral time step (plasim.f90 spectrala :2757-2918,
+ * spectrald :3645-3999), one model state, without their diagnostics ----
+ * spectrala: the adiabatic step -- divergence at t from the implicit equation
+ * (Hoskins and Simmons 1975 eq. 17, the inverse bm1(n) of makebm), surface
+ * pressure and temperature tendencies (eqs. 15, 14), the first part of the
+ * Robert-Asselin time filter, the leapfrog step, spp(1:2) = 0.
+ * spectrald: the diabatic tendencies (the forward gridpointd set's sdt, szt,
+ * stt, sqt) added, the implicit restoration (damp, srp), Rayleigh drag (tfrc)
+ * and hyperdiffusion (tdiss*, sak) tendencies, no drag or diffusion of the
+ * planetary vorticity, the optional top sponge, the second part of the filter.
+ * Rates are in the model's time unit 1/Omega, as plasim.f90:1583-1615 scales
+ * them; ndel/nhdiff define sak (:1617-1633). */
+typedef struct {
+    int nlev, nqspec, nsponge, nhdiff;
+    double delt, delt2, pnu, pnu21, plavor, dampsp, akap;
+    double t0[64], sigmah[64], dsigma[64];
+    double damp[64], tdisst[64], tdissq[64], tdissd[64], tdissz[64], tfrc[64];
+    int ndel[64];
+} exotx_spec_params;
+/* Earth defaults: 32 steps per rotation, pnu = 0.1, PlaSim's dissipation
+ * time scales and drag, the reference profile of exotx_gp_params_default */
+exotx_status exotx_spec_params_default(int nlev, exotx_spec_params *p);
+typedef struct exotx_specconst_s *exotx_specconst;
+/* the level matrices (initsi), bm1(n) for n = 1..NTRU (makebm) and sak for the
+ * plan's truncation, on the device */
+exotx_status exotx_specconst_create(exotx_plan p, const exotx_spec_params *sp, exotx_specconst *out);
+exotx_status exotx_specconst_destroy(exotx_specconst c);
+/* DEVICE arrays [level][NRSP] (sp*: [NRSP]), updated in place */
+typedef struct {
+    void *sdp, *szp, *stp, *sqp, *spp;   /* time level t, advanced to t + dt */
+    void *sdm, *szm, *stm, *sqm, *spm;   /* time level t - dt, filtered */
+    void *sdt, *szt, *stt, *sqt, *spt;   /* tendencies (spectrala reads gridpointa's, spectrald gridpointd's) */
+    const void *sop;                     /* surface geopotential [NRSP] (spectrala) */
+    const void *srp;                     /* restoration temperature [level][NRSP] (spectrald) */
+} exotx_spec_state;
+exotx_status exotx_spectrala(exotx_specconst c, int prec, const exotx_spec_state *s, exotx_stream st);
+exotx_status exotx_spectrald(exotx_specconst c, int prec, const exotx_spec_state *s, exotx_stream st);
+
 /* ---- radiation column pass (radmod.f90 radstep :927-1110) ---- */
 typedef struct {
     int nlev, nhor, nlon;                 /* nlon: longitudes per latitude row */

@@ -137,6 +137,30 @@ void oracle_initsi(int nlev, const double *sigmah, const double *dsigma, const d
                    double *g, double *c, double *tkp, double *t01s2, double *rdsig);
 void oracle_gridpoint(const oracle_gppar *P, const double *gin, double *gout, double *dw, const double *rcsq);
 
+/* ---------------- semi-implicit spectral step (exo_oracle_spec.c) ---------------- */
+typedef struct {
+    int nlev, ntru, nqspec, nsponge;
+    double delt, delt2, pnu, pnu21, plavor, dampsp;
+    const double *t0, *dsigma;                            /* [nlev] */
+    const double *g, *tau;                                /* [nlev*nlev] column major */
+    const double *bm1;                                    /* [(ntru+1)*nlev*nlev], jn = 0 unused */
+    const double *damp, *tdisst, *tdissq, *tdissd, *tdissz, *tfrc;   /* [nlev], scaled rates */
+    const double *sak;                                    /* [nlev][NRSP] */
+} oracle_specpar;
+typedef struct {
+    double *sdp, *szp, *stp, *sqp, *spp;   /* time level t (updated to t+dt) */
+    double *sdm, *szm, *stm, *sqm, *spm;   /* time level t-dt (filtered) */
+    double *sdt, *szt, *stt, *sqt, *spt;   /* tendencies */
+    const double *sop, *srp;               /* surface geopotential [NRSP], restoration T [nlev][NRSP] */
+} oracle_specstate;
+void oracle_tau(int L, const double *sigmah, const double *dsigma, const double *rdsig, const double *tkp,
+                const double *t01s2, const double *c, double *tau);
+void oracle_makebm(int L, int ntru, double delt, const double *t0, const double *dsigma, const double *g,
+                   const double *tau, double *bm1);
+void oracle_sak(int L, int ntru, const int *ndel, int nhdiff, double *sak);
+void oracle_spectrala(const oracle_specpar *P, oracle_specstate *S);
+void oracle_spectrald(const oracle_specpar *P, oracle_specstate *S);
+
 /* ---------------- OpenMP drivers (timed CPU baseline) ---------------- */
 int  oracle_num_threads(void);
 void oracle_inverse_set(const oracle_leg *L, int nlev, const double *spin, double *gpout,

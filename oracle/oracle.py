@@ -97,6 +97,11 @@ def _declare(L):
     L.oracle_forward_set.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_int]
     L.oracle_gridpoint.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
     L.oracle_initsi.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp, _dp, _dp, _dp]
+    L.oracle_tau.argtypes = [C.c_int] + [_dp] * 7
+    L.oracle_makebm.argtypes = [C.c_int, C.c_int, C.c_double] + [_dp] * 5
+    L.oracle_sak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, _dp]
+    L.oracle_spectrala.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_spectrald.argtypes = [C.c_void_p, C.c_void_p]
     L.oracle_inverse_set_d.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_double, C.c_int]
     L.oracle_forward_set_d.argtypes = [P(LegTables), C.c_int, _dp, _dp, C.c_int]
 
@@ -333,3 +338,61 @@ def gridpoint(gin, nlev, nlon, sigmah, dsigma, t0, akap, rdbrv, adv, psurf, ww, 
     rc = np.ascontiguousarray(rcsq, dtype=np.float64)
     lib().oracle_gridpoint(C.byref(p), _ptr(gin), _ptr(gout), _ptr(dw), _ptr(rc))
     return gout, dw
+
+
+SPEC_STATE = ("sdp", "szp", "stp", "sqp", "spp", "sdm", "szm", "stm", "sqm", "spm",
+              "sdt", "szt", "stt", "sqt", "spt", "sop", "srp")
+
+
+class SpecPar(C.Structure):
+    _fields_ = [("nlev", C.c_int), ("ntru", C.c_int), ("nqspec", C.c_int), ("nsponge", C.c_int)] + \
+               [(n, C.c_double) for n in ("delt", "delt2", "pnu", "pnu21", "plavor", "dampsp")] + \
+               [(n, _dp) for n in ("t0", "dsigma", "g", "tau", "bm1", "damp", "tdisst", "tdissq", "tdissd",
+                                   "tdissz", "tfrc", "sak")]
+
+
+class SpecState(C.Structure):
+    _fields_ = [(n, _dp) for n in SPEC_STATE]
+
+
+def spec_setup(ntru, nlev, sigmah, dsigma, t0, akap, delt, ndel, nhdiff):
+    """(g, tau, bm1, sak) of initsi, makebm and the diffusion (plasim.f90:1709-1760, :1683-1704, :1617-1633)."""
+    L = nlev
+    g, c, tkp, t01s2, rdsig = initsi(sigmah, dsigma, t0, akap)
+    gF, cF = np.ascontiguousarray(g.ravel(order="F")), np.ascontiguousarray(c.ravel(order="F"))
+    tau = np.zeros(L * L)
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (sigmah, dsigma, rdsig, tkp, t01s2)]
+    lib().oracle_tau(L, *[_ptr(x) for x in a], _ptr(cF), _ptr(tau))
+    bm1 = np.zeros((ntru + 1) * L * L)
+    t0a, dsa = np.ascontiguousarray(t0, dtype=np.float64), np.ascontiguousarray(dsigma, dtype=np.float64)
+    lib().oracle_makebm(L, ntru, delt, _ptr(t0a), _ptr(dsa), _ptr(gF), _ptr(tau), _ptr(bm1))
+    nrsp = (ntru + 1) * (ntru + 2)
+    sak = np.zeros(L * nrsp)
+    nd = (C.c_int * L)(*[int(x) for x in ndel[:L]])
+    lib().oracle_sak(L, ntru, nd, nhdiff, _ptr(sak))
+    return gF, tau, bm1, sak
+
+
+def spectral_step(part, p, ntru, state):
+    """spectrala ("a") or spectrald ("d") on a dict of [L][NRSP] arrays (copies
+    returned).  p: mapping with nlev, nqspec, nsponge, delt, delt2, pnu, pnu21,
+    plavor, dampsp, t0, sigmah, dsigma, damp, tdiss*, tfrc, akap, ndel, nhdiff."""
+    L = p["nlev"]
+    gF, tau, bm1, sak = spec_setup(ntru, L, p["sigmah"][:L], p["dsigma"][:L], p["t0"][:L], p["akap"], p["delt"],
+                                   p["ndel"], p["nhdiff"])
+    P = SpecPar()
+    P.nlev, P.ntru, P.nqspec, P.nsponge = L, ntru, p["nqspec"], p["nsponge"]
+    for k in ("delt", "delt2", "pnu", "pnu21", "plavor", "dampsp"):
+        setattr(P, k, p[k])
+    keep = {k: np.ascontiguousarray(np.asarray(p[k], dtype=np.float64)[:L]) for k in
+            ("t0", "dsigma", "damp", "tdisst", "tdissq", "tdissd", "tdissz", "tfrc")}
+    keep.update(g=gF, tau=tau, bm1=bm1, sak=sak)
+    for k, v in keep.items():
+        setattr(P, k, _ptr(v))
+    out = {k: np.array(v, dtype=np.float64, order="C", copy=True) for k, v in state.items()}
+    S = SpecState()
+    for k in SPEC_STATE:
+        if k in out:
+            setattr(S, k, _ptr(out[k]))
+    (lib().oracle_spectrala if part == "a" else lib().oracle_spectrald)(C.byref(P), C.byref(S))
+    return out
