@@ -92,6 +92,7 @@ SIGNATURES = {
     "exotx_gpconst_destroy": [_P],
     "exotx_gridpoint": [_P, _P, _I, _P, _P, _P, _P, _I, _S],
     "exotx_spec_params_default": [_I, _P],
+    "exotx_plan_tune": [_P, _I, C.c_longlong],
     "exotx_specconst_create": [_P, _P, C.POINTER(C.c_void_p)],
     "exotx_specconst_destroy": [_P],
     "exotx_spectrala": [_P, _I, _P, _S],

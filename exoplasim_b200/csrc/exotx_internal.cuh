@@ -104,6 +104,10 @@ struct exotx_plan_s {
     size_t work_bytes = 0;
     exotx::TcTables *tc = nullptr;
     exotx::HostPipe *hpipe = nullptr;  // device slots and streams of exotx_sets_host
+    // bytes of m-major Fourier intermediate one tensor-core launch covers
+    // (instances are grouped up to this, at least one): the intermediate is
+    // written by one kernel and read by the next, so it should stay in L2
+    size_t chunk_inv = 80u << 20, chunk_fwd = 80u << 20;
 };
 
 namespace exotx {

@@ -452,9 +452,9 @@ static exotx_status tc_inverse_run(exotx_plan p, const float *spin, float *gpout
     EXOTX_TRY(tc_tables(p, &T));
     const long long nrsp = 2LL * p->ncsp, nhor = (long long)p->nlat * p->nlon;
     const int nfo = dset ? 4 * L + 1 : 6 * L + 3;
-    // chunk instances so the m-major Fourier intermediate stays L2-resident (<= 80 MB of the 126 MB L2)
+    // chunk instances so the m-major Fourier intermediate stays L2-resident
     const size_t per_inst = (size_t)nfo * p->nlat * p->ntp1 * sizeof(float2);
-    int chunk = (int)std::max<size_t>(1, (80u << 20) / per_inst);
+    int chunk = (int)std::max<size_t>(1, p->chunk_inv / per_inst);
     chunk = std::min(chunk, ninst);
     EXOTX_TRY(ensure_work(p, per_inst * chunk));
     const int4 *jobs;
@@ -506,7 +506,7 @@ static exotx_status tc_forward_run(exotx_plan p, const float *gpin, float *spout
     const long long nrsp = 2LL * p->ncsp, nhor = (long long)p->nlat * p->nlon;
     const int nfi = dset ? 4 * L : 9 * L + 1, nfo = dset ? 4 * L : 4 * L + 1;
     const size_t per_inst = (size_t)nfi * p->nlat * p->ntp1 * sizeof(float2);
-    int chunk = (int)std::max<size_t>(1, (80u << 20) / per_inst);
+    int chunk = (int)std::max<size_t>(1, p->chunk_fwd / per_inst);
     chunk = std::min(chunk, ninst);
     EXOTX_TRY(ensure_work(p, per_inst * chunk));
     const int4 *jobs;

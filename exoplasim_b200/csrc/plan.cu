@@ -398,3 +398,12 @@ EXOTX_API exotx_status exotx_plan_table(exotx_plan p, int which, double *out) {
     EXOTX_CUDA(cudaMemcpy(out, p->d_qref + which * tsz, sizeof(double) * tsz, cudaMemcpyDeviceToHost));
     return EXOTX_OK;
 }
+
+EXOTX_API exotx_status exotx_plan_tune(exotx_plan p, int key, long long value) {
+    if (!p || value < 0) return EXOTX_BAD_ARG;
+    switch (key) {
+        case EXOTX_TUNE_CHUNK_INV: p->chunk_inv = (size_t)value; return EXOTX_OK;
+        case EXOTX_TUNE_CHUNK_FWD: p->chunk_fwd = (size_t)value; return EXOTX_OK;
+    }
+    return EXOTX_BAD_ARG;
+}

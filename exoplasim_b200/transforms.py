@@ -88,6 +88,13 @@ class Plan:
     def handle(self):
         return self._h
 
+    def tune(self, chunk_inv=None, chunk_fwd=None):
+        """Bytes of Fourier intermediate per tensor-core launch (exotx_plan_tune)."""
+        if chunk_inv is not None:
+            call("exotx_plan_tune", self._h, 0, int(chunk_inv))
+        if chunk_fwd is not None:
+            call("exotx_plan_tune", self._h, 1, int(chunk_fwd))
+
     # ---------------------------------------------------------------- tables
     def gauss(self):
         """(sid, gwd) as float64 numpy arrays, north first (inigau outputs)."""

@@ -74,6 +74,14 @@ exotx_status exotx_plan_gauss(exotx_plan p, double *sid, double *gwd);
  * which = 0..7 for qi,qj,qc,qe,qm,qq,qu,qv (legmod.f90:13-20) */
 exotx_status exotx_plan_table(exotx_plan p, int which, double *out);
 
+/* Tunables of a plan's tensor-core sets (no counterpart in the reference):
+ * the bytes of m-major Fourier intermediate one inverse (forward) launch
+ * covers -- instances are grouped up to it, at least one per launch -- so that
+ * the intermediate one kernel writes is still in L2 when the next reads it.
+ * Default 80 MB each. */
+typedef enum { EXOTX_TUNE_CHUNK_INV = 0, EXOTX_TUNE_CHUNK_FWD = 1 } exotx_tune_key;
+exotx_status exotx_plan_tune(exotx_plan p, int key, long long value);
+
 /* inigau (gaussmod.f90:5-40) on the device: sid(nlat), gwd(nlat) device arrays */
 exotx_status exotx_inigau(int nlat, double *sid, double *gwd, exotx_stream s);
 
