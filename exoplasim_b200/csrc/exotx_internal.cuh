@@ -108,6 +108,7 @@ struct exotx_plan_s {
     // (instances are grouped up to this, at least one): the intermediate is
     // written by one kernel and read by the next, so it should stay in L2
     size_t chunk_inv = 80u << 20, chunk_fwd = 80u << 20;
+    int inv_half_ok = 1;   // the inverse kernel may run two CTAs per SM where they fit
 };
 
 namespace exotx {

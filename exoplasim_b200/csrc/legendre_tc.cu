@@ -317,14 +317,30 @@ static constexpr size_t kPersistSmemMin = 116 * 1024;
 
 #include "legendre_tc_kernels.cuh"
 
+// the half-table inverse mode runs where two CTAs fit an SM with 64-column
+// qi tiles (and 32-column qu/qv tiles, 256 TMEM columns each)
+static constexpr size_t kInvHalfSmemMax = 112 * 1024;
+static bool inv_half(exotx_plan p, int nj8) {
+    return p->inv_half_ok && inv_smem_half(nj8, p->ntp1, 64) <= kInvHalfSmemMax;
+}
+
 // inverse column tiles: as wide as shared memory (both parities of one table
-// plus the staged columns) and TMEM (tables x parities x columns <= 256) allow
-static void inv_tiles(int nj8, int ntp1, int *nc_qi, int *nc_uv) {
+// plus the staged columns) and TMEM (tables x parities x columns <= 256) allow;
+// in the half-table mode 64 (qi, qj) and 32 (qu/qv) columns
+static void inv_tiles_full(int nj8, int ntp1, int *nc_qi, int *nc_uv) {
     int a = 128, b = 64;
     while (a > 16 && inv_smem(nj8, ntp1, a) > TC_SMEM_MAX) a -= 16;
     while (b > 16 && inv_smem(nj8, ntp1, b) > TC_SMEM_MAX) b -= 16;
     *nc_qi = a;
     *nc_uv = b;
+}
+static void inv_tiles(exotx_plan p, int nj8, int *nc_qi, int *nc_uv) {
+    if (inv_half(p, nj8)) {
+        *nc_qi = 64;
+        *nc_uv = 32;
+        return;
+    }
+    inv_tiles_full(nj8, p->ntp1, nc_qi, nc_uv);
 }
 
 // forward kernel variants, tried in order until the widest job fits shared memory:
@@ -408,7 +424,7 @@ static exotx_status tc_jobs(exotx_plan p, TcTables *T, int dir, int L, int ninst
         }
     std::vector<int4> v;
     int INV_NC_QI, INV_NC_UV;
-    inv_tiles(T->nj8, p->ntp1, &INV_NC_QI, &INV_NC_UV);
+    inv_tiles(p, T->nj8, &INV_NC_QI, &INV_NC_UV);
     for (int m = 0; m < p->ntp1; m++) {
         if (dir == 0) {
             const int n0 = ninst * (dset ? 2 * L + 1 : 4 * L + 1) * 2, n1 = dset ? 0 : ninst * 2, n2 = ninst * L * 4;
@@ -461,8 +477,10 @@ static exotx_status tc_inverse_run(exotx_plan p, const float *spin, float *gpout
     int njobs;
     EXOTX_TRY(tc_jobs(p, T, 0, L, chunk, &jobs, &njobs, dset));
     int nc_qi, nc_uv;
-    inv_tiles(T->nj8, p->ntp1, &nc_qi, &nc_uv);
-    size_t smem = std::max(inv_smem(T->nj8, p->ntp1, nc_qi), inv_smem(T->nj8, p->ntp1, nc_uv));
+    inv_tiles(p, T->nj8, &nc_qi, &nc_uv);
+    const bool half = inv_half(p, T->nj8);
+    size_t smem = half ? std::max(inv_smem_half(T->nj8, p->ntp1, nc_qi), inv_smem_half(T->nj8, p->ntp1, nc_uv))
+                       : std::max(inv_smem(T->nj8, p->ntp1, nc_qi), inv_smem(T->nj8, p->ntp1, nc_uv));
     if (smem > TC_SMEM_MAX) return EXOTX_BAD_DIM;
     EXOTX_CUDA(cudaFuncSetAttribute(k_tc_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
     for (int i0 = 0; i0 < ninst; i0 += chunk) {
@@ -473,6 +491,7 @@ static exotx_status tc_inverse_run(exotx_plan p, const float *spin, float *gpout
         TcInvLaunch P;
         P.jobs = jl;
         P.nprod = 6;
+        P.half = half ? 1 : 0;
         TcInvArgs &A = P.seg[0];
         A.tab = T->inv; A.off = T->d_inv_off; A.woff = p->d_woff;
         A.spin = spin + (size_t)i0 * (4 * L + 1) * nrsp;
@@ -483,7 +502,7 @@ static exotx_status tc_inverse_run(exotx_plan p, const float *spin, float *gpout
         A.plavor = (float)p->desc.plavor;
         A.dset = dset;
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
-        EXOTX_CUDA(launch_pdl(k_tc_inverse, dim3(nj), dim3(TCI), smem, s, P));   // set-up overlaps the last tail
+        EXOTX_CUDA(launch_pdl(k_tc_inverse, dim3(nj), dim3(half ? TCI_HALF : TCI), smem, s, P));   // set-up overlaps the last tail
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
         EXOTX_TRY(fft_inverse_l<float>((const float *)p->d_work, gpout + (size_t)i0 * nfo * nhor, p->nlon, A.nrows,
@@ -593,7 +612,7 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
         const int L = g.L, ni = g.ninst;
         if (dir == 0) {
             int a, b;
-            inv_tiles(T->nj8, p->ntp1, &a, &b);
+            inv_tiles_full(T->nj8, p->ntp1, &a, &b);   // ensembles run the one-CTA-per-SM mode
             a = std::max(16, std::min(a, nc_qi_cap) & ~15);
             b = std::max(16, std::min(b, nc_uv_cap) & ~15);
             smax = std::max(smax, std::max(inv_smem(T->nj8, p->ntp1, a), inv_smem(T->nj8, p->ntp1, b)));

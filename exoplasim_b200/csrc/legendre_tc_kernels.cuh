@@ -32,6 +32,11 @@ struct TcInvLaunch {
     TcInvArgs seg[TC_MAXSEG];
     const int4 *jobs;       // (m, group | seg << 2, first column, columns)
     int nprod;
+    // 0: one CTA of 512 threads per SM, a table's two parity halves staged
+    // together, 512 TMEM columns.  1: two CTAs of 256 threads per SM, one
+    // parity half of a table in shared memory at a time and 256 TMEM columns,
+    // so one CTA's copies, staging and epilogue overlap the other's MMAs.
+    int half = 0;
 };
 
 // spectral row (complex, filter not applied) feeding column pair gq, and
@@ -61,15 +66,19 @@ __device__ __forceinline__ const float2 *inv_row(const TcInvArgs &A, int group, 
     return reinterpret_cast<const float2 *>(A.spin + ((size_t)inst * nf + f) * A.nrsp);
 }
 
-// 16 warps: all stage operands; thread 0 issues the table copies and MMAs;
-// in the epilogue warp w drains TMEM lane quarter w % 4 for column chunk w / 4
+// 16 warps (8 in the half-table mode): all stage operands; thread 0 issues
+// the table copies and MMAs; in the epilogue warp w drains TMEM lane quarter
+// w % 4 for column chunks w / 4, w / 4 + nwarps / 4, ...
 constexpr int TCI = 512;
+constexpr int TCI_HALF = 256;
 
 __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcInvLaunch P) {
     extern __shared__ __align__(128) unsigned char sm[];
     const int4 jb = P.jobs[blockIdx.x];
     const TcInvArgs &A = P.seg[jb.y >> 2];
     const int nprod = P.nprod;
+    const bool half = P.half != 0;
+    const int nthr = blockDim.x, nsub = nthr >> 7;   // column-chunk groups of 4 warps
     const int m = jb.x, group = jb.y & 3, c0 = jb.z, nc = jb.w;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, sub = warp >> 2;
     const int K = A.ntp1 - m;
@@ -79,7 +88,8 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
     const int ntab = group == 2 ? 2 : 1;
     const int nj8 = A.nj8;
     const size_t ttile[2] = {(size_t)nj8 * Kp[0] * 2, (size_t)nj8 * Kp[1] * 2};
-    const size_t tbytes = 3 * (ttile[0] + ttile[1]);
+    // the table buffer: both parity halves, or (half mode) the larger one
+    const size_t tbytes = half ? 3 * ttile[0] : 3 * (ttile[0] + ttile[1]);
     // data tiles use the padded operand layout (core matrices 144 bytes apart along K)
     const size_t dtile[2] = {(size_t)(ncp / 8) * (Kp[0] / 8) * tc::kPadLbo, (size_t)(ncp / 8) * (Kp[1] / 8) * tc::kPadLbo};
     unsigned char *tab = sm;
@@ -89,15 +99,17 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
     uint64_t *bar_mma = bar_tma + 1;
     uint64_t *bar_done = bar_tma + 2;
     uint32_t *slot = reinterpret_cast<uint32_t *>(bar_tma + 3);
+    const uint32_t tcols = half ? 256 : 512;
+    const int t0 = group == 0 ? 0 : (group == 1 ? 1 : 2);
     pdl_trigger();
-    if (warp == 0) tc::tmem_alloc(slot, 512);
+    if (warp == 0) tc::tmem_alloc(slot, tcols);
     if (tid == 0) {
         tc::mbar_init(bar_tma, 1);
         tc::mbar_init(bar_mma, 1);
         tc::mbar_init(bar_done, 1);
         tc::mbar_fence_init();
-        // first table copy goes out before the staging so the two overlap
-        const int t0 = group == 0 ? 0 : (group == 1 ? 1 : 2);
+        // first table copy (half mode: parity 0 of the first table) goes out
+        // before the staging so the two overlap
         tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
         tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0], (uint32_t)tbytes, bar_tma);
     }
@@ -115,11 +127,11 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
         const int npair = ncp >> 1, hk = Kp[0] >> 1;   // Kp[0] >= Kp[1]
         const int nslot = npair * hk;
         const int w0 = A.woff[m];
-        for (int s0 = tid; s0 < nslot; s0 += INV_SLOTS * TCI) {
+        for (int s0 = tid; s0 < nslot; s0 += INV_SLOTS * nthr) {
             float2 x[INV_SLOTS][2][2];   // [slot][parity][k - 2l]
 #pragma unroll
             for (int i = 0; i < INV_SLOTS; i++) {
-                const int s = s0 + i * TCI, q = s / hk, l = s - q * hk;
+                const int s = s0 + i * nthr, q = s / hk, l = s - q * hk;
                 bool zv = false;
                 const float2 *row = (s < nslot && 2 * q < nc) ? inv_row(A, group, (c0 + 2 * q) >> 1, &zv) : nullptr;
 #pragma unroll
@@ -134,7 +146,7 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
             }
 #pragma unroll
             for (int i = 0; i < INV_SLOTS; i++) {
-                const int s = s0 + i * TCI, q = s / hk, l = s - q * hk;
+                const int s = s0 + i * nthr, q = s / hk, l = s - q * hk;
                 if (s >= nslot) break;
 #pragma unroll
                 for (int p = 0; p < 2; p++) {
@@ -157,7 +169,41 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
     tc::fence_after_sync();
     const uint32_t tmem = *slot;
     bool ok = true;
-    if (tid == 0) {
+    if (tid == 0 && half) {
+        // one parity half of one table at a time through one buffer: copy,
+        // MMAs, and the next copy once those MMAs have read the buffer
+        const uint32_t idesc = tc::idesc_bf16(128, ncp);
+        const int np = Kq[1] ? 2 : 1, nh = ntab * np;
+        for (int hix = 0; hix < nh && ok; hix++) {
+            const int ti = hix / np, p = hix - ti * np;
+            if (hix > 0) {
+                ok = tc::mbar_wait(bar_mma, (hix - 1) & 1);
+                if (!ok) break;
+                const uint32_t hb = (uint32_t)(3 * ttile[p]);
+                tc::mbar_arrive_expect_tx(bar_tma, hb);
+                tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0 + ti] + (p ? 3 * ttile[0] : 0), hb, bar_tma);
+            }
+            ok = tc::mbar_wait(bar_tma, hix & 1);
+            if (!ok) break;
+            tc::fence_after_sync();
+            const uint32_t dm = tmem + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp);
+            const uint32_t dc = tmem + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp);
+            const uint32_t sbo = (uint32_t)(Kp[p] / 8) * 128, sbo_b = (uint32_t)(Kp[p] / 8) * tc::kPadLbo;
+            const uint64_t da0 = tc::smem_desc(tab, 128, sbo);
+            const uint64_t db0 = tc::smem_desc(dat + (p ? 3 * dtile[0] : 0), tc::kPadLbo, sbo_b);
+            const uint32_t tt = (uint32_t)ttile[p], dt = (uint32_t)dtile[p];
+            for (int kc = 0; kc < Kp[p] / 16; kc++) {
+#pragma unroll
+                for (int pr = 0; pr < 6; pr++)
+                    if (pr < nprod)
+                        tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
+                                     tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 2 * tc::kPadLbo), idesc,
+                                     kc > 0 || pr > 1);
+            }
+            tc::mma_commit(hix == nh - 1 ? bar_done : bar_mma);
+        }
+        if (!ok) atomicExch(&g_tc_error, 1);
+    } else if (tid == 0) {
         const uint32_t idesc = tc::idesc_bf16(128, ncp);
         for (int ti = 0; ti < ntab && ok; ti++) {
             if (ti > 0) {
@@ -217,7 +263,7 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
         if (group < 2) {
             // P-type qi: N = D0 + D1, S = D0 - D1; Q-type qj: S = D1 - D0
             const float ss = group == 0 ? 1.f : -1.f;
-            for (int cc = sub * 16; cc < ncp; cc += 64) {
+            for (int cc = sub * 16; cc < ncp; cc += 16 * nsub) {
                 uint32_t rm0[16], rc0[16], rm1[16], rc1[16];
                 tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(0 * ncp + cc), rm0);
                 tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(1 * ncp + cc), rc0);
@@ -268,7 +314,7 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
             // dv2uv: u = qv*Z - i*qu*D, v = -i*qu*Z - qv*D; qu P-type, qv Q-type.
             // accumulators r = (table, parity): 0 qu p0, 1 qu p1, 2 qv p0, 3 qv p1;
             // columns Dr, Di, Zr, Zi per level; a chunk of 8 columns is 2 levels
-            for (int cc = sub * 8; cc < ncp; cc += 32) {
+            for (int cc = sub * 8; cc < ncp; cc += 8 * nsub) {
                 uint32_t rm[4][8], rc[4][8];
 #pragma unroll
                 for (int r = 0; r < 4; r++) {
@@ -307,12 +353,18 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 512);
+    if (warp == 0) tc::tmem_dealloc(tmem, tcols);
 }
 
 static size_t inv_smem(int nj8, int K, int ncp) {
     const int Kp0 = pad16(kpar(K, 0)), Kp1 = pad16(kpar(K, 1));
     return 3 * (size_t)nj8 * (Kp0 + Kp1) * 2 + 3 * (size_t)(ncp / 8) * ((Kp0 + Kp1) / 8) * tc::kPadLbo +
+           (size_t)(128 - nj8) * 64 * 2 + 128 + 80;
+}
+// the same in the half-table mode: one parity half (the larger) of a table
+static size_t inv_smem_half(int nj8, int K, int ncp) {
+    const int Kp0 = pad16(kpar(K, 0)), Kp1 = pad16(kpar(K, 1));
+    return 3 * (size_t)nj8 * Kp0 * 2 + 3 * (size_t)(ncp / 8) * ((Kp0 + Kp1) / 8) * tc::kPadLbo +
            (size_t)(128 - nj8) * 64 * 2 + 128 + 80;
 }
 

@@ -404,6 +404,16 @@ EXOTX_API exotx_status exotx_plan_tune(exotx_plan p, int key, long long value) {
     switch (key) {
         case EXOTX_TUNE_CHUNK_INV: p->chunk_inv = (size_t)value; return EXOTX_OK;
         case EXOTX_TUNE_CHUNK_FWD: p->chunk_fwd = (size_t)value; return EXOTX_OK;
+        case EXOTX_TUNE_INV_HALF:
+            if (value > 1) return EXOTX_BAD_ARG;
+            if (p->inv_half_ok != (int)value) {
+                // the cached inverse job lists follow the mode: rebuild them
+                // (after the work that may still read them)
+                EXOTX_CUDA(cudaDeviceSynchronize());
+                tc_free(p);
+                p->inv_half_ok = (int)value;
+            }
+            return EXOTX_OK;
     }
     return EXOTX_BAD_ARG;
 }

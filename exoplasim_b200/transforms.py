@@ -88,12 +88,15 @@ class Plan:
     def handle(self):
         return self._h
 
-    def tune(self, chunk_inv=None, chunk_fwd=None):
-        """Bytes of Fourier intermediate per tensor-core launch (exotx_plan_tune)."""
+    def tune(self, chunk_inv=None, chunk_fwd=None, inv_half=None):
+        """exotx_plan_tune: bytes of Fourier intermediate per tensor-core launch,
+        and whether the inverse kernel may run two CTAs per SM."""
         if chunk_inv is not None:
             call("exotx_plan_tune", self._h, 0, int(chunk_inv))
         if chunk_fwd is not None:
             call("exotx_plan_tune", self._h, 1, int(chunk_fwd))
+        if inv_half is not None:
+            call("exotx_plan_tune", self._h, 2, int(bool(inv_half)))
 
     # ---------------------------------------------------------------- tables
     def gauss(self):

@@ -79,7 +79,10 @@ exotx_status exotx_plan_table(exotx_plan p, int which, double *out);
  * covers -- instances are grouped up to it, at least one per launch -- so that
  * the intermediate one kernel writes is still in L2 when the next reads it.
  * Default 80 MB each. */
-typedef enum { EXOTX_TUNE_CHUNK_INV = 0, EXOTX_TUNE_CHUNK_FWD = 1 } exotx_tune_key;
+/* EXOTX_TUNE_INV_HALF: 1 (default) lets the inverse kernel run two CTAs
+ * per SM, each holding one parity half of a table, where they fit shared
+ * memory; 0 keeps one CTA per SM with both halves. */
+typedef enum { EXOTX_TUNE_CHUNK_INV = 0, EXOTX_TUNE_CHUNK_FWD = 1, EXOTX_TUNE_INV_HALF = 2 } exotx_tune_key;
 exotx_status exotx_plan_tune(exotx_plan p, int key, long long value);
 
 /* inigau (gaussmod.f90:5-40) on the device: sid(nlat), gwd(nlat) device arrays */
