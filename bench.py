@@ -63,12 +63,19 @@ def fft_bytes(nlat, nlev, half, esz):
     return rows * (nlon * esz + (ntru + 1) * 2 * esz)
 
 
-# DRAM bytes per launch of the dominant kernel from one ncu capture (dram__bytes_read.sum
-# + dram__bytes_write.sum), keyed by (kernel, workload); the summary with its command is
-# in profiles/.
-# k_tc_forward_pipe on two T127 L20 instances (one launch of the default step), one
-# cold-cache ncu capture: 99.2 MB read + 5.8 MB written
-NCU_TRAFFIC = {("tc_forward", WORKLOAD): 99.17056e6 + 5.818368e6}
+# DRAM bytes per INSTANCE of the dominant kernel from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch over a known number
+# of instances, divided by it), keyed by (kernel, workload); scaled to a launch by
+# the instances it processes (the traffic grows in proportion: the intermediate
+# is read once per instance, the tables once per launch are small beside it).
+# k_tc_forward_pipe on two T127 L20 instances, one cold-cache ncu capture:
+# 99.2 MB read + 5.8 MB written.  The summary with its command is in profiles/.
+NCU_TRAFFIC_PER_INST = {("tc_forward", WORKLOAD): (99.17056e6 + 5.818368e6) / 2}
+
+
+def traffic_per_launch(kernel, inst_per_launch):
+    t = NCU_TRAFFIC_PER_INST.get((kernel, WORKLOAD))
+    return None if t is None else t * inst_per_launch
 
 
 def args_():
@@ -370,7 +377,7 @@ def run_ours(a, rank, world, local_rank):
     D = kernels[dom]
     roof = {"bound": "tensor" if D["bound"] == "tensor" else "hbm", "kernel": dom, "achieved": D["achieved"],
             "peak": D["peak"], "unit": D["unit"], "frac": D["frac"],
-            "traffic": NCU_TRAFFIC.get((dom, WORKLOAD)), "peak_kind": peak_kind,
+            "traffic": traffic_per_launch(dom, B * a.steps / D["launches"]), "peak_kind": peak_kind,
             "algorithmic_per_launch": D["algorithmic_per_launch"],
             "algorithmic_unit": "flops" if D["unit"] == "TFLOP/s" else "bytes",
             "ms_per_launch": D["ms_per_launch"]}

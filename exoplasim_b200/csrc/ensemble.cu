@@ -2,8 +2,9 @@
 // runs one model state per process, plasim.f90 gridpointa :2396-2486).
 // Instances of different truncations and level counts are grouped into
 // segments of one resolution and level count; each half of the round trip is
-// one tensor-core Legendre launch plus one FFT launch over all segments, so
-// the whole ensemble step is four kernels (and one CUDA graph when captured).
+// one tensor-core Legendre launch plus one FFT launch over all segments, and
+// the forward half one small launch more for the FP64 global means, so the
+// whole ensemble step is five kernels (and one CUDA graph when captured).
 // Segments whose rows have a register-resident FFT kernel (NLON 384) take one
 // FFT launch more per half when they are mixed with other lengths.
 #include <algorithm>
@@ -75,7 +76,10 @@ static exotx_status ens_forward(exotx_ensemble e, const float *gpin, float *spou
         f[i] = FftEnsSeg{gpin + e->seg_gin[i], v[i].W, rows, 1, rows, p->nlon, p->ntp1, folded ? p->nlat : 0};
     }
     EXOTX_TRY(fft_ens(true, f.data(), (int)f.size(), s));
-    return tc_ens_run(v.data(), (int)v.size(), 1, e->jobs[1], e->njobs[1], e->smem[1], e->nprod, s);
+    EXOTX_TRY(tc_ens_run(v.data(), (int)v.size(), 1, e->jobs[1], e->njobs[1], e->smem[1], e->nprod, s));
+    std::vector<const float *> g(v.size());
+    for (size_t i = 0; i < v.size(); i++) g[i] = gpin + e->seg_gin[i];
+    return tc_ens_n0(v.data(), g.data(), (int)v.size(), s);   // global means in FP64
 }
 
 // acc[0] += sum (a-b)^2, acc[1] += sum b^2

@@ -107,8 +107,11 @@ struct exotx_plan_s {
     // bytes of m-major Fourier intermediate one tensor-core launch covers
     // (instances are grouped up to this, at least one): the intermediate is
     // written by one kernel and read by the next, so it should stay in L2
-    size_t chunk_inv = 80u << 20, chunk_fwd = 80u << 20;
-    int inv_half_ok = 1;   // the inverse kernel may run two CTAs per SM where they fit
+    // 512 MB: up to 21 T127 L20 instances per inverse launch, 14 per forward;
+    // fewer, larger launches measured faster than L2-sized ones (T127 L20,
+    // 8 instances: 10.2K round trips/s with one launch per half, 9.5K with 80 MB)
+    size_t chunk_inv = (size_t)512 << 20, chunk_fwd = (size_t)512 << 20;
+    int inv_half_ok = 0;   // the inverse kernel may run two CTAs per SM where they fit
 };
 
 namespace exotx {
@@ -165,9 +168,12 @@ struct FftEnsSeg {
     int fold_nlat = 0;  // forward: > 0 writes the equator-folded layout for nlat-row fields
 };
 // forward FFT into the equator-folded m-major layout of the tensor-core forward
-// kernel (E = north + south rows, then O = north - south, per field) (fft.cu)
+// kernel (E = north + south rows, then O = north - south, per field) (fft.cu).
+// rowsum (may be null): also the FP64 sum of every grid row, in the order of
+// row_sum_fp64 (register-resident lengths only; EXOTX_NOT_BUILT otherwise)
 exotx_status fft_forward_fold(const float *in, float *out, int n, int nlat, long long lot, int kf, long long f_ms,
-                              cudaStream_t s);
+                              double *rowsum, cudaStream_t s);
+bool fft_fold_rowsum(int n);   // whether fft_forward_fold forms row sums for grid length n
 exotx_status fft_ens(bool fwd, const FftEnsSeg *segs, int nseg, cudaStream_t s);
 
 // element-wise FP64 <-> FP32 conversion of n device reals (fortran_abi.cu)
@@ -204,6 +210,7 @@ exotx_status tc_ens_jobs(const EnsSeg *segs, int nseg, int dir, int nc_qi_cap, i
 exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_jobs, int njobs, size_t smem,
                         int nprod, cudaStream_t s);
 bool tc_ens_fwd_folded(const EnsSeg *segs, int nseg);
+exotx_status tc_ens_n0(const EnsSeg *segs, const float *const *gpin, int nseg, cudaStream_t s);
 exotx_status tc_error_reset(cudaStream_t s);
 exotx_status tc_error_read(int *err, cudaStream_t s);
 // the same for the FFT kernels' bounded waits (fft.cu)

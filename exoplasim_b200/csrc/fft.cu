@@ -708,41 +708,75 @@ __device__ __forceinline__ void rf_setup(const RfSmem<N> &S, const cpx<float> *_
 // After a timeout every thread waits once more (bounded) for copies still in
 // flight, so none lands in shared memory after the block has left (out of
 // line: the error path takes no registers from the transform).
-__device__ __noinline__ void rf_loads_timed_out(uint64_t *bar) {
+__device__ __noinline__ void rf_loads_timed_out(uint64_t *bar, uint32_t phase) {
     if (threadIdx.x == 0) atomicExch(&g_fft_error, 1);
-    tc::mbar_wait(bar, 0);
+    tc::mbar_wait(bar, phase);
 }
-__device__ __forceinline__ bool rf_wait_loads(uint64_t *bar) {
-    const bool ok = __syncthreads_and(tc::mbar_wait(bar, 0)) != 0;
-    if (!ok) rf_loads_timed_out(bar);
+__device__ __forceinline__ bool rf_wait_loads(uint64_t *bar, uint32_t phase = 0) {
+    const bool ok = __syncthreads_and(tc::mbar_wait(bar, phase)) != 0;
+    if (!ok) rf_loads_timed_out(bar, phase);
     return ok;
 }
 
-// Forward complex transform of the block's RB rows; afterwards row r's Z[k]
-// sits at S.r[r * RZ + k] (visible to the block).  grow(r) is row r's index in
-// g (rows of n floats), or < 0 for a zero row.  False if the loads timed out.
+// FP64 sum of a grid row of 2 P Q reals held by P consecutive lanes, lane t
+// holding the complex elements t + P j (j < Q): each lane adds its values in
+// j order (real part first), then the P lanes combine by an xor butterfly, so
+// every lane ends with the same value.  The n = 0 kernel (legendre_tc.cu) reproduces
+// this order when it sums the rows from global memory.
+template <int P, int Q>
+__device__ __forceinline__ double row_sum_fp64(const cpx<float> *v) {
+    double a = 0.0;
+#pragma unroll
+    for (int j = 0; j < Q; j++) {
+        a += (double)v[j].x;
+        a += (double)v[j].y;
+    }
+#pragma unroll
+    for (int o = 1; o < P; o <<= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    return a;
+}
+
+// Warp 0 issues one bulk copy per row of the block into `stage` (row stride
+// RG), completing on `bar`; rows without a source (grow(r) < 0) are zeroed by
+// their own threads.  grow(r) is row r's index in g (rows of n floats).
 template <int N, typename RowOf>
-__device__ __forceinline__ bool rf_forward_rows(const float *__restrict__ g, RowOf grow, const RfSmem<N> &S) {
+__device__ __forceinline__ void rf_issue_rows(const float *__restrict__ g, RowOf grow, cpx<float> *stage,
+                                              uint64_t *bar) {
     using Lay = RfLayout<N>;
-    constexpr int P = Lay::P, Q = Lay::Q, H = Lay::H, QP = Q / P, RB = Lay::RB;
+    constexpr int P = Lay::P, H = Lay::H, RB = Lay::RB;
     const int t = threadIdx.x % P, r = threadIdx.x / P;
-    if (threadIdx.x < 32) {   // warp 0: one bulk copy per row
+    if (threadIdx.x < 32) {
         const long long gr = threadIdx.x < RB ? grow(threadIdx.x) : -1ll;
         const unsigned valid = __ballot_sync(0xffffffffu, gr >= 0);
-        if (threadIdx.x == 0) tc::mbar_arrive_expect_tx(S.bar, (uint32_t)__popc(valid) * (uint32_t)(N * 4));
+        if (threadIdx.x == 0) tc::mbar_arrive_expect_tx(bar, (uint32_t)__popc(valid) * (uint32_t)(N * 4));
         __syncwarp();
-        if (gr >= 0) tc::bulk_g2s(S.r + threadIdx.x * Lay::RG, g + gr * N, N * 4, S.bar);
+        if (gr >= 0) tc::bulk_g2s(stage + threadIdx.x * Lay::RG, g + gr * N, N * 4, bar);
     }
     if (grow(r) < 0) {   // zero rows: written here, never by a copy
-        for (int j = t; j < H; j += P) S.r[r * Lay::RG + j] = cpx<float>{0.f, 0.f};
+        for (int j = t; j < H; j += P) stage[r * Lay::RG + j] = cpx<float>{0.f, 0.f};
     }
-    if (!rf_wait_loads(S.bar)) return false;
+}
+
+// Forward complex transform of the block's RB rows staged in `stage` (the
+// loads complete); afterwards row r's Z[k] sits at x[r * RZ + k] (visible to
+// the block).  `stage` and `x` may be the same region.  after_read() runs
+// once every thread has its row values in registers (a block barrier lies
+// before it), before x is written.
+template <int N, bool RSUM = false, typename AfterRead>
+__device__ __forceinline__ void rf_forward_core(const cpx<float> *stage, cpx<float> *x, const cpx<float> *tqs,
+                                                AfterRead after_read, double *rsum = nullptr) {
+    using Lay = RfLayout<N>;
+    constexpr int P = Lay::P, Q = Lay::Q, QP = Q / P;
+    const int t = threadIdx.x % P, r = threadIdx.x / P;
     cpx<float> v[Q];
-    const cpx<float> *s = S.r + r * Lay::RG + t;
+    const cpx<float> *s = stage + r * Lay::RG + t;
 #pragma unroll
     for (int j = 0; j < Q; j++) v[j] = s[P * j];
+    if constexpr (RSUM) *rsum = row_sum_fp64<P, Q>(v);
+    __syncthreads();   // the staged rows are read
+    after_read();
     dftQ<float, -1, Q>(v);
-    const cpx<float> *tq = S.tq + t * Lay::RT;
+    const cpx<float> *tq = tqs + t * Lay::RT;
 #pragma unroll
     for (int q = 2; q < Q; q += 2) {
         const float4 f = *reinterpret_cast<const float4 *>(tq + q);
@@ -750,26 +784,35 @@ __device__ __forceinline__ bool rf_forward_rows(const float *__restrict__ g, Row
         v[q + 1] = cmul(v[q + 1], cpx<float>{f.z, f.w});
     }
     v[1] = cmul(v[1], tq[1]);
-    __syncthreads();   // the staged rows are read; the transposition overwrites them
-    cpx<float> *x = S.r + r * Lay::RS;
+    cpx<float> *xr = x + r * Lay::RS;
 #pragma unroll
     for (int q = 0; q < Q; q += 2)
-        *reinterpret_cast<float4 *>(x + t * Lay::RT + q) = make_float4(v[q].x, v[q].y, v[q + 1].x, v[q + 1].y);
+        *reinterpret_cast<float4 *>(xr + t * Lay::RT + q) = make_float4(v[q].x, v[q].y, v[q + 1].x, v[q + 1].y);
     __syncthreads();
     cpx<float> z[QP][P];
 #pragma unroll
     for (int i = 0; i < QP; i++) {
 #pragma unroll
-        for (int u = 0; u < P; u++) z[i][u] = x[u * Lay::RT + QP * t + i];
+        for (int u = 0; u < P; u++) z[i][u] = xr[u * Lay::RT + QP * t + i];
         dft8<float, -1>(z[i]);
     }
     __syncthreads();   // the spectra overwrite the transposition buffer
-    cpx<float> *zs = S.r + r * Lay::RZ;
+    cpx<float> *zs = x + r * Lay::RZ;
 #pragma unroll
     for (int i = 0; i < QP; i++)
 #pragma unroll
         for (int m = 0; m < P; m++) zs[QP * t + i + Q * m] = z[i][m];
     __syncthreads();
+}
+
+// Forward complex transform of the block's RB rows; afterwards row r's Z[k]
+// sits at S.r[r * RZ + k] (visible to the block).  grow(r) is row r's index in
+// g (rows of n floats), or < 0 for a zero row.  False if the loads timed out.
+template <int N, typename RowOf>
+__device__ __forceinline__ bool rf_forward_rows(const float *__restrict__ g, RowOf grow, const RfSmem<N> &S) {
+    rf_issue_rows<N>(g, grow, S.r, S.bar);
+    if (!rf_wait_loads(S.bar)) return false;
+    rf_forward_core<N>(S.r, S.r, S.tq, [] {});
     return true;
 }
 
@@ -865,6 +908,106 @@ __device__ __forceinline__ void rfft_fwd_fold_rf_body(const float *gp, float *fc
     }
 }
 
+// Persistent form of rfft_fwd_fold_rf_body.  A block sets up its twiddle
+// tables once and walks the items blk = blockIdx.x, + gridDim.x, ... (an item
+// is RB/2 latitude pairs of one field).  The grid rows are staged in their own
+// region G, apart from the transposition/spectra region X, so the bulk loads
+// of the next item are issued as soon as this item's rows are in registers
+// and arrive while it is transformed and written out.
+template <int N> struct RfPLayout {
+    using Lay = RfLayout<N>;
+    static constexpr int RX = Lay::RS > Lay::RZ ? Lay::RS : Lay::RZ;
+    static constexpr size_t OFF_X = (size_t)Lay::RB * Lay::RG * 8, OFF_TQ = OFF_X + (size_t)Lay::RB * RX * 8,
+                            OFF_RT = OFF_TQ + (size_t)Lay::P * Lay::RT * 8, OFF_BAR = OFF_RT + (size_t)Lay::H * 8,
+                            SMEM = OFF_BAR + 16;
+    static_assert(OFF_X % 16 == 0 && OFF_TQ % 16 == 0 && OFF_BAR % 16 == 0, "16-byte aligned regions");
+};
+
+template <int N, bool RSUM>
+__global__ void __launch_bounds__(128) k_rfft_fwd_fold_rf_p(const float *gp, float *fc, int nlat, long long lot,
+                                                             int kf, long long f_ms, long long nitems,
+                                                             const cpx<float> *__restrict__ w,
+                                                             const cpx<float> *__restrict__ rt, double *rowsum) {
+    using Lay = RfLayout<N>;
+    using PL = RfPLayout<N>;
+    constexpr int H = Lay::H, RB = Lay::RB, PR = RB / 2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cpx<float> *G = reinterpret_cast<cpx<float> *>(smraw), *X = reinterpret_cast<cpx<float> *>(smraw + PL::OFF_X);
+    cpx<float> *tqs = reinterpret_cast<cpx<float> *>(smraw + PL::OFF_TQ);
+    cpx<float> *rts = reinterpret_cast<cpx<float> *>(smraw + PL::OFF_RT);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + PL::OFF_BAR);
+    const int nlath = nlat / 2, nbpf = (nlath + PR - 1) / PR;
+    pdl_trigger();
+    if (threadIdx.x == 0) {
+        tc::mbar_init(bar, 1);
+        tc::mbar_fence_init();
+    }
+    for (int i = threadIdx.x; i < Lay::P * Lay::Q; i += blockDim.x) {
+        const int t = i / Lay::Q, q = i - t * Lay::Q;
+        tqs[t * Lay::RT + q] = w[t * q];   // t q < h
+    }
+    for (int k = threadIdx.x; k < H; k += blockDim.x) rts[k] = rt[k];
+    __syncthreads();
+    pdl_wait();   // the grid rows may come from the previous kernel, which may still read the output
+    auto grow_of = [&](long long item) {
+        const long long field = item / nbpf;
+        const int j0 = (int)(item - field * nbpf) * PR;
+        const bool fin = field * nlat < lot;
+        return [=](int r) {
+            const int j = j0 + (r % PR);
+            return (fin && j < nlath) ? field * nlat + (r < PR ? j : nlat - 1 - j) : -1ll;
+        };
+    };
+    long long item = blockIdx.x;
+    if (item < nitems) rf_issue_rows<N>(gp, grow_of(item), G, bar);
+    const float scale = 1.f / (float)N;
+    const int kh = min(H / 2, kf - 1);
+    for (uint32_t phase = 0; item < nitems; phase ^= 1) {
+        if (!rf_wait_loads(bar, phase)) return;
+        const long long next = item + gridDim.x;
+        double rs = 0.0;
+        const long long myrow = RSUM ? grow_of(item)(threadIdx.x / Lay::P) : -1ll;
+        rf_forward_core<N, RSUM>(G, X, tqs, [&] {
+            if (next < nitems) {
+                tc::fence_proxy_async();   // G was read (and zero rows written) through the generic proxy
+                rf_issue_rows<N>(gp, grow_of(next), G, bar);
+            }
+        }, &rs);
+        if (RSUM && myrow >= 0 && threadIdx.x % Lay::P == 0) rowsum[myrow] = rs;
+        const long long field = item / nbpf;
+        const int j0 = (int)(item - field * nbpf) * PR;
+        const bool fin = field * nlat < lot;
+        for (int it = threadIdx.x; it < PR * (kh + 1); it += blockDim.x) {
+            const int pr = it % PR, k = it / PR, k2 = H - k, j = j0 + pr;
+            if (!fin || j >= nlath) continue;
+            cpx<float> *fr = reinterpret_cast<cpx<float> *>(fc) + field * nlat + j;   // E row; O is nlath further
+            const cpx<float> *zn = X + pr * Lay::RZ, *zs = X + (pr + PR) * Lay::RZ;
+            const cpx<float> an = zn[k], as = zs[k];
+            if (k == 0) {
+                const cpx<float> xn{(an.x + an.y) * scale, 0.f}, xs{(as.x + as.y) * scale, 0.f};
+                fr[0] = cpx<float>{xn.x + xs.x, 0.f};
+                fr[nlath] = cpx<float>{xn.x - xs.x, 0.f};
+                continue;
+            }
+            const cpx<float> bn = zn[k2], bs = zs[k2], wk = rts[k];
+            cpx<float> xn = rf_split(an, bn, wk, scale), xs = rf_split(as, bs, wk, scale);
+            cpx<float> *fk = fr + (long long)k * f_ms;
+            fk[0] = cpx<float>{xn.x + xs.x, xn.y + xs.y};
+            fk[nlath] = cpx<float>{xn.x - xs.x, xn.y - xs.y};
+            if (k2 < kf && k2 != k) {
+                const cpx<float> wk2 = rts[k2];
+                xn = rf_split(bn, an, wk2, scale);
+                xs = rf_split(bs, as, wk2, scale);
+                fk = fr + (long long)k2 * f_ms;
+                fk[0] = cpx<float>{xn.x + xs.x, xn.y + xs.y};
+                fk[nlath] = cpx<float>{xn.x - xs.x, xn.y - xs.y};
+            }
+        }
+        __syncthreads();   // X is read before the next item's transposition writes it
+        item = next;
+    }
+}
+
 // rfft_inv_ct_body for the register-resident lengths: the block's
 // coefficients c_k (k < kf) are staged k-major in shared memory by plain
 // coalesced loads (a k's RB rows are one run of the m-major side); each thread
@@ -954,6 +1097,121 @@ __device__ __forceinline__ void rfft_inv_rf_body(const float *fc, float *gp, lon
     if (threadIdx.x < rows) {
         bulk_s2g(gp + (row0 + threadIdx.x) * N, S.r + threadIdx.x * Lay::RG, N * 4);
         bulk_commit_wait_read();
+    }
+}
+
+// Persistent form of rfft_inv_rf_body.  A block sets up its twiddle tables
+// once and walks the items blk = blockIdx.x, + gridDim.x, ... (RB rows each).
+// The coefficients are staged k-major in their own region C by asynchronous
+// 8-byte copies (cp.async), so the next item's copies are issued as soon as
+// this item's coefficients are read and arrive while it is transformed and
+// stored; the transposition and the staged grid rows use a second region.
+__device__ __forceinline__ void cp_async8(void *dst_smem, const void *src_gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(tc::smem_u32(dst_smem)), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <int N> struct RfIPLayout {
+    using Lay = RfLayout<N>;
+    static constexpr int RW = Lay::RS > Lay::RG ? Lay::RS : Lay::RG;
+    // C takes kf x RC complex values (kf <= H); then the work region, the twiddle tables
+    static __host__ __device__ size_t off_w(int kf) { return ((size_t)kf * Lay::RC * 8 + 15) & ~(size_t)15; }
+    static __host__ __device__ size_t off_tq(int kf) { return off_w(kf) + (size_t)Lay::RB * RW * 8; }
+    static __host__ __device__ size_t off_rt(int kf) { return off_tq(kf) + (size_t)Lay::P * Lay::RT * 8; }
+    static __host__ __device__ size_t smem(int kf) { return off_rt(kf) + (size_t)Lay::H * 8; }
+};
+
+template <int N>
+__global__ void __launch_bounds__(128) k_rfft_inv_rf_p(const float *fc, float *gp, long long lot, int kf,
+                                                        long long f_rs, long long f_ms, long long nitems,
+                                                        const cpx<float> *__restrict__ w,
+                                                        const cpx<float> *__restrict__ rt) {
+    using Lay = RfLayout<N>;
+    using PL = RfIPLayout<N>;
+    constexpr int P = Lay::P, Q = Lay::Q, H = Lay::H, RB = Lay::RB, QP = Q / P;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cpx<float> *cs = reinterpret_cast<cpx<float> *>(smraw);   // c_k of row r at cs[k * RC + r]
+    cpx<float> *wk_s = reinterpret_cast<cpx<float> *>(smraw + PL::off_w(kf));
+    cpx<float> *tqs = reinterpret_cast<cpx<float> *>(smraw + PL::off_tq(kf));
+    cpx<float> *rts = reinterpret_cast<cpx<float> *>(smraw + PL::off_rt(kf));
+    const int t = threadIdx.x % P, r = threadIdx.x / P;
+    pdl_trigger();
+    for (int i = threadIdx.x; i < P * Q; i += blockDim.x) {
+        const int tt = i / Q, q = i - tt * Q;
+        tqs[tt * Lay::RT + q] = w[tt * q];   // t q < h
+    }
+    for (int k = threadIdx.x; k < H; k += blockDim.x) rts[k] = rt[k];
+    pdl_wait();   // the coefficients come from the previous kernel
+    const cpx<float> *fcc = reinterpret_cast<const cpx<float> *>(fc);
+    auto issue = [&](long long item) {
+        const long long row0 = item * RB;
+        const int rows = (int)min((long long)RB, lot - row0);
+        for (int i = threadIdx.x; i < kf * RB; i += blockDim.x) {
+            const int k = i / RB, rr = i - k * RB;
+            cpx<float> *dst = cs + k * Lay::RC + rr;
+            if (rr < rows) cp_async8(dst, fcc + (row0 + rr) * f_rs + (long long)k * f_ms);
+            else *dst = cpx<float>{0.f, 0.f};
+        }
+        cp_async_commit();
+    };
+    long long item = blockIdx.x;
+    if (item < nitems) issue(item);
+    for (; item < nitems; item += gridDim.x) {
+        const long long row0 = item * RB;
+        const int rows = (int)min((long long)RB, lot - row0);
+        cp_async_wait_all();
+        __syncthreads();   // this item's coefficients are in; the previous item's grid rows have left
+        cpx<float> z[QP][P];
+#pragma unroll
+        for (int i = 0; i < QP; i++) {
+            const int q = QP * t + i;
+#pragma unroll
+            for (int m = 0; m < P; m++) {
+                const int k = q + Q * m, k2 = H - k;
+                cpx<float> a{0.f, 0.f}, b{0.f, 0.f};
+                if (k < kf) {
+                    a = cs[k * Lay::RC + r];
+                    if (k == 0) a.y = 0.f;
+                }
+                if (k > 0 && k2 < kf) b = cs[k2 * Lay::RC + r];
+                // Z_k of the half-length complex sequence (c = 0 for k >= kf, the m = 0 imaginary part ignored)
+                const cpx<float> E{a.x + b.x, a.y - b.y}, D{a.x - b.x, a.y + b.y};
+                cpx<float> wk = rts[k];
+                wk.y = -wk.y;
+                const cpx<float> O = cmul(D, wk);
+                z[i][m] = cpx<float>{E.x - O.y, E.y + O.x};
+            }
+            dft8<float, +1>(z[i]);
+        }
+        __syncthreads();   // the staged coefficients are read: the next item's copies may land
+        if (item + gridDim.x < nitems) issue(item + gridDim.x);
+        cpx<float> *x = wk_s + r * Lay::RS;
+#pragma unroll
+        for (int i = 0; i < QP; i++)
+#pragma unroll
+            for (int u = 0; u < P; u++) x[u * Lay::RT + QP * t + i] = z[i][u];
+        __syncthreads();
+        cpx<float> v[Q];
+        const cpx<float> *tq = tqs + t * Lay::RT;
+#pragma unroll
+        for (int q = 0; q < Q; q += 2) {
+            const float4 f = *reinterpret_cast<const float4 *>(x + t * Lay::RT + q);
+            const float4 wq = *reinterpret_cast<const float4 *>(tq + q);
+            v[q] = q ? cmul(cpx<float>{f.x, f.y}, cpx<float>{wq.x, -wq.y}) : cpx<float>{f.x, f.y};
+            v[q + 1] = cmul(cpx<float>{f.z, f.w}, cpx<float>{wq.z, -wq.w});
+        }
+        dftQ<float, +1, Q>(v);
+        __syncthreads();   // the transposition is read; the grid rows are staged over it
+        cpx<float> *gs = wk_s + r * Lay::RG + t;
+#pragma unroll
+        for (int j = 0; j < Q; j++) gs[P * j] = v[j];
+        tc::fence_proxy_async();   // the staged rows feed the bulk stores
+        __syncthreads();
+        if (threadIdx.x < rows) {
+            bulk_s2g(gp + (row0 + threadIdx.x) * N, wk_s + threadIdx.x * Lay::RG, N * 4);
+            bulk_commit_wait_read();
+        }
     }
 }
 
@@ -1119,6 +1377,16 @@ static exotx_status launch_ct(bool fwd, const T *in, T *out, long long lot, int 
     return EXOTX_OK;
 }
 
+// blocks of a kernel resident on the whole device at once (SMs x blocks per SM)
+static exotx_status resident_slots(const void *kernel, int threads, size_t smem, int *slots) {
+    int dev = 0, occ = 0, nsm = 0;
+    EXOTX_CUDA(cudaGetDevice(&dev));
+    EXOTX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem));
+    EXOTX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    *slots = nsm * (occ < 1 ? 1 : occ);
+    return EXOTX_OK;
+}
+
 template <int N>
 static exotx_status launch_rf(bool fwd, const float *in, float *out, long long lot, int kf, long long f_rs,
                               long long f_ms, const cpx<float> *w, const cpx<float> *r, cudaStream_t s) {
@@ -1127,12 +1395,24 @@ static exotx_status launch_rf(bool fwd, const float *in, float *out, long long l
     const int kid = fwd ? EXOTX_K_FFT_FORWARD : EXOTX_K_FFT_INVERSE;
     if (fwd)
         EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_rf<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM));
-    else
+    else if (kf > Lay::H)
         EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_inv_rf<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM));
+    long long grid = nb;
+    size_t smem_p = 0;
+    if (!fwd && kf <= Lay::H) {   // persistent form: one block per resident slot
+        smem_p = RfIPLayout<N>::smem(kf);
+        EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_inv_rf_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_p));
+        int slots = 0;
+        EXOTX_TRY(resident_slots((const void *)k_rfft_inv_rf_p<N>, Lay::NT, smem_p, &slots));
+        grid = std::min<long long>(nb, slots);
+    }
     cudaEvent_t ev = ktimer_start(kid, s);
     if (fwd)
         EXOTX_CUDA(launch_pdl(k_rfft_fwd_rf<N>, dim3((unsigned)nb), dim3(Lay::NT), Lay::SMEM, s, in, out, lot, kf, f_rs,
                               f_ms, w, r));
+    else if (smem_p)
+        EXOTX_CUDA(launch_pdl(k_rfft_inv_rf_p<N>, dim3((unsigned)grid), dim3(Lay::NT), smem_p, s, in, out, lot, kf,
+                              f_rs, f_ms, nb, w, r));
     else
         EXOTX_CUDA(launch_pdl(k_rfft_inv_rf<N>, dim3((unsigned)nb), dim3(Lay::NT), Lay::SMEM, s, in, out, lot, kf, f_rs,
                               f_ms, w, r));
@@ -1305,16 +1585,21 @@ template exotx_status fft_forward_l<float>(const float *, float *, int, long lon
 
 template <int N>
 static exotx_status launch_fold(const float *in, float *out, int nlat, long long lot, int kf, long long f_ms,
-                                const cpx<float> *w, const cpx<float> *r, cudaStream_t s) {
+                                const cpx<float> *w, const cpx<float> *r, double *rowsum, cudaStream_t s) {
+    if (rowsum && !rf_len<N>()) return EXOTX_NOT_BUILT;
     if constexpr (rf_len<N>()) {
         using Lay = RfLayout<N>;
+        using PL = RfPLayout<N>;
         const int nbpf = (nlat / 2 + Lay::RB / 2 - 1) / (Lay::RB / 2);
         const long long nb = (lot / nlat) * nbpf;
-        EXOTX_CUDA(cudaFuncSetAttribute(k_rfft_fwd_fold_rf<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)Lay::SMEM));
+        auto kern = rowsum ? k_rfft_fwd_fold_rf_p<N, true> : k_rfft_fwd_fold_rf_p<N, false>;
+        EXOTX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
+        int slots = 0;
+        EXOTX_TRY(resident_slots((const void *)kern, Lay::NT, PL::SMEM, &slots));
+        const long long grid = std::min<long long>(nb, slots);
         cudaEvent_t ev = ktimer_start(EXOTX_K_FFT_FORWARD, s);
-        EXOTX_CUDA(launch_pdl(k_rfft_fwd_fold_rf<N>, dim3((unsigned)nb), dim3(Lay::NT), Lay::SMEM, s, in, out, nlat, lot,
-                              kf, f_ms, w, r));
+        EXOTX_CUDA(launch_pdl(kern, dim3((unsigned)grid), dim3(Lay::NT), PL::SMEM, s, in, out, nlat, lot, kf, f_ms, nb,
+                              w, r, rowsum));
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_FFT_FORWARD, s, ev);
         return EXOTX_OK;
@@ -1337,8 +1622,10 @@ static exotx_status launch_fold(const float *in, float *out, int nlat, long long
 // forward transform of lot = fields x nlat grid rows of length n = 2 nlat into
 // the equator-folded m-major layout (rfft_fwd_fold_body); EXOTX_NOT_BUILT when
 // n has no specialised kernel or the buffers are not 16-byte aligned
+bool fft_fold_rowsum(int n) { return n == 384; }   // the register-resident lengths (RfShape)
+
 exotx_status fft_forward_fold(const float *in, float *out, int n, int nlat, long long lot, int kf, long long f_ms,
-                              cudaStream_t s) {
+                              double *rowsum, cudaStream_t s) {
     if (n != 2 * nlat || nlat < 2 || lot % nlat) return EXOTX_BAD_ARG;
     exotx_status st;
     const FftTables *t = fft_tables(n, &st);
@@ -1347,13 +1634,13 @@ exotx_status fft_forward_fold(const float *in, float *out, int n, int nlat, long
     if (!aligned16(in) || !aligned16(out)) return EXOTX_NOT_BUILT;
     const cpx<float> *w = wt<float>(t), *r = rt<float>(t);
     switch (n) {
-        case 64: return launch_fold<64>(in, out, nlat, lot, kf, f_ms, w, r, s);
-        case 128: return launch_fold<128>(in, out, nlat, lot, kf, f_ms, w, r, s);
-        case 192: return launch_fold<192>(in, out, nlat, lot, kf, f_ms, w, r, s);
-        case 256: return launch_fold<256>(in, out, nlat, lot, kf, f_ms, w, r, s);
-        case 320: return launch_fold<320>(in, out, nlat, lot, kf, f_ms, w, r, s);
-        case 384: return launch_fold<384>(in, out, nlat, lot, kf, f_ms, w, r, s);
-        case 512: return launch_fold<512>(in, out, nlat, lot, kf, f_ms, w, r, s);
+        case 64: return launch_fold<64>(in, out, nlat, lot, kf, f_ms, w, r, rowsum, s);
+        case 128: return launch_fold<128>(in, out, nlat, lot, kf, f_ms, w, r, rowsum, s);
+        case 192: return launch_fold<192>(in, out, nlat, lot, kf, f_ms, w, r, rowsum, s);
+        case 256: return launch_fold<256>(in, out, nlat, lot, kf, f_ms, w, r, rowsum, s);
+        case 320: return launch_fold<320>(in, out, nlat, lot, kf, f_ms, w, r, rowsum, s);
+        case 384: return launch_fold<384>(in, out, nlat, lot, kf, f_ms, w, r, rowsum, s);
+        case 512: return launch_fold<512>(in, out, nlat, lot, kf, f_ms, w, r, rowsum, s);
     }
     return EXOTX_NOT_BUILT;
 }

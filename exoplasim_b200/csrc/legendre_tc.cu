@@ -518,6 +518,130 @@ exotx_status tc_inverse_batch_d(exotx_plan p, const float *spin, float *gpout, i
     return tc_inverse_run(p, spin, gpout, L, ninst, 1, s);
 }
 
+// The global means (the n = 0 coefficients) of the mixed forward set in FP64.
+// For m = n = 0 the tables qe, qm and qq vanish (Q_00 = 0, m = 0, n(n+1) = 0),
+// so mktend's temperature, qtend's humidity and fc2sp(gvpp) reduce to
+// sum_lat qc_00(lat) A0(lat) skgpsp(0), A0 the zonal mean of the grid row
+// (fc2sp legmod.f90:178-223, mktend :555-602).  One block per (instance,
+// field) sums its grid rows in FP64 from the FP32 grid input and overwrites
+// the coefficient the tensor cores wrote: the model's mass (ln ps) and
+// energy budgets then close in FP64 (the reference keeps spp(1:2) conserved,
+// plasim.f90:2937-2938).  Field f of an instance: 0..L-1 temperature, L..2L-1
+// humidity, 2L the ln ps tendency (gridpointa only).  One launch covers the
+// segments of an ensemble as well.
+struct N0Seg {
+    const float *gpin;
+    const double *rowsum; // FP64 grid-row sums from the forward FFT (may be null: summed here)
+    float *spout;
+    const double *qc00;   // qc(w = 0, lat), stride qstride
+    const double *fg;     // skgpsp
+    int qstride, L, nfi, nfo, nlat, nlon, nrsp, dset, nf, blk0;
+};
+struct N0Launch {
+    N0Seg seg[TC_MAXSEG];
+    int nseg;
+};
+
+constexpr int N0_MAXLAT = 1024;
+
+__global__ void __launch_bounds__(256) k_n0_fp64(const __grid_constant__ N0Launch P) {
+    __shared__ double rs[N0_MAXLAT];
+    pdl_trigger();
+    int si = 0;
+    while (si + 1 < P.nseg && (int)blockIdx.x >= P.seg[si + 1].blk0) si++;
+    const N0Seg &S = P.seg[si];
+    const int b = blockIdx.x - S.blk0, L = S.L;
+    const int inst = b / S.nf, f = b - inst * S.nf;
+    int fin, fout;
+    if (f < L) { fin = f; fout = L + f; }                                    // tn (gtdt) -> stf
+    else if (f < 2 * L) { fin = S.dset ? 2 * L + f : f; fout = 2 * L + f; }  // qn (gqdt) -> sqf
+    else { fin = 7 * L; fout = 4 * L; }                                      // gvpp -> spf
+    const long long row0 = ((long long)inst * S.nfi + fin) * S.nlat;
+    pdl_wait();   // the grid, the row sums and the tensor cores' outputs come from earlier kernels
+    if (S.rowsum) {
+        for (int lat = threadIdx.x; lat < S.nlat; lat += blockDim.x) rs[lat] = S.rowsum[row0 + lat];
+    } else {
+        // eight lanes per row in the order of the forward FFT's row sums: lane t
+        // adds the complex elements t + 8 j (real part first), then an xor butterfly
+        const int t = threadIdx.x & 7, g = threadIdx.x >> 3, ng = blockDim.x >> 3, h = S.nlon / 2;
+        for (int lat0 = 0; lat0 < S.nlat; lat0 += ng) {
+            const int lat = lat0 + g;
+            double a = 0.0;
+            if (lat < S.nlat) {
+                const float2 *row = reinterpret_cast<const float2 *>(S.gpin + (size_t)(row0 + lat) * S.nlon);
+                for (int e = t; e < h; e += 8) {
+                    const float2 x = row[e];
+                    a += (double)x.x;
+                    a += (double)x.y;
+                }
+            }
+            for (int o = 1; o < 8; o <<= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+            if (lat < S.nlat && t == 0) rs[lat] = a;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double acc = 0.0;
+        for (int lat = threadIdx.x; lat < S.nlat; lat += 32) acc += S.qc00[(size_t)lat * S.qstride] * (rs[lat] / (double)S.nlon);
+        for (int o = 1; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) {
+            float *o = S.spout + ((size_t)inst * S.nfo + fout) * S.nrsp;
+            o[0] = (float)(acc * S.fg[0]);
+            o[1] = 0.0f;
+        }
+    }
+}
+
+static void n0_seg(N0Seg &g, exotx_plan p, const float *gpin, const double *rowsum, float *spout, int L, int dset,
+                   int blk0) {
+    g.gpin = gpin;
+    g.rowsum = rowsum;
+    g.spout = spout;
+    // qc(w = 0, lat) of the FP64 reference tables [t][lat][w] (qc is table 2)
+    g.qc00 = p->d_qref + (size_t)2 * p->nlat * p->ncsp;
+    g.qstride = p->ncsp;
+    g.fg = p->d_fg64;
+    g.L = L;
+    g.nfi = dset ? 4 * L : 9 * L + 1;
+    g.nfo = dset ? 4 * L : 4 * L + 1;
+    g.nlat = p->nlat;
+    g.nlon = p->nlon;
+    g.nrsp = 2 * p->ncsp;
+    g.dset = dset;
+    g.nf = dset ? 2 * L : 2 * L + 1;
+    g.blk0 = blk0;
+}
+
+static exotx_status n0_launch(const N0Launch &P, int nblk, cudaStream_t s) {
+    if (nblk == 0) return EXOTX_OK;
+    for (int i = 0; i < P.nseg; i++)
+        if (P.seg[i].nlat > N0_MAXLAT) return EXOTX_BAD_DIM;
+    EXOTX_CUDA(launch_pdl(k_n0_fp64, dim3((unsigned)nblk), dim3(256), 0, s, P));
+    EXOTX_CHECK_LAUNCH();
+    return EXOTX_OK;
+}
+
+static exotx_status n0_fp64(exotx_plan p, const float *gsrc, const double *rowsum, float *sout, int L, int ni,
+                            int dset, cudaStream_t s) {
+    N0Launch P;
+    P.nseg = 1;
+    n0_seg(P.seg[0], p, gsrc, rowsum, sout, L, dset, 0);
+    return n0_launch(P, ni * P.seg[0].nf, s);
+}
+
+// the FP64 global means of every segment of an ensemble's forward set (gridpointa)
+exotx_status tc_ens_n0(const EnsSeg *segs, const float *const *gpin, int nseg, cudaStream_t s) {
+    if (nseg < 1 || nseg > TC_MAXSEG) return EXOTX_BAD_ARG;
+    N0Launch P;
+    P.nseg = nseg;
+    int nblk = 0;
+    for (int i = 0; i < nseg; i++) {
+        n0_seg(P.seg[i], segs[i].p, gpin[i], nullptr, segs[i].spout, segs[i].L, 0, nblk);
+        nblk += segs[i].ninst * P.seg[i].nf;
+    }
+    return n0_launch(P, nblk, s);
+}
+
 static exotx_status tc_forward_run(exotx_plan p, const float *gpin, float *spout, int L, int ninst, int dset,
                                    cudaStream_t s) {
     TcTables *T;
@@ -527,7 +651,11 @@ static exotx_status tc_forward_run(exotx_plan p, const float *gpin, float *spout
     const size_t per_inst = (size_t)nfi * p->nlat * p->ntp1 * sizeof(float2);
     int chunk = (int)std::max<size_t>(1, p->chunk_fwd / per_inst);
     chunk = std::min(chunk, ninst);
-    EXOTX_TRY(ensure_work(p, per_inst * chunk));
+    // the FP64 grid-row sums of the n = 0 coefficients follow the intermediate,
+    // where the folded FFT forms them (register-resident lengths)
+    const bool with_rs = fft_fold_rowsum(p->nlon);
+    const size_t rs_off = (per_inst * chunk + 255) & ~(size_t)255;
+    EXOTX_TRY(ensure_work(p, with_rs ? rs_off + (size_t)chunk * nfi * p->nlat * sizeof(double) : per_inst * chunk));
     const int4 *jobs;
     int njobs;
     EXOTX_TRY(tc_jobs(p, T, 1, L, chunk, &jobs, &njobs));
@@ -545,11 +673,14 @@ static exotx_status tc_forward_run(exotx_plan p, const float *gpin, float *spout
         // the persistent kernel reads the intermediate folded about the equator where
         // the grid length has a specialised FFT; otherwise as north and south rows
         bool folded = false;
+        double *rowsum = nullptr;
         if (v3) {
+            double *rs = with_rs ? reinterpret_cast<double *>(static_cast<char *>(p->d_work) + rs_off) : nullptr;
             const exotx_status sf = fft_forward_fold(gsrc, (float *)p->d_work, p->nlon, p->nlat, nrows, p->ntp1,
-                                                     nrows, s);
+                                                     nrows, rs, s);
             if (sf != EXOTX_OK && sf != EXOTX_NOT_BUILT) return sf;
             folded = sf == EXOTX_OK;
+            if (folded) rowsum = rs;
         }
         if (!folded)
             EXOTX_TRY(fft_forward_l<float>(gsrc, (float *)p->d_work, p->nlon, nrows, p->ntp1, 1, nrows, s));
@@ -560,6 +691,7 @@ static exotx_status tc_forward_run(exotx_plan p, const float *gpin, float *spout
             fwd3_args(P3.seg[0], p, T, L, (const float2 *)p->d_work, nrows, spout + (size_t)i0 * nfo * nrsp);
             P3.seg[0].dset = dset;
             EXOTX_TRY(launch_fwd_pipe(P3, nj, T->njc, folded, s));
+            EXOTX_TRY(n0_fp64(p, gsrc, rowsum, spout + (size_t)i0 * nfo * nrsp, L, ni, dset, s));
             continue;
         }
         TcFwdLaunch P;
@@ -575,6 +707,7 @@ static exotx_status tc_forward_run(exotx_plan p, const float *gpin, float *spout
         A.L = L; A.nlat = p->nlat; A.nlath = p->nlath; A.njc = T->njc; A.ntp1 = p->ntp1; A.nrsp = (int)nrsp;
         A.dset = dset;
         EXOTX_TRY(launch_fwd(P, lv, nj, smem, s));
+        EXOTX_TRY(n0_fp64(p, gsrc, nullptr, spout + (size_t)i0 * nfo * nrsp, L, ni, dset, s));
     }
     return EXOTX_OK;
 }

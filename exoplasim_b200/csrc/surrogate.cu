@@ -210,14 +210,16 @@ __global__ void k_silu_bwd(const float *dH, const float *Z, float *dZ, long long
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         dZ[i] = dH[i] * silu_grad(Z[i]);
 }
-// mean squared error over n x nout; dY = d(loss)/dY; loss accumulated into *loss
-__global__ void k_mse(const float *Y, const float *T, float *dY, long long n, float scale, float *loss) {
+// mean (optionally weighted: Wt per element, may be null) squared error over
+// n x nout; dY = d(loss)/dY; loss accumulated into *loss
+__global__ void k_mse(const float *Y, const float *T, const float *Wt, float *dY, long long n, float scale,
+                      float *loss) {
     __shared__ float red[256];
     float acc = 0.f;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const float d = Y[i] - T[i];
-        dY[i] = 2.f * d * scale;
-        acc += d * d;
+        const float d = Y[i] - T[i], w = Wt ? Wt[i] : 1.f;
+        dY[i] = 2.f * w * d * scale;
+        acc += w * d * d;
     }
     red[threadIdx.x] = acc;
     __syncthreads();
@@ -713,11 +715,16 @@ EXOTX_API exotx_status exotx_mlp_forward(exotx_mlp net, const float *X, float *Y
 
 EXOTX_API exotx_status exotx_mlp_backward(exotx_mlp net, const float *X, const float *Tt, int n, float *loss,
                                           exotx_stream sv) {
+    return exotx_mlp_backward_weighted(net, X, Tt, nullptr, n, loss, sv);
+}
+
+EXOTX_API exotx_status exotx_mlp_backward_weighted(exotx_mlp net, const float *X, const float *Tt, const float *Wt,
+                                                   int n, float *loss, exotx_stream sv) {
     if (!net || !X || !Tt || n < 1 || n > net->maxb) return EXOTX_BAD_ARG;
     cudaStream_t s = (cudaStream_t)sv;
     EXOTX_TRY(mlp_forward(net, X, n, s));
     const long long ny = (long long)n * net->nout;
-    k_mse<<<grid_for(ny), 256, 0, s>>>(ws_Y(net), Tt, ws_dY(net), ny, 1.f / (float)ny, loss);
+    k_mse<<<grid_for(ny), 256, 0, s>>>(ws_Y(net), Tt, Wt, ws_dY(net), ny, 1.f / (float)ny, loss);
     EXOTX_CHECK_LAUNCH();
     const float *dZ = ws_dY(net);
     int cur = 0;

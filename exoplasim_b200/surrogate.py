@@ -117,10 +117,15 @@ class Mlp:
         call("exotx_mlp_forward", self._h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), n, _stream())
         return Y
 
-    def backward(self, X, T, loss):
-        """Gradients of the mean squared error of rows X against T; loss (device) += it."""
-        call("exotx_mlp_backward", self._h, C.c_void_p(X.data_ptr()), C.c_void_p(T.data_ptr()), X.shape[0],
-             C.c_void_p(loss.data_ptr()), _stream())
+    def backward(self, X, T, loss, W=None):
+        """Gradients of the mean squared error of rows X against T, each element's
+        squared error weighted by W (same shape) when given; loss (device) += it."""
+        if W is None:
+            call("exotx_mlp_backward", self._h, C.c_void_p(X.data_ptr()), C.c_void_p(T.data_ptr()), X.shape[0],
+                 C.c_void_p(loss.data_ptr()), _stream())
+        else:
+            call("exotx_mlp_backward_weighted", self._h, C.c_void_p(X.data_ptr()), C.c_void_p(T.data_ptr()),
+                 C.c_void_p(W.data_ptr()), X.shape[0], C.c_void_p(loss.data_ptr()), _stream())
 
     def adam(self, lr, step, b1=0.9, b2=0.999, eps=1e-8):
         call("exotx_mlp_adam", self._h, C.c_float(lr), C.c_float(b1), C.c_float(b2), C.c_float(eps), step,
@@ -213,13 +218,29 @@ def norm_stats(X, Y, margin=0.02):
 
 
 # ------------------------------------------------------------------ training
-def train(net, X, Y, epochs=16, batch=4096, lr=1e-3, lr_min=1e-5, seed=0, log=None):
-    """Adam over normalised (X, Y) on the device; cosine learning-rate decay."""
+def judged_weights(X, nlev, ys, adv, flux_k_per_day_per_w=0.1):
+    """Per-element loss weights that make the training loss the squared error in
+    the units the surrogate is judged in: a normalised heating output's error e
+    is e * ys / ((ps / 1e5)(1 + ADV q)) K/day, so its weight is that factor
+    squared; a surface flux's error of 1 W/m2 counts as flux_k_per_day_per_w
+    K/day.  Scaled to mean 1."""
+    L = nlev
+    hs = heating_scale(X, L, adv).float()
+    W = torch.empty((X.shape[0], L + 4), dtype=torch.float32, device=X.device)
+    W[:, :L] = (ys[:L] / hs) ** 2
+    W[:, L:] = (flux_k_per_day_per_w * ys[L:]) ** 2
+    return (W / W.mean()).contiguous()
+
+
+def train(net, X, Y, epochs=16, batch=4096, lr=1e-3, lr_min=1e-5, seed=0, log=None, weighted=False, adv=None):
+    """Adam over normalised (X, Y) on the device; cosine learning-rate decay.
+    weighted: the loss of judged_weights (needs the radiation constant adv)."""
     n = X.shape[0]
     xm = torch.as_tensor(net.norm["xm"], device="cuda")
     xs = torch.as_tensor(net.norm["xs"], device="cuda")
     ym = torch.as_tensor(net.norm["ym"], device="cuda")
     ys = torch.as_tensor(net.norm["ys"], device="cuda")
+    Wt = judged_weights(X, net.nout - 4, ys, adv) if weighted else None
     Xn = ((X - xm) / xs).contiguous()
     Yn = ((Y - ym) / ys).contiguous()
     gen = torch.Generator(device="cuda")
@@ -237,9 +258,10 @@ def train(net, X, Y, epochs=16, batch=4096, lr=1e-3, lr_min=1e-5, seed=0, log=No
             idx = perm[b * batch:(b + 1) * batch]
             xb = Xn.index_select(0, idx)
             yb = Yn.index_select(0, idx)
+            wb = Wt.index_select(0, idx) if Wt is not None else None
             step += 1
             rate = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * step / total))
-            net.backward(xb, yb, loss)
+            net.backward(xb, yb, loss, wb)
             net.adam(rate, step)
         ep_loss = loss.item() / steps_per_epoch
         hist.append(ep_loss)
@@ -297,6 +319,27 @@ def evaluate(net, nlev=20, seed=900000, nchunk=4, precision="fp64"):
             "columns": ncol}
 
 
+def fallback_curve(net, ps_min_list, nlev=20, seed=900000, nchunk=4):
+    """Heating RMS against the fallback fraction when columns with surface
+    pressure below ps_min go to the plain radstep kernel: the range test of
+    exotx_rad_surrogate with the lower bound of the ln ps feature raised to
+    ln(ps_min).  Returns [(ps_min, fallback fraction, heating RMS K/day,
+    surface-flux RMS W/m2)]; the network's own ranges are restored after."""
+    nrm = {k: v.copy() for k, v in net.norm.items()}
+    ips = 3 * nlev + 2
+    rows = []
+    try:
+        for pmin in ps_min_list:
+            xlo = nrm["xlo"].copy()
+            xlo[ips] = max(xlo[ips], math.log(pmin)) if pmin > 0 else xlo[ips]
+            net.set_norm(nrm["xm"], nrm["xs"], xlo, nrm["xhi"], nrm["ym"], nrm["ys"])
+            ev = evaluate(net, nlev, seed, nchunk)
+            rows.append((pmin, ev["fallback_fraction"], ev["heating_rms_K_per_day"], ev["surface_flux_rms_W_m2"]))
+    finally:
+        net.set_norm(nrm["xm"], nrm["xs"], nrm["xlo"], nrm["xhi"], nrm["ym"], nrm["ys"])
+    return rows
+
+
 def main():
     a = argparse.ArgumentParser()
     a.add_argument("--train", required=True, help="output .npz")
@@ -306,6 +349,7 @@ def main():
     a.add_argument("--lr", type=float, default=1e-3)
     a.add_argument("--nlev", type=int, default=20)
     a.add_argument("--seed", type=int, default=0)
+    a.add_argument("--weighted", action="store_true", help="loss in K/day (and W/m2) instead of normalised units")
     args = a.parse_args()
     t0 = time.time()
     X, Y = dataset(args.columns, args.nlev, seed=1000)
@@ -313,8 +357,9 @@ def main():
     net = Mlp(nin_for(args.nlev), nout_for(args.nlev), max_batch=args.batch)
     net.init(args.seed)
     net.set_norm(*norm_stats(X, Y))
+    adv = R.default_params(args.nlev, 2 * GRID_NLAT * GRID_NLAT, 2 * GRID_NLAT).adv
     hist = train(net, X, Y, epochs=args.epochs, batch=args.batch, lr=args.lr,
-                 log=lambda s: print(s, flush=True))
+                 log=lambda s: print(s, flush=True), weighted=args.weighted, adv=adv)
     ev = evaluate(net, args.nlev)
     print(ev, flush=True)
     net.save(args.train, loss=np.array(hist), columns=X.shape[0], epochs=args.epochs,

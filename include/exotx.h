@@ -78,10 +78,12 @@ exotx_status exotx_plan_table(exotx_plan p, int which, double *out);
  * the bytes of m-major Fourier intermediate one inverse (forward) launch
  * covers -- instances are grouped up to it, at least one per launch -- so that
  * the intermediate one kernel writes is still in L2 when the next reads it.
- * Default 80 MB each. */
-/* EXOTX_TUNE_INV_HALF: 1 (default) lets the inverse kernel run two CTAs
- * per SM, each holding one parity half of a table, where they fit shared
- * memory; 0 keeps one CTA per SM with both halves. */
+ * Default 512 MB each: fewer, larger launches measured faster than L2-sized
+ * ones at T127 L20. */
+/* EXOTX_TUNE_INV_HALF: 1 lets the inverse kernel run two CTAs per SM, each
+ * holding one parity half of a table, where they fit shared memory; 0 (the
+ * default: the two measured alike at T127 L20) keeps one CTA per SM with both
+ * halves. */
 typedef enum { EXOTX_TUNE_CHUNK_INV = 0, EXOTX_TUNE_CHUNK_FWD = 1, EXOTX_TUNE_INV_HALF = 2 } exotx_tune_key;
 exotx_status exotx_plan_tune(exotx_plan p, int key, long long value);
 
@@ -397,6 +399,10 @@ exotx_status exotx_mlp_forward(exotx_mlp net, const float *X, float *Y, int n, e
  * gradients land in the net's gradient array; *loss (device) += the loss */
 exotx_status exotx_mlp_backward(exotx_mlp net, const float *X, const float *T, int n, float *loss,
                                 exotx_stream s);
+/* the same with the squared error of element (b, o) weighted by W[b * nout + o]
+ * (device, n x nout; NULL = all 1): a loss in the units the outputs are judged in */
+exotx_status exotx_mlp_backward_weighted(exotx_mlp net, const float *X, const float *T, const float *W, int n,
+                                         float *loss, exotx_stream s);
 exotx_status exotx_mlp_adam(exotx_mlp net, float lr, float beta1, float beta2, float eps, int step,
                             exotx_stream s);
 /* BF16 tensor-core copy of the current weights (width 256, nin <= 80, nout <= 32) */

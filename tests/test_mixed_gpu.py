@@ -72,3 +72,73 @@ def test_mixed_batch_matches_single(plans):
         assert torch.equal(gb[i], g1)
         assert torch.equal(sb[i], s1)
     assert tc_error() == 0
+
+
+def _fp64_rounded_once(x, ref):
+    # x is the FP64 value ref rounded once to the float32 output: within half
+    # a float32 ulp of it (plus FP64 summation-order noise), where a sum in
+    # FP32 or on the tensor cores lands several ulps away
+    return abs(x - ref) <= 0.5 * float(np.spacing(np.float32(abs(ref)))) + 1e-14 * abs(ref)
+
+
+@pytest.mark.parametrize("nlat", [64, 192])
+def test_mixed_global_means_are_fp64(oracle, nlat):
+    # the n = 0 coefficients of the forward set (temperature, humidity, ln ps
+    # tendencies) are summed in FP64 on the mixed path and rounded once to the
+    # float32 output; at NLON 384 from the row sums the forward FFT forms,
+    # elsewhere from the grid
+    nlev = 10
+    P = Plan(nlat)
+    L = oracle.Leg(nlat)
+    gin = S.grid_tendencies(nlat, nlev, seed=21)
+    gin[:nlev] += 0.3          # tn with a global mean well above its variance
+    gin[7 * nlev] += 0.02      # gvpp
+    g32 = torch.as_tensor(gin, device="cuda").float()
+    refs = L.forward_set(g32.double().cpu().numpy().reshape(9 * nlev + 1, -1), nlev)
+    sp = P.forward_set(g32, nlev, precision="mixed").double().cpu().numpy()
+    for f in list(range(nlev, 2 * nlev)) + list(range(3 * nlev, 4 * nlev)) + [4 * nlev]:
+        assert _fp64_rounded_once(sp[f][0], refs[f][0]), (f, sp[f][0], refs[f][0])
+        assert sp[f][1] == 0.0
+    # the vorticity and divergence have no n = 0 mode
+    for f in list(range(0, nlev)) + list(range(2 * nlev, 3 * nlev)):
+        assert sp[f][0] == 0.0 and sp[f][1] == 0.0
+
+
+def test_mixed_d_set_global_means_are_fp64(oracle):
+    # the gridpointd forward set's temperature and humidity tendencies
+    # (fc2sp of gtdt, gqdt) carry FP64 n = 0 coefficients as well
+    nlat, nlev = 64, 10
+    P = Plan(nlat)
+    L = oracle.Leg(nlat)
+    rng = np.random.default_rng(22)
+    gin = rng.standard_normal((4 * nlev, nlat, 2 * nlat)) * 1e-5
+    gin[:nlev] += 2e-5          # gtdt with a nonzero global mean
+    gin[3 * nlev:] += 1e-6      # gqdt
+    g32 = torch.as_tensor(gin, device="cuda").float()
+    refs = L.forward_set_d(g32.double().cpu().numpy().reshape(4 * nlev, -1), nlev)
+    sp = P.forward_set_d(g32, nlev, precision="mixed").double().cpu().numpy()
+    for f in list(range(nlev, 2 * nlev)) + list(range(3 * nlev, 4 * nlev)):
+        assert _fp64_rounded_once(sp[f][0], refs[f][0]), (f, sp[f][0], refs[f][0])
+        assert sp[f][1] == 0.0
+
+
+def test_mixed_mass_drift_over_round_trips():
+    # 1000 round trips of ln ps through the mixed sets (inverse: sp -> grid,
+    # forward: grid as gvpp -> spf): the global mean drifts only by the float32
+    # rounding of the grid values, as FP64 sums of them carry it
+    nlat, nlev = 32, 1
+    P = Plan(nlat)
+    spin = torch.zeros((4 * nlev + 1, P.nrsp), device="cuda")
+    rng = np.random.default_rng(4)
+    sp0 = S.spectral_field(rng, P.ntru, 1, "nn1")[0]
+    sp0[0] = 11.5 * np.sqrt(2.0)     # ln(1e5 Pa) in the n = 0 mode
+    spin[4 * nlev] = torch.as_tensor(sp0, device="cuda").float()
+    gin = torch.zeros((9 * nlev + 1, nlat, 2 * nlat), device="cuda")
+    start = float(spin[4 * nlev, 0])
+    for _ in range(1000):
+        g = P.inverse_set(spin, nlev, precision="mixed")
+        gin[7 * nlev] = g[6 * nlev + 2]
+        out = P.forward_set(gin, nlev, precision="mixed")
+        spin[4 * nlev] = out[4 * nlev]
+    drift = abs(float(spin[4 * nlev, 0]) - start) / abs(start)
+    assert drift < 2e-7, drift
