@@ -772,9 +772,9 @@ __device__ __forceinline__ void rf_forward_core(const cpx<float> *stage, cpx<flo
     const cpx<float> *s = stage + r * Lay::RG + t;
 #pragma unroll
     for (int j = 0; j < Q; j++) v[j] = s[P * j];
-    if constexpr (RSUM) *rsum = row_sum_fp64<P, Q>(v);
     __syncthreads();   // the staged rows are read
     after_read();
+    if constexpr (RSUM) *rsum = row_sum_fp64<P, Q>(v);   // after the next loads are on their way
     dftQ<float, -1, Q>(v);
     const cpx<float> *tq = tqs + t * Lay::RT;
 #pragma unroll

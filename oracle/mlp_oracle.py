@@ -46,15 +46,17 @@ def forward(params, layers, X):
     return h, zs, hs
 
 
-def loss_and_grads(params, layers, X, T):
-    """Mean squared error and its gradient in the flat parameter layout."""
+def loss_and_grads(params, layers, X, T, W=None):
+    """Mean squared error (each element's squared error weighted by W when
+    given) and its gradient in the flat parameter layout."""
     params = np.asarray(params, np.float64)
     P = unpack(params, layers)
     Y, zs, hs = forward(params, layers, X)
     n = Y.size
     d = Y - np.asarray(T, np.float64)
-    loss = float((d * d).sum() / n)
-    dz = 2.0 * d / n
+    w = np.ones_like(d) if W is None else np.asarray(W, np.float64)
+    loss = float((w * d * d).sum() / n)
+    dz = 2.0 * w * d / n
     g = np.zeros_like(params)
     for l in range(len(P) - 1, -1, -1):
         wo, bo, di, do = layers[l]

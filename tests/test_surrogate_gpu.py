@@ -66,6 +66,29 @@ def test_forward_and_gradients_vs_oracle(width, nhid, n):
     assert _relmax(net.params.cpu().numpy(), pref) < 1e-5
 
 
+def test_weighted_gradients_vs_oracle():
+    # the loss in judged units: every element's squared error weighted
+    from oracle import mlp_oracle as MO
+    n = 128
+    net = SG.Mlp(NIN, NOUT, width=32, nhidden=2, max_batch=n)
+    net.init(seed=4)
+    g = np.random.default_rng(6)
+    X = g.standard_normal((n, NIN)).astype(np.float32)
+    T = g.standard_normal((n, NOUT)).astype(np.float32)
+    W = g.uniform(0.1, 10.0, (n, NOUT)).astype(np.float32)
+    params = net.params.cpu().numpy()
+    loss = torch.zeros(1, device="cuda")
+    net.backward(torch.as_tensor(X, device="cuda"), torch.as_tensor(T, device="cuda"), loss,
+                 torch.as_tensor(W, device="cuda"))
+    lref, gref = MO.loss_and_grads(params, net.layers, X, T, W)
+    torch.cuda.synchronize()
+    assert abs(loss.item() - lref) / lref < 1e-4
+    G = net.grads.cpu().numpy()
+    for wo, bo, di, do in net.layers:
+        assert _relmax(G[wo:wo + di * do], gref[wo:wo + di * do]) < 1e-4
+        assert _relmax(G[bo:bo + do], gref[bo:bo + do]) < 1e-4
+
+
 def test_training_reduces_loss(chunk):
     params, dev, X, Y, _, _ = chunk
     net = SG.Mlp(NIN, NOUT, max_batch=1024)
