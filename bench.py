@@ -68,9 +68,10 @@ def fft_bytes(nlat, nlev, half, esz):
 # of instances, divided by it), keyed by (kernel, workload); scaled to a launch by
 # the instances it processes (the traffic grows in proportion: the intermediate
 # is read once per instance, the tables once per launch are small beside it).
-# k_tc_forward_pipe on two T127 L20 instances, one cold-cache ncu capture:
-# 99.2 MB read + 5.8 MB written.  The summary with its command is in profiles/.
-NCU_TRAFFIC_PER_INST = {("tc_forward", WORKLOAD): (99.17056e6 + 5.818368e6) / 2}
+# k_tc_forward_pipe over eight T127 L20 instances (one launch of the default
+# step), one ncu capture: 312.3 MB read + 42.1 MB written.  The summary with its
+# command is in profiles/.
+NCU_TRAFFIC_PER_INST = {("tc_forward", WORKLOAD): (312293376 + 42070272) / 8}
 
 
 def traffic_per_launch(kernel, inst_per_launch):
@@ -215,6 +216,69 @@ def relerr_fields(a, b):
     return float((num / den).max())
 
 
+def dynamics_step(a, plan, spin64, gin64, B, world, time_graph, dev):
+    """A whole dynamics timestep of B states on the device, in FP32 with the
+    mixed transforms: the inverse gridpointa set -> the grid-point step
+    (exp ln ps, calcgp, flux products) -> the forward set -> spectrala per
+    state -> the inverse gridpointd set -> the forward gridpointd set (its grid
+    tendencies, the physics' output, synthetic here) -> spectrald per state
+    (plasim.f90 gridpointa :2396-2486, spectrala :2757-2918, gridpointd
+    :3142-3433, spectrald :3645-3999).  The states advance in place."""
+    import torch
+
+    from exoplasim_b200 import gridpoint as GP
+    from exoplasim_b200 import spectral as SP
+    from exoplasim_b200.replicas import max_over_ranks
+
+    L, nrsp = NLEV, plan.nrsp
+    gpc = GP.GpConst(GP.default_params(L))
+    spc = SP.SpecConst(plan, SP.default_params(L))
+    state = spin64.float().unsqueeze(0).repeat(B, 1, 1).contiguous()     # sd st sz sq sp at t
+    prev = state.clone()                                                  # at t - dt
+    ga = torch.empty((B, 6 * L + 3, NLAT, 2 * NLAT), device=dev)
+    gf = torch.empty((B, 9 * L + 1, NLAT, 2 * NLAT), device=dev)
+    tend_a = torch.empty((B, 4 * L + 1, nrsp), device=dev)
+    gd = torch.empty((B, 4 * L + 1, NLAT, 2 * NLAT), device=dev)
+    phys = gin64[:4 * L].float().unsqueeze(0).repeat(B, 1, 1, 1).contiguous() * 1e-2
+    tend_d = torch.empty((B, 4 * L, nrsp), device=dev)
+    sop = torch.zeros(nrsp, device=dev)
+    srp = state[0, L:2 * L].clone()
+
+    def views(x, i, nf):
+        v = x[i]
+        return {"d": v[0:L], "t": v[L:2 * L], "z": v[2 * L:3 * L], "q": v[3 * L:4 * L],
+                "p": v[4 * L] if nf > 4 * L else None}
+
+    states_a, states_d = [], []
+    for i in range(B):
+        sp_, sm_, ta, td = views(state, i, 4 * L + 1), views(prev, i, 4 * L + 1), views(tend_a, i, 4 * L + 1), \
+            views(tend_d, i, 4 * L)
+        base = {"sdp": sp_["d"], "szp": sp_["z"], "stp": sp_["t"], "sqp": sp_["q"], "spp": sp_["p"],
+                "sdm": sm_["d"], "szm": sm_["z"], "stm": sm_["t"], "sqm": sm_["q"], "spm": sm_["p"],
+                "sop": sop, "srp": srp}
+        states_a.append({**base, "sdt": ta["d"], "szt": ta["z"], "stt": ta["t"], "sqt": ta["q"], "spt": ta["p"]})
+        states_d.append({**base, "sdt": td["d"], "szt": td["z"], "stt": td["t"], "sqt": td["q"],
+                         "spt": ta["p"]})
+
+    def step():
+        plan.inverse_set_batch(state, L, precision="mixed", out=ga)
+        GP.gridpoint(plan, gpc, ga, gf)
+        plan.forward_set_batch(gf, L, precision="mixed", out=tend_a)
+        for st in states_a:
+            SP.spectrala(spc, st)
+        plan.inverse_set_d_batch(state, L, "mixed", out=gd)
+        plan.forward_set_d_batch(phys, L, "mixed", out=tend_d)
+        for st in states_d:
+            SP.spectrald(spc, st)
+
+    ms, nl, st_ms = time_graph(step, a.steps, a.warmup, with_steps=True)
+    med = max_over_ranks(statistics.median(st_ms))
+    return {"chain": "inverse set, calcgp, forward set, spectrala, inverse d-set, forward d-set, spectrald",
+            "precision": "mixed transforms, FP32 grid-point and spectral steps", "ms_per_step": med,
+            "timesteps_per_s": world * B / (med / 1000.0), "launches_per_step": nl,
+            "finite": bool(torch.isfinite(state).all())}
+
+
 def run_ours(a, rank, world, local_rank):
     import torch
 
@@ -330,6 +394,7 @@ def run_ours(a, rank, world, local_rank):
                     "ms_per_step": med_t, "timesteps_per_s": world * B / (med_t / 1000.0),
                     "launches_per_step": nl_t}
         del ba, sd_in, gd_in, gd_out, sd_out
+        timestep["dynamics_step"] = dynamics_step(a, plan, spin64, gin64, B, world, time_graph, dev)
 
     # per-stage timing of the primary precision
     bufs = make(torch.float32) if primary != "fp64" else make(torch.float64)

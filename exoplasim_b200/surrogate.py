@@ -146,6 +146,7 @@ class Mlp:
             net.params.copy_(torch.as_tensor(d["params"], dtype=torch.float32))
         net.set_norm(d["xm"], d["xs"], d["xlo"], d["xhi"], d["ym"], d["ys"])
         net.meta = {k: d[k] for k in d.files if k not in ("params",)}
+        net.prepare()   # a loaded network is ready for exotx_rad_surrogate
         return net
 
 
