@@ -230,10 +230,18 @@ def dynamics_step(a, plan, spin64, gin64, B, world, time_graph, dev):
     from exoplasim_b200 import spectral as SP
     from exoplasim_b200.replicas import max_over_ranks
 
+    from exoplasim_b200 import synthetic as S
+
     L, nrsp = NLEV, plan.nrsp
     gpc = GP.GpConst(GP.default_params(L))
     spc = SP.SpecConst(plan, SP.default_params(L))
-    state = spin64.float().unsqueeze(0).repeat(B, 1, 1).contiguous()     # sd st sz sq sp at t
+    # the synthetic spectra scaled to atmospheric amplitudes (winds of tens of
+    # m/s, temperature anomalies of a few K) so the states stay finite over
+    # the timed steps; planetary vorticity and ln ps as they are
+    s0 = spin64.clone()
+    s0[:4 * L] *= 0.01
+    s0[2 * L:3 * L, 2] += 0.99 * S.EZ
+    state = s0.float().unsqueeze(0).repeat(B, 1, 1).contiguous()          # sd st sz sq sp at t
     prev = state.clone()                                                  # at t - dt
     ga = torch.empty((B, 6 * L + 3, NLAT, 2 * NLAT), device=dev)
     gf = torch.empty((B, 9 * L + 1, NLAT, 2 * NLAT), device=dev)

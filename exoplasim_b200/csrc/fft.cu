@@ -762,7 +762,7 @@ __device__ __forceinline__ void rf_issue_rows(const float *__restrict__ g, RowOf
 // the block).  `stage` and `x` may be the same region.  after_read() runs
 // once every thread has its row values in registers (a block barrier lies
 // before it), before x is written.
-template <int N, bool RSUM = false, typename AfterRead>
+template <int N, bool RSUM = false, int RZ = RfLayout<N>::RZ, typename AfterRead>
 __device__ __forceinline__ void rf_forward_core(const cpx<float> *stage, cpx<float> *x, const cpx<float> *tqs,
                                                 AfterRead after_read, double *rsum = nullptr) {
     using Lay = RfLayout<N>;
@@ -797,7 +797,7 @@ __device__ __forceinline__ void rf_forward_core(const cpx<float> *stage, cpx<flo
         dft8<float, -1>(z[i]);
     }
     __syncthreads();   // the spectra overwrite the transposition buffer
-    cpx<float> *zs = x + r * Lay::RZ;
+    cpx<float> *zs = x + r * RZ;
 #pragma unroll
     for (int i = 0; i < QP; i++)
 #pragma unroll
@@ -916,7 +916,11 @@ __device__ __forceinline__ void rfft_fwd_fold_rf_body(const float *gp, float *fc
 // and arrive while it is transformed and written out.
 template <int N> struct RfPLayout {
     using Lay = RfLayout<N>;
-    static constexpr int RX = Lay::RS > Lay::RZ ? Lay::RS : Lay::RZ;
+    // spectra row stride of the folded kernel: RZF = 2 mod 16, so a half-warp's
+    // eight latitude pairs at two consecutive k fall on 16 distinct bank pairs
+    static constexpr int RZF = Lay::H + 2;
+    static_assert(RZF % 16 == 2, "spectra stride");
+    static constexpr int RX = Lay::RS > RZF ? Lay::RS : RZF;
     static constexpr size_t OFF_X = (size_t)Lay::RB * Lay::RG * 8, OFF_TQ = OFF_X + (size_t)Lay::RB * RX * 8,
                             OFF_RT = OFF_TQ + (size_t)Lay::P * Lay::RT * 8, OFF_BAR = OFF_RT + (size_t)Lay::H * 8,
                             SMEM = OFF_BAR + 16;
@@ -967,7 +971,7 @@ __global__ void __launch_bounds__(128) k_rfft_fwd_fold_rf_p(const float *gp, flo
         const long long next = item + gridDim.x;
         double rs = 0.0;
         const long long myrow = RSUM ? grow_of(item)(threadIdx.x / Lay::P) : -1ll;
-        rf_forward_core<N, RSUM>(G, X, tqs, [&] {
+        rf_forward_core<N, RSUM, PL::RZF>(G, X, tqs, [&] {
             if (next < nitems) {
                 tc::fence_proxy_async();   // G was read (and zero rows written) through the generic proxy
                 rf_issue_rows<N>(gp, grow_of(next), G, bar);
@@ -981,7 +985,7 @@ __global__ void __launch_bounds__(128) k_rfft_fwd_fold_rf_p(const float *gp, flo
             const int pr = it % PR, k = it / PR, k2 = H - k, j = j0 + pr;
             if (!fin || j >= nlath) continue;
             cpx<float> *fr = reinterpret_cast<cpx<float> *>(fc) + field * nlat + j;   // E row; O is nlath further
-            const cpx<float> *zn = X + pr * Lay::RZ, *zs = X + (pr + PR) * Lay::RZ;
+            const cpx<float> *zn = X + pr * PL::RZF, *zs = X + (pr + PR) * PL::RZF;
             const cpx<float> an = zn[k], as = zs[k];
             if (k == 0) {
                 const cpx<float> xn{(an.x + an.y) * scale, 0.f}, xs{(as.x + as.y) * scale, 0.f};

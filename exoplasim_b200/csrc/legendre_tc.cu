@@ -329,8 +329,8 @@ static bool inv_half(exotx_plan p, int nj8) {
 // in the half-table mode 64 (qi, qj) and 32 (qu/qv) columns
 static void inv_tiles_full(int nj8, int ntp1, int *nc_qi, int *nc_uv) {
     int a = 128, b = 64;
-    while (a > 16 && inv_smem(nj8, ntp1, a) > TC_SMEM_MAX) a -= 16;
-    while (b > 16 && inv_smem(nj8, ntp1, b) > TC_SMEM_MAX) b -= 16;
+    while (a > 16 && inv_smem(nj8, ntp1, a) + TCI_BARS > TC_SMEM_MAX) a -= 16;
+    while (b > 16 && inv_smem(nj8, ntp1, b) + TCI_BARS > TC_SMEM_MAX) b -= 16;
     *nc_qi = a;
     *nc_uv = b;
 }
@@ -355,14 +355,18 @@ static int fwd_level(exotx_plan p, const TcTables *T) {
 }
 // the persistent stacked-split forward kernel runs wherever its tables exist and fit
 static bool use_fwd3(const TcTables *T) { return T->has3 && fpipe_smem(T->njc) <= TC_SMEM_MAX; }
+// SMs of the current device (the grid of the persistent kernels)
+static exotx_status sm_count(int *nsm) {
+    int dev = 0;
+    EXOTX_CUDA(cudaGetDevice(&dev));
+    EXOTX_CUDA(cudaDeviceGetAttribute(nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (*nsm < 1) *nsm = 1;
+    return EXOTX_OK;
+}
 // the persistent stacked-split forward kernel: one CTA per SM walks the job list
 static exotx_status launch_fwd_pipe(TcFwd3Launch &P, int njobs, int njmax, bool folded, cudaStream_t s) {
-    static int nsm = 0;
-    if (!nsm) {
-        int dev = 0;
-        EXOTX_CUDA(cudaGetDevice(&dev));
-        EXOTX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    }
+    int nsm = 0;
+    EXOTX_TRY(sm_count(&nsm));
     const size_t smem = std::max(fpipe_smem(njmax), kPersistSmemMin);   // one CTA per SM
     if (smem > TC_SMEM_MAX) return EXOTX_BAD_DIM;
     P.njobs = njobs;
@@ -481,8 +485,16 @@ static exotx_status tc_inverse_run(exotx_plan p, const float *spin, float *gpout
     const bool half = inv_half(p, T->nj8);
     size_t smem = half ? std::max(inv_smem_half(T->nj8, p->ntp1, nc_qi), inv_smem_half(T->nj8, p->ntp1, nc_uv))
                        : std::max(inv_smem(T->nj8, p->ntp1, nc_qi), inv_smem(T->nj8, p->ntp1, nc_uv));
+    // the persistent kernel keeps its barriers in front of the tables, and asks
+    // for enough shared memory that two of its CTAs never share an SM (TMEM)
+    if (!half) smem = std::max(smem + TCI_BARS, kPersistSmemMin);
     if (smem > TC_SMEM_MAX) return EXOTX_BAD_DIM;
-    EXOTX_CUDA(cudaFuncSetAttribute(k_tc_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+    if (half)
+        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+    else
+        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_inverse_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+    int nsm = 0;
+    EXOTX_TRY(sm_count(&nsm));
     for (int i0 = 0; i0 < ninst; i0 += chunk) {
         const int ni = std::min(chunk, ninst - i0);
         const int4 *jl = jobs;
@@ -502,7 +514,10 @@ static exotx_status tc_inverse_run(exotx_plan p, const float *spin, float *gpout
         A.plavor = (float)p->desc.plavor;
         A.dset = dset;
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
-        EXOTX_CUDA(launch_pdl(k_tc_inverse, dim3(nj), dim3(half ? TCI_HALF : TCI), smem, s, P));   // set-up overlaps the last tail
+        if (half)
+            EXOTX_CUDA(launch_pdl(k_tc_inverse, dim3(nj), dim3(TCI_HALF), smem, s, P));   // set-up overlaps the last tail
+        else
+            EXOTX_CUDA(launch_pdl(k_tc_inverse_p, dim3(std::min(nj, nsm)), dim3(TCI), smem, s, P, nj));
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
         EXOTX_TRY(fft_inverse_l<float>((const float *)p->d_work, gpout + (size_t)i0 * nfo * nhor, p->nlon, A.nrows,
@@ -824,9 +839,14 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
             A.L = g.L; A.nlat = p->nlat; A.nlath = p->nlath; A.nj8 = T->nj8; A.ntp1 = p->ntp1;
             A.nrsp = 2 * p->ncsp; A.plavor = (float)p->desc.plavor;
         }
-        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
+        // the persistent kernel: barriers in front of the tables, one CTA per SM
+        const size_t smem_p = std::max(smem + TCI_BARS, kPersistSmemMin);
+        if (smem_p > TC_SMEM_MAX) return EXOTX_BAD_DIM;
+        int nsm = 0;
+        EXOTX_TRY(sm_count(&nsm));
+        EXOTX_CUDA(cudaFuncSetAttribute(k_tc_inverse_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM_MAX));
         cudaEvent_t ev = ktimer_start(EXOTX_K_TC_INVERSE, s);
-        k_tc_inverse<<<njobs, TCI, smem, s>>>(P);
+        k_tc_inverse_p<<<std::min(njobs, nsm), TCI, smem_p, s>>>(P, njobs);
         EXOTX_CHECK_LAUNCH();
         ktimer_stop(EXOTX_K_TC_INVERSE, s, ev);
     } else {

@@ -72,48 +72,58 @@ __device__ __forceinline__ const float2 *inv_row(const TcInvArgs &A, int group, 
 constexpr int TCI = 512;
 constexpr int TCI_HALF = 256;
 
-__global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcInvLaunch P) {
-    extern __shared__ __align__(128) unsigned char sm[];
-    const int4 jb = P.jobs[blockIdx.x];
-    const TcInvArgs &A = P.seg[jb.y >> 2];
-    const int nprod = P.nprod;
-    const bool half = P.half != 0;
-    const int nthr = blockDim.x, nsub = nthr >> 7;   // column-chunk groups of 4 warps
-    const int m = jb.x, group = jb.y & 3, c0 = jb.z, nc = jb.w;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, sub = warp >> 2;
-    const int K = A.ntp1 - m;
-    const int Kq[2] = {kpar(K, 0), kpar(K, 1)};
-    const int Kp[2] = {pad16(Kq[0]), pad16(Kq[1])};
-    const int ncp = pad16(nc);
-    const int ntab = group == 2 ? 2 : 1;
-    const int nj8 = A.nj8;
-    const size_t ttile[2] = {(size_t)nj8 * Kp[0] * 2, (size_t)nj8 * Kp[1] * 2};
+// Per-job geometry of the inverse kernel: job (m, group, first column,
+// columns); the table buffer at `tab`, the staged data tiles right after it.
+struct InvJob {
+    int m, group, c0, nc, K, ncp, ntab, nj8, t0;
+    int Kq[2], Kp[2];
+    size_t ttile[2], tbytes, dtile[2];
+    unsigned char *tab, *dat;
+};
+__device__ __forceinline__ InvJob inv_job(const TcInvArgs &A, int4 jb, unsigned char *tab, bool half) {
+    InvJob J;
+    J.m = jb.x;
+    J.group = jb.y & 3;
+    J.c0 = jb.z;
+    J.nc = jb.w;
+    J.K = A.ntp1 - J.m;
+    J.Kq[0] = kpar(J.K, 0);
+    J.Kq[1] = kpar(J.K, 1);
+    J.Kp[0] = pad16(J.Kq[0]);
+    J.Kp[1] = pad16(J.Kq[1]);
+    J.ncp = pad16(J.nc);
+    J.ntab = J.group == 2 ? 2 : 1;
+    J.nj8 = A.nj8;
+    J.ttile[0] = (size_t)J.nj8 * J.Kp[0] * 2;
+    J.ttile[1] = (size_t)J.nj8 * J.Kp[1] * 2;
     // the table buffer: both parity halves, or (half mode) the larger one
-    const size_t tbytes = half ? 3 * ttile[0] : 3 * (ttile[0] + ttile[1]);
+    J.tbytes = half ? 3 * J.ttile[0] : 3 * (J.ttile[0] + J.ttile[1]);
     // data tiles use the padded operand layout (core matrices 144 bytes apart along K)
-    const size_t dtile[2] = {(size_t)(ncp / 8) * (Kp[0] / 8) * tc::kPadLbo, (size_t)(ncp / 8) * (Kp[1] / 8) * tc::kPadLbo};
-    unsigned char *tab = sm;
-    unsigned char *dat = sm + tbytes;
-    unsigned char *tail = dat + 3 * (dtile[0] + dtile[1]) + (size_t)(128 - nj8) * 64 * 2 + 128;
-    uint64_t *bar_tma = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
-    uint64_t *bar_mma = bar_tma + 1;
-    uint64_t *bar_done = bar_tma + 2;
-    uint32_t *slot = reinterpret_cast<uint32_t *>(bar_tma + 3);
-    const uint32_t tcols = half ? 256 : 512;
-    const int t0 = group == 0 ? 0 : (group == 1 ? 1 : 2);
-    pdl_trigger();
-    if (warp == 0) tc::tmem_alloc(slot, tcols);
-    if (tid == 0) {
-        tc::mbar_init(bar_tma, 1);
-        tc::mbar_init(bar_mma, 1);
-        tc::mbar_init(bar_done, 1);
-        tc::mbar_fence_init();
-        // first table copy (half mode: parity 0 of the first table) goes out
-        // before the staging so the two overlap
-        tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
-        tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0], (uint32_t)tbytes, bar_tma);
-    }
-    pdl_wait();   // the spectral input and the intermediate are shared with earlier kernels
+    J.dtile[0] = (size_t)(J.ncp / 8) * (J.Kp[0] / 8) * tc::kPadLbo;
+    J.dtile[1] = (size_t)(J.ncp / 8) * (J.Kp[1] / 8) * tc::kPadLbo;
+    J.t0 = J.group == 0 ? 0 : (J.group == 1 ? 1 : 2);
+    J.tab = tab;
+    J.dat = tab + J.tbytes;
+    return J;
+}
+// bytes from the table buffer's start to the end of the job's data tiles and
+// the padding the MMAs read past them (table rows nj8..127 of the M=128 tile)
+__device__ __forceinline__ size_t inv_job_bytes(const InvJob &J) {
+    return J.tbytes + 3 * (J.dtile[0] + J.dtile[1]) + (size_t)(128 - J.nj8) * 64 * 2 + 128;
+}
+
+// thread 0: the job's first table copy (half mode: parity 0 of the first table)
+__device__ __forceinline__ void inv_first_copy(const TcInvArgs &A, const InvJob &J, uint64_t *bar_tma) {
+    tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)J.tbytes);
+    tc::bulk_g2s(J.tab, A.tab + A.off[J.m * 4 + J.t0], (uint32_t)J.tbytes, bar_tma);
+}
+
+// all threads: stage the job's spectral columns (both parities) as split BF16 operands
+__device__ __forceinline__ void inv_stage(const TcInvArgs &A, const InvJob &J, int tid, int nthr) {
+    const int m = J.m, group = J.group, c0 = J.c0, nc = J.nc, ncp = J.ncp;
+    const int Kq[2] = {J.Kq[0], J.Kq[1]}, Kp[2] = {J.Kp[0], J.Kp[1]};
+    const size_t dtile[2] = {J.dtile[0], J.dtile[1]};
+    unsigned char *dat = J.dat;
     // stage the spectral columns of both parities.  A slot is one column pair
     // q (re, im) and the modes k = 2l, 2l+1 of both parities, i.e. the four
     // consecutive spectral entries n - m = 4l .. 4l+3: consecutive threads
@@ -163,34 +173,46 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
             }
         }
     }
-    tc::fence_proxy_async();
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *slot;
+}
+
+// thread 0, full mode: the job's MMAs, table by table (the first table's copy
+// is already issued); ntma / nmma count the completed phases of bar_tma /
+// bar_mma, ncopy the copies issued on bar_tma; the last table's commit
+// arrives on bar_done
+__device__ __forceinline__ bool inv_mma_full(const TcInvArgs &A, const InvJob &J, uint32_t tmem, int nprod,
+                                             uint64_t *bar_tma, uint64_t *bar_mma, uint64_t *bar_done,
+                                             uint32_t &ntma, uint32_t &nmma, uint32_t &ncopy) {
+    const int m = J.m, ncp = J.ncp, ntab = J.ntab;
+    const int Kq[2] = {J.Kq[0], J.Kq[1]}, Kp[2] = {J.Kp[0], J.Kp[1]};
+    const size_t ttile[2] = {J.ttile[0], J.ttile[1]}, dtile[2] = {J.dtile[0], J.dtile[1]}, tbytes = J.tbytes;
+    unsigned char *tab = J.tab, *dat = J.dat;
     bool ok = true;
-    if (tid == 0 && half) {
-        // one parity half of one table at a time through one buffer: copy,
-        // MMAs, and the next copy once those MMAs have read the buffer
-        const uint32_t idesc = tc::idesc_bf16(128, ncp);
-        const int np = Kq[1] ? 2 : 1, nh = ntab * np;
-        for (int hix = 0; hix < nh && ok; hix++) {
-            const int ti = hix / np, p = hix - ti * np;
-            if (hix > 0) {
-                ok = tc::mbar_wait(bar_mma, (hix - 1) & 1);
-                if (!ok) break;
-                const uint32_t hb = (uint32_t)(3 * ttile[p]);
-                tc::mbar_arrive_expect_tx(bar_tma, hb);
-                tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0 + ti] + (p ? 3 * ttile[0] : 0), hb, bar_tma);
-            }
-            ok = tc::mbar_wait(bar_tma, hix & 1);
+    const uint32_t idesc = tc::idesc_bf16(128, ncp);
+    for (int ti = 0; ti < ntab && ok; ti++) {
+        if (ti > 0) {
+            ok = tc::mbar_wait(bar_mma, nmma & 1);  // table buffer free again
+            nmma++;
             if (!ok) break;
-            tc::fence_after_sync();
+            const int t = 2 + ti;
+            tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
+            tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t], (uint32_t)tbytes, bar_tma);
+            ncopy++;
+        }
+        ok = tc::mbar_wait(bar_tma, ntma & 1);
+        if (!ok) break;   // the copy is still counted as outstanding (ntma < ncopy)
+        ntma++;
+        tc::fence_after_sync();
+        size_t to = 0, dd = 0;
+        for (int p = 0; p < 2; p++) {
+            if (!Kq[p]) break;
+            // hi*hi products and the five smaller correction products go to
+            // separate accumulators (the tensor-core adder truncates; keeping the
+            // large term's chain short bounds that error), summed in the epilogue
             const uint32_t dm = tmem + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp);
             const uint32_t dc = tmem + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp);
             const uint32_t sbo = (uint32_t)(Kp[p] / 8) * 128, sbo_b = (uint32_t)(Kp[p] / 8) * tc::kPadLbo;
-            const uint64_t da0 = tc::smem_desc(tab, 128, sbo);
-            const uint64_t db0 = tc::smem_desc(dat + (p ? 3 * dtile[0] : 0), tc::kPadLbo, sbo_b);
+            const uint64_t da0 = tc::smem_desc(tab + to, 128, sbo);
+            const uint64_t db0 = tc::smem_desc(dat + dd, tc::kPadLbo, sbo_b);
             const uint32_t tt = (uint32_t)ttile[p], dt = (uint32_t)dtile[p];
             for (int kc = 0; kc < Kp[p] / 16; kc++) {
 #pragma unroll
@@ -200,160 +222,294 @@ __global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcIn
                                      tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 2 * tc::kPadLbo), idesc,
                                      kc > 0 || pr > 1);
             }
-            tc::mma_commit(hix == nh - 1 ? bar_done : bar_mma);
+            to += 3 * ttile[p];
+            dd += 3 * dtile[p];
         }
-        if (!ok) atomicExch(&g_tc_error, 1);
-    } else if (tid == 0) {
-        const uint32_t idesc = tc::idesc_bf16(128, ncp);
-        for (int ti = 0; ti < ntab && ok; ti++) {
-            if (ti > 0) {
-                ok = tc::mbar_wait(bar_mma, (ti - 1) & 1);  // table buffer free again
-                if (!ok) break;
-                const int t = 2 + ti;
-                tc::mbar_arrive_expect_tx(bar_tma, (uint32_t)tbytes);
-                tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t], (uint32_t)tbytes, bar_tma);
-            }
-            ok = tc::mbar_wait(bar_tma, ti & 1);
-            if (!ok) break;
-            tc::fence_after_sync();
-            size_t to = 0, dd = 0;
-            for (int p = 0; p < 2; p++) {
-                if (!Kq[p]) break;
-                // hi*hi products and the five smaller correction products go to
-                // separate accumulators (the tensor-core adder truncates; keeping the
-                // large term's chain short bounds that error), summed in the epilogue
-                const uint32_t dm = tmem + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp);
-                const uint32_t dc = tmem + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp);
-                const uint32_t sbo = (uint32_t)(Kp[p] / 8) * 128, sbo_b = (uint32_t)(Kp[p] / 8) * tc::kPadLbo;
-                const uint64_t da0 = tc::smem_desc(tab + to, 128, sbo);
-                const uint64_t db0 = tc::smem_desc(dat + dd, tc::kPadLbo, sbo_b);
-                const uint32_t tt = (uint32_t)ttile[p], dt = (uint32_t)dtile[p];
-                for (int kc = 0; kc < Kp[p] / 16; kc++) {
-#pragma unroll
-                    for (int pr = 0; pr < 6; pr++)
-                        if (pr < nprod)
-                            tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
-                                         tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 2 * tc::kPadLbo), idesc,
-                                         kc > 0 || pr > 1);
-                }
-                to += 3 * ttile[p];
-                dd += 3 * dtile[p];
-            }
-            // intermediate batches recycle the table buffer; the last one releases the epilogue
-            tc::mma_commit(ti == ntab - 1 ? bar_done : bar_mma);
-        }
-        if (!ok) atomicExch(&g_tc_error, 1);
+        // intermediate batches recycle the table buffer; the last one releases the epilogue
+        tc::mma_commit(ti == ntab - 1 ? bar_done : bar_mma);
     }
+    if (!ok) atomicExch(&g_tc_error, 1);
+    return ok;
+}
+
+// thread 0, half mode: one parity half of one table at a time through one
+// buffer: copy, MMAs, and the next copy once those MMAs have read the buffer
+__device__ __forceinline__ bool inv_mma_half(const TcInvArgs &A, const InvJob &J, uint32_t tmem, int nprod,
+                                             uint64_t *bar_tma, uint64_t *bar_mma, uint64_t *bar_done) {
+    const int m = J.m, ncp = J.ncp, ntab = J.ntab, t0 = J.t0;
+    const int Kq[2] = {J.Kq[0], J.Kq[1]}, Kp[2] = {J.Kp[0], J.Kp[1]};
+    const size_t ttile[2] = {J.ttile[0], J.ttile[1]}, dtile[2] = {J.dtile[0], J.dtile[1]};
+    unsigned char *tab = J.tab, *dat = J.dat;
+    bool ok = true;
+    // one parity half of one table at a time through one buffer: copy,
+    // MMAs, and the next copy once those MMAs have read the buffer
+    const uint32_t idesc = tc::idesc_bf16(128, ncp);
+    const int np = Kq[1] ? 2 : 1, nh = ntab * np;
+    for (int hix = 0; hix < nh && ok; hix++) {
+        const int ti = hix / np, p = hix - ti * np;
+        if (hix > 0) {
+            ok = tc::mbar_wait(bar_mma, (hix - 1) & 1);
+            if (!ok) break;
+            const uint32_t hb = (uint32_t)(3 * ttile[p]);
+            tc::mbar_arrive_expect_tx(bar_tma, hb);
+            tc::bulk_g2s(tab, A.tab + A.off[m * 4 + t0 + ti] + (p ? 3 * ttile[0] : 0), hb, bar_tma);
+        }
+        ok = tc::mbar_wait(bar_tma, hix & 1);
+        if (!ok) break;
+        tc::fence_after_sync();
+        const uint32_t dm = tmem + (uint32_t)(((ti * 2 + p) * 2 + 0) * ncp);
+        const uint32_t dc = tmem + (uint32_t)(((ti * 2 + p) * 2 + 1) * ncp);
+        const uint32_t sbo = (uint32_t)(Kp[p] / 8) * 128, sbo_b = (uint32_t)(Kp[p] / 8) * tc::kPadLbo;
+        const uint64_t da0 = tc::smem_desc(tab, 128, sbo);
+        const uint64_t db0 = tc::smem_desc(dat + (p ? 3 * dtile[0] : 0), tc::kPadLbo, sbo_b);
+        const uint32_t tt = (uint32_t)ttile[p], dt = (uint32_t)dtile[p];
+        for (int kc = 0; kc < Kp[p] / 16; kc++) {
+#pragma unroll
+            for (int pr = 0; pr < 6; pr++)
+                if (pr < nprod)
+                    tc::mma_bf16(pr == 0 ? dm : dc, tc::desc_add(da0, tc::pair_a(pr) * tt + kc * 256),
+                                 tc::desc_add(db0, tc::pair_b(pr) * dt + kc * 2 * tc::kPadLbo), idesc,
+                                 kc > 0 || pr > 1);
+        }
+        tc::mma_commit(hix == nh - 1 ? bar_done : bar_mma);
+    }
+    if (!ok) atomicExch(&g_tc_error, 1);
+    return ok;
+}
+
+// all threads (a warp-uniform test, as the TMEM loads need whole warps): TMEM
+// lane = latitude pair j, quarters past the last pair hold nothing; drain
+// the accumulators and write the job's m-major Fourier rows
+__device__ __forceinline__ void inv_epilogue(const TcInvArgs &A, const InvJob &J, uint32_t tmem, int warp, int lane,
+                                             int nsub) {
+    const int quarter = warp & 3, sub = warp >> 2;
+    if (quarter * 32 >= A.nlath) return;
+    const int m = J.m, group = J.group, c0 = J.c0, nc = J.nc, ncp = J.ncp;
+    const int Kq[2] = {J.Kq[0], J.Kq[1]};
+    const int j = quarter * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+    // gridpointa writes gu gv gt gd gz gq gpj gpmt gp (6L+3 fields),
+    // gridpointd gu gv gt gq gp (4L+1)
+    const int L = A.L, nfo = A.dset ? 4 * L + 1 : 6 * L + 3, nf = A.dset ? 2 * L + 1 : 4 * L + 1;
+    const bool has1 = Kq[1] > 0;
+    const bool row_ok = j < A.nlath;
+    const int latN = j, latS = A.nlat - 1 - j;
+    float2 *Wm = A.W + (size_t)m * A.nrows;
+    if (group < 2) {
+        // P-type qi: N = D0 + D1, S = D0 - D1; Q-type qj: S = D1 - D0
+        const float ss = group == 0 ? 1.f : -1.f;
+        for (int cc = sub * 16; cc < ncp; cc += 16 * nsub) {
+            uint32_t rm0[16], rc0[16], rm1[16], rc1[16];
+            tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(0 * ncp + cc), rm0);
+            tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(1 * ncp + cc), rc0);
+            if (has1) {
+                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(2 * ncp + cc), rm1);
+                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(3 * ncp + cc), rc1);
+            }
+            tc::tmem_wait_ld();
+            // column pair gq = (c0 + cc)/2 + i/2: instance and field without a
+            // division per pair (a chunk holds 8 pairs, fewer than nf)
+            const int gq0 = (c0 + cc) >> 1;
+            const int inst0 = group == 0 ? gq0 / nf : gq0, f0 = group == 0 ? gq0 - inst0 * nf : 4 * L;
+#pragma unroll
+            for (int i = 0; i < 16; i += 2) {
+                const float d0r = __uint_as_float(rm0[i]) + __uint_as_float(rc0[i]);
+                const float d0i = __uint_as_float(rm0[i + 1]) + __uint_as_float(rc0[i + 1]);
+                const float d1r = has1 ? __uint_as_float(rm1[i]) + __uint_as_float(rc1[i]) : 0.f;
+                const float d1i = has1 ? __uint_as_float(rm1[i + 1]) + __uint_as_float(rc1[i + 1]) : 0.f;
+                if (!row_ok || cc + i >= nc) continue;
+                int inst = inst0, f = f0;
+                if (group == 0) {
+                    f += i >> 1;
+                    while (f >= nf) { f -= nf; inst++; }
+                } else {
+                    inst += i >> 1;
+                }
+                const float2 vn = make_float2(d0r + d1r, d0i + d1i);
+                const float2 vs = make_float2(ss * (d0r - d1r), ss * (d0i - d1i));
+                int F;
+                if (A.dset) F = 2 * L + f;                    // st -> gt, sq -> gq, sp -> gp
+                else if (group == 1) F = 6 * L;               // gpj
+                else if (f < L) F = 3 * L + f;                // sd -> gd
+                else if (f < 2 * L) F = f + L;                // st -> gt
+                else if (f < 4 * L) F = f + 2 * L;            // sz -> gz, sq -> gq
+                else F = 6 * L + 2;                           // sp -> gp
+                float2 *wr = Wm + (size_t)(inst * nfo + F) * A.nlat;
+                wr[latN] = vn;
+                wr[latS] = vs;
+                if (group == 0 && !A.dset && f == 4 * L) {    // gpmt = i*m*gp
+                    const float fm = (float)m;
+                    float2 *wt = Wm + (size_t)(inst * nfo + 6 * L + 1) * A.nlat;
+                    wt[latN] = make_float2(-fm * vn.y, fm * vn.x);
+                    wt[latS] = make_float2(-fm * vs.y, fm * vs.x);
+                }
+            }
+        }
+    } else {
+        // dv2uv: u = qv*Z - i*qu*D, v = -i*qu*Z - qv*D; qu P-type, qv Q-type.
+        // accumulators r = (table, parity): 0 qu p0, 1 qu p1, 2 qv p0, 3 qv p1;
+        // columns Dr, Di, Zr, Zi per level; a chunk of 8 columns is 2 levels
+        for (int cc = sub * 8; cc < ncp; cc += 8 * nsub) {
+            uint32_t rm[4][8], rc[4][8];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                if ((r & 1) && !has1) continue;
+                tc::tmem_ld8_nw(tmem + lane_addr + (uint32_t)((r * 2 + 0) * ncp + cc), rm[r]);
+                tc::tmem_ld8_nw(tmem + lane_addr + (uint32_t)((r * 2 + 1) * ncp + cc), rc[r]);
+            }
+            tc::tmem_wait_ld();
+            float d[4][8];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int i = 0; i < 8; i++)
+                    d[r][i] = ((r & 1) && !has1) ? 0.f : __uint_as_float(rm[r][i]) + __uint_as_float(rc[r][i]);
+            const int q0 = (c0 + cc) >> 2;                    // (instance, level) of the chunk's first level
+            const int inst0 = q0 / L, l0 = q0 - inst0 * L;
+#pragma unroll
+            for (int i = 0; i < 8; i += 4) {
+                if (!row_ok || cc + i >= nc) continue;
+                int inst = inst0, l = l0 + (i >> 2);
+                if (l >= L) { l -= L; inst++; }
+                const int Dr = i, Di = i + 1, Zr = i + 2, Zi = i + 3;
+                const float urs = d[0][Di] + d[3][Zr], ura = d[1][Di] + d[2][Zr];
+                const float uis = -d[0][Dr] + d[3][Zi], uia = -d[1][Dr] + d[2][Zi];
+                const float vrs = d[0][Zi] - d[3][Dr], vra = d[1][Zi] - d[2][Dr];
+                const float vis = -d[0][Zr] - d[3][Di], via = -d[1][Zr] - d[2][Di];
+                float2 *wu = Wm + (size_t)(inst * nfo + l) * A.nlat;
+                float2 *wv = Wm + (size_t)(inst * nfo + L + l) * A.nlat;
+                wu[latN] = make_float2(urs + ura, uis + uia);
+                wu[latS] = make_float2(urs - ura, uis - uia);
+                wv[latN] = make_float2(vrs + vra, vis + via);
+                wv[latS] = make_float2(vrs - vra, vis - via);
+            }
+        }
+    }
+}
+
+// One job per CTA (half mode: two CTAs of 256 threads per SM)
+__global__ void __launch_bounds__(TCI) k_tc_inverse(const __grid_constant__ TcInvLaunch P) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const int4 jb = P.jobs[blockIdx.x];
+    const TcInvArgs &A = P.seg[jb.y >> 2];
+    const int nprod = P.nprod;
+    const bool half = P.half != 0;
+    const int nthr = blockDim.x, nsub = nthr >> 7;   // column-chunk groups of 4 warps
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const InvJob J = inv_job(A, jb, sm, half);
+    unsigned char *tail = sm + inv_job_bytes(J);
+    uint64_t *bar_tma = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(tail) + 15) & ~(uintptr_t)15);
+    uint64_t *bar_mma = bar_tma + 1;
+    uint64_t *bar_done = bar_tma + 2;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar_tma + 3);
+    const uint32_t tcols = half ? 256 : 512;
+    pdl_trigger();
+    if (warp == 0) tc::tmem_alloc(slot, tcols);
+    if (tid == 0) {
+        tc::mbar_init(bar_tma, 1);
+        tc::mbar_init(bar_mma, 1);
+        tc::mbar_init(bar_done, 1);
+        tc::mbar_fence_init();
+        // the first table copy goes out before the staging so the two overlap
+        inv_first_copy(A, J, bar_tma);
+    }
+    pdl_wait();   // the spectral input and the intermediate are shared with earlier kernels
+    inv_stage(A, J, tid, nthr);
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    bool ok = true;
+    uint32_t ntma = 0, nmma = 0, ncopy = 1;   // thread 0's bar_tma accounting (full mode)
+    if (tid == 0)
+        ok = half ? inv_mma_half(A, J, tmem, nprod, bar_tma, bar_mma, bar_done)
+                  : inv_mma_full(A, J, tmem, nprod, bar_tma, bar_mma, bar_done, ntma, nmma, ncopy);
     __syncthreads();
     ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, 0));  // warp-uniform for the .sync.aligned TMEM loads
     if (!ok && lane == 0) atomicExch(&g_tc_error, 2);
     tc::fence_after_sync();
-    // epilogue: TMEM lane = latitude pair j; quarters past the last pair hold
-    // nothing (a warp-uniform test, as the TMEM loads need whole warps)
-    if (ok && quarter * 32 < A.nlath) {
-        const int j = quarter * 32 + lane;
-        const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
-        // gridpointa writes gu gv gt gd gz gq gpj gpmt gp (6L+3 fields),
-        // gridpointd gu gv gt gq gp (4L+1)
-        const int L = A.L, nfo = A.dset ? 4 * L + 1 : 6 * L + 3, nf = A.dset ? 2 * L + 1 : 4 * L + 1;
-        const bool has1 = Kq[1] > 0;
-        const bool row_ok = j < A.nlath;
-        const int latN = j, latS = A.nlat - 1 - j;
-        float2 *Wm = A.W + (size_t)m * A.nrows;
-        if (group < 2) {
-            // P-type qi: N = D0 + D1, S = D0 - D1; Q-type qj: S = D1 - D0
-            const float ss = group == 0 ? 1.f : -1.f;
-            for (int cc = sub * 16; cc < ncp; cc += 16 * nsub) {
-                uint32_t rm0[16], rc0[16], rm1[16], rc1[16];
-                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(0 * ncp + cc), rm0);
-                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(1 * ncp + cc), rc0);
-                if (has1) {
-                    tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(2 * ncp + cc), rm1);
-                    tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(3 * ncp + cc), rc1);
-                }
-                tc::tmem_wait_ld();
-                // column pair gq = (c0 + cc)/2 + i/2: instance and field without a
-                // division per pair (a chunk holds 8 pairs, fewer than nf)
-                const int gq0 = (c0 + cc) >> 1;
-                const int inst0 = group == 0 ? gq0 / nf : gq0, f0 = group == 0 ? gq0 - inst0 * nf : 4 * L;
-#pragma unroll
-                for (int i = 0; i < 16; i += 2) {
-                    const float d0r = __uint_as_float(rm0[i]) + __uint_as_float(rc0[i]);
-                    const float d0i = __uint_as_float(rm0[i + 1]) + __uint_as_float(rc0[i + 1]);
-                    const float d1r = has1 ? __uint_as_float(rm1[i]) + __uint_as_float(rc1[i]) : 0.f;
-                    const float d1i = has1 ? __uint_as_float(rm1[i + 1]) + __uint_as_float(rc1[i + 1]) : 0.f;
-                    if (!row_ok || cc + i >= nc) continue;
-                    int inst = inst0, f = f0;
-                    if (group == 0) {
-                        f += i >> 1;
-                        while (f >= nf) { f -= nf; inst++; }
-                    } else {
-                        inst += i >> 1;
-                    }
-                    const float2 vn = make_float2(d0r + d1r, d0i + d1i);
-                    const float2 vs = make_float2(ss * (d0r - d1r), ss * (d0i - d1i));
-                    int F;
-                    if (A.dset) F = 2 * L + f;                    // st -> gt, sq -> gq, sp -> gp
-                    else if (group == 1) F = 6 * L;               // gpj
-                    else if (f < L) F = 3 * L + f;                // sd -> gd
-                    else if (f < 2 * L) F = f + L;                // st -> gt
-                    else if (f < 4 * L) F = f + 2 * L;            // sz -> gz, sq -> gq
-                    else F = 6 * L + 2;                           // sp -> gp
-                    float2 *wr = Wm + (size_t)(inst * nfo + F) * A.nlat;
-                    wr[latN] = vn;
-                    wr[latS] = vs;
-                    if (group == 0 && !A.dset && f == 4 * L) {    // gpmt = i*m*gp
-                        const float fm = (float)m;
-                        float2 *wt = Wm + (size_t)(inst * nfo + 6 * L + 1) * A.nlat;
-                        wt[latN] = make_float2(-fm * vn.y, fm * vn.x);
-                        wt[latS] = make_float2(-fm * vs.y, fm * vs.x);
-                    }
-                }
-            }
-        } else {
-            // dv2uv: u = qv*Z - i*qu*D, v = -i*qu*Z - qv*D; qu P-type, qv Q-type.
-            // accumulators r = (table, parity): 0 qu p0, 1 qu p1, 2 qv p0, 3 qv p1;
-            // columns Dr, Di, Zr, Zi per level; a chunk of 8 columns is 2 levels
-            for (int cc = sub * 8; cc < ncp; cc += 8 * nsub) {
-                uint32_t rm[4][8], rc[4][8];
-#pragma unroll
-                for (int r = 0; r < 4; r++) {
-                    if ((r & 1) && !has1) continue;
-                    tc::tmem_ld8_nw(tmem + lane_addr + (uint32_t)((r * 2 + 0) * ncp + cc), rm[r]);
-                    tc::tmem_ld8_nw(tmem + lane_addr + (uint32_t)((r * 2 + 1) * ncp + cc), rc[r]);
-                }
-                tc::tmem_wait_ld();
-                float d[4][8];
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int i = 0; i < 8; i++)
-                        d[r][i] = ((r & 1) && !has1) ? 0.f : __uint_as_float(rm[r][i]) + __uint_as_float(rc[r][i]);
-                const int q0 = (c0 + cc) >> 2;                    // (instance, level) of the chunk's first level
-                const int inst0 = q0 / L, l0 = q0 - inst0 * L;
-#pragma unroll
-                for (int i = 0; i < 8; i += 4) {
-                    if (!row_ok || cc + i >= nc) continue;
-                    int inst = inst0, l = l0 + (i >> 2);
-                    if (l >= L) { l -= L; inst++; }
-                    const int Dr = i, Di = i + 1, Zr = i + 2, Zi = i + 3;
-                    const float urs = d[0][Di] + d[3][Zr], ura = d[1][Di] + d[2][Zr];
-                    const float uis = -d[0][Dr] + d[3][Zi], uia = -d[1][Dr] + d[2][Zi];
-                    const float vrs = d[0][Zi] - d[3][Dr], vra = d[1][Zi] - d[2][Dr];
-                    const float vis = -d[0][Zr] - d[3][Di], via = -d[1][Zr] - d[2][Di];
-                    float2 *wu = Wm + (size_t)(inst * nfo + l) * A.nlat;
-                    float2 *wv = Wm + (size_t)(inst * nfo + L + l) * A.nlat;
-                    wu[latN] = make_float2(urs + ura, uis + uia);
-                    wu[latS] = make_float2(urs - ura, uis - uia);
-                    wv[latN] = make_float2(vrs + vra, vis + via);
-                    wv[latS] = make_float2(vrs - vra, vis - via);
-                }
-            }
+    if (ok) inv_epilogue(A, J, tmem, warp, lane, nsub);
+    // after a timeout, copies issued but never waited for land before the block exits
+    if (tid == 0 && !ok && !half)
+        while (ntma < ncopy) tc::mbar_wait(bar_tma, ntma++ & 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, tcols);
+}
+
+// Persistent form (full mode): one CTA of 512 threads per SM walks the jobs
+// blockIdx.x, + gridDim.x, ...  The barriers sit at the start of shared memory
+// and the table buffer after them.  Once a job's MMAs have completed, thread 0
+// issues the next job's first table copy, which lands while this job's
+// epilogue drains TMEM; the next job's staging follows the epilogue.
+constexpr int TCI_BARS = 128;   // bytes in front of the table buffer
+__global__ void __launch_bounds__(TCI) k_tc_inverse_p(const __grid_constant__ TcInvLaunch P, int njobs) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *bar_tma = reinterpret_cast<uint64_t *>(sm);
+    uint64_t *bar_mma = bar_tma + 1;
+    uint64_t *bar_done = bar_tma + 2;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar_tma + 3);
+    unsigned char *tabbuf = sm + TCI_BARS;
+    const int nprod = P.nprod;
+    const int nthr = blockDim.x, nsub = nthr >> 7;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    pdl_trigger();
+    if (warp == 0) tc::tmem_alloc(slot, 512);
+    int j = blockIdx.x;
+    uint32_t ncopy = 0;   // table copies issued on bar_tma (thread 0)
+    if (tid == 0) {
+        tc::mbar_init(bar_tma, 1);
+        tc::mbar_init(bar_mma, 1);
+        tc::mbar_init(bar_done, 1);
+        tc::mbar_fence_init();
+        if (j < njobs) {   // job descriptors and tables are host-built: before the dependent-launch wait
+            const int4 jb = P.jobs[j];
+            inv_first_copy(P.seg[jb.y >> 2], inv_job(P.seg[jb.y >> 2], jb, tabbuf, false), bar_tma);
+            ncopy++;
         }
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, tcols);
+    tc::fence_after_sync();
+    const uint32_t tmem = *slot;
+    pdl_wait();   // the spectral input and the intermediate are shared with earlier kernels
+    uint32_t ntma = 0, nmma = 0, ndone = 0;
+    bool ok = true;
+    for (; j < njobs; j += gridDim.x) {
+        const int4 jb = P.jobs[j];
+        const TcInvArgs &A = P.seg[jb.y >> 2];
+        const InvJob J = inv_job(A, jb, tabbuf, false);
+        inv_stage(A, J, tid, nthr);
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        __syncthreads();   // staged; the previous job's TMEM loads have completed
+        tc::fence_after_sync();
+        if (tid == 0) inv_mma_full(A, J, tmem, nprod, bar_tma, bar_mma, bar_done, ntma, nmma, ncopy);
+        ok = __all_sync(0xffffffffu, tc::mbar_wait(bar_done, ndone & 1));   // warp-uniform
+        ndone++;
+        ok = __syncthreads_and(ok) != 0;   // block-uniform, so every thread leaves the loop together
+        if (!ok) {
+            if (tid == 0) atomicExch(&g_tc_error, 2);
+            break;
+        }
+        tc::fence_after_sync();
+        // the MMAs have read the table buffer and the data tiles: the next job's
+        // first table lands while this job's epilogue runs
+        if (tid == 0 && j + (int)gridDim.x < njobs) {
+            const int4 jn = P.jobs[j + gridDim.x];
+            inv_first_copy(P.seg[jn.y >> 2], inv_job(P.seg[jn.y >> 2], jn, tabbuf, false), bar_tma);
+            ncopy++;
+        }
+        inv_epilogue(A, inv_job(A, jb, tabbuf, false), tmem, warp, lane, nsub);   // recomputed: fewer live registers
+        tc::fence_before_sync();
+    }
+    // after a timeout, copies issued but never waited for land before the block exits
+    if (tid == 0 && !ok)
+        while (ntma < ncopy) tc::mbar_wait(bar_tma, ntma++ & 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 512);
 }
 
 static size_t inv_smem(int nj8, int K, int ncp) {
