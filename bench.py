@@ -17,6 +17,7 @@ hosts) on all host cores, on the same workload, and prints the same line.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -234,13 +235,18 @@ def dynamics_step(a, plan, spin64, gin64, B, world, time_graph, dev):
 
     L, nrsp = NLEV, plan.nrsp
     gpc = GP.GpConst(GP.default_params(L))
-    spc = SP.SpecConst(plan, SP.default_params(L))
-    # the synthetic spectra scaled to atmospheric amplitudes (winds of tens of
-    # m/s, temperature anomalies of a few K) so the states stay finite over
-    # the timed steps; planetary vorticity and ln ps as they are
+    # a T127 time step: 256 per rotation (about 5.6 minutes of an Earth day)
+    dt = 2.0 * math.pi / 256.0
+    spc = SP.SpecConst(plan, SP.default_params(L, delt=dt, delt2=2.0 * dt))
+    # the synthetic spectra scaled to atmospheric amplitudes (winds of about
+    # 10 m/s, temperature anomalies of tens of K, surface-pressure anomalies of
+    # about 1%) so the states stay finite over the timed steps; the planetary
+    # vorticity kept, and ln(ps / psurf) with a zero global mean, as the model
+    # holds it (spectrala keeps spp(1:2) = 0)
     s0 = spin64.clone()
-    s0[:4 * L] *= 0.01
+    s0 *= 0.01
     s0[2 * L:3 * L, 2] += 0.99 * S.EZ
+    s0[4 * L, 0:2] = 0.0
     state = s0.float().unsqueeze(0).repeat(B, 1, 1).contiguous()          # sd st sz sq sp at t
     prev = state.clone()                                                  # at t - dt
     ga = torch.empty((B, 6 * L + 3, NLAT, 2 * NLAT), device=dev)
