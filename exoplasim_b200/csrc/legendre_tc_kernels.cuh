@@ -299,24 +299,31 @@ __device__ __forceinline__ void inv_epilogue(const TcInvArgs &A, const InvJob &J
         // P-type qi: N = D0 + D1, S = D0 - D1; Q-type qj: S = D1 - D0
         const float ss = group == 0 ? 1.f : -1.f;
         for (int cc = sub * 16; cc < ncp; cc += 16 * nsub) {
-            uint32_t rm0[16], rc0[16], rm1[16], rc1[16];
-            tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(0 * ncp + cc), rm0);
-            tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(1 * ncp + cc), rc0);
-            if (has1) {
-                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(2 * ncp + cc), rm1);
-                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(3 * ncp + cc), rc1);
+            // parity 0's main and correction accumulators, summed, then parity 1's
+            // (two loads in flight at a time: fewer live registers)
+            float d0[16], d1[16];
+            {
+                uint32_t ra[16], rb[16];
+                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(0 * ncp + cc), ra);
+                tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(1 * ncp + cc), rb);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; i++) d0[i] = __uint_as_float(ra[i]) + __uint_as_float(rb[i]);
+                if (has1) {
+                    tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(2 * ncp + cc), ra);
+                    tc::tmem_ld16_nw(tmem + lane_addr + (uint32_t)(3 * ncp + cc), rb);
+                    tc::tmem_wait_ld();
+                }
+#pragma unroll
+                for (int i = 0; i < 16; i++) d1[i] = has1 ? __uint_as_float(ra[i]) + __uint_as_float(rb[i]) : 0.f;
             }
-            tc::tmem_wait_ld();
             // column pair gq = (c0 + cc)/2 + i/2: instance and field without a
             // division per pair (a chunk holds 8 pairs, fewer than nf)
             const int gq0 = (c0 + cc) >> 1;
             const int inst0 = group == 0 ? gq0 / nf : gq0, f0 = group == 0 ? gq0 - inst0 * nf : 4 * L;
 #pragma unroll
             for (int i = 0; i < 16; i += 2) {
-                const float d0r = __uint_as_float(rm0[i]) + __uint_as_float(rc0[i]);
-                const float d0i = __uint_as_float(rm0[i + 1]) + __uint_as_float(rc0[i + 1]);
-                const float d1r = has1 ? __uint_as_float(rm1[i]) + __uint_as_float(rc1[i]) : 0.f;
-                const float d1i = has1 ? __uint_as_float(rm1[i + 1]) + __uint_as_float(rc1[i + 1]) : 0.f;
+                const float d0r = d0[i], d0i = d0[i + 1], d1r = d1[i], d1i = d1[i + 1];
                 if (!row_ok || cc + i >= nc) continue;
                 int inst = inst0, f = f0;
                 if (group == 0) {
