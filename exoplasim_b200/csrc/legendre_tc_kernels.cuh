@@ -1103,6 +1103,7 @@ constexpr int FP_THREADS = 512;
 constexpr int FP_NST = 320;              // staging threads
 constexpr int FP_ACC = 144;              // TMEM columns of a slot: 3 x the widest table's columns
 constexpr int FP_SLOTS = 2;              // staging slots per thread kept in flight for one tile
+constexpr int FP_FOLD_DEPTH = 2;         // tiles ahead whose folded-intermediate loads are in flight
 
 struct FpLayout {
     uint32_t tb, ob;                     // bytes of a table slot and of an operand slot
@@ -1357,9 +1358,10 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
         pdl_wait();   // the intermediate comes from the previous kernel
         // slots per thread kept in flight for a tile, and how many tiles ahead
         // they are loaded: the folded intermediate needs one slot per thread
-        // per tile (eight latitude pairs), so its loads run two tiles ahead
-        constexpr int SL = FOLD ? 1 : FP_SLOTS, DEPTH = FOLD ? 2 : 1;
-        F3Slot q0[SL], q1[SL], q2[SL];   // tiles i, i+1, i+2
+        // per tile (eight latitude pairs), so its loads run FP_FOLD_DEPTH tiles
+        // ahead (a ring of registers: q[d] holds tile i + d)
+        constexpr int SL = FOLD ? 1 : FP_SLOTS, DEPTH = FOLD ? FP_FOLD_DEPTH : 1;
+        F3Slot q[DEPTH + 1][SL];
         auto load = [&](const TcFwd3Args &A, int4 jb, int t, int sl, F3Slot &v) {
             if constexpr (FOLD)
                 f3_load_fold<NLT>(A, jb.x, jb.y & 0xffff, jb.z, jb.w & 0xff, jb.z == 0, t, jb.w >> 8, sl, v);
@@ -1370,15 +1372,13 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             if constexpr (FOLD) f3_store_fold<NLT>(t, sl, njc, bt, v);
             else f3_store<NLT>(t, p, sl, njc, bt, v);
         };
-        if (ntile > 0) {
-            const int4 jb = job(0);
 #pragma unroll
-            for (int k = 0; k < SL; k++) load(P.seg[jb.y >> 16], jb, 0, stid + k * FP_NST, q0[k]);
-        }
-        if (DEPTH == 2 && ntile > 1) {
-            const int4 jb = job(1);
+        for (int d = 0; d < DEPTH; d++) {
+            if (d < ntile) {
+                const int4 jb = job(d);
 #pragma unroll
-            for (int k = 0; k < SL; k++) load(P.seg[jb.y >> 16], jb, 1, stid + k * FP_NST, q1[k]);
+                for (int k = 0; k < SL; k++) load(P.seg[jb.y >> 16], jb, d & 3, stid + k * FP_NST, q[d][k]);
+            }
         }
         for (int i = 0; i < ntile; i++) {
             const int b = i & 1, u = i >> 1, t = i & 3;
@@ -1389,17 +1389,14 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
                 // later tiles' loads are in flight while this one is stored
                 const int4 jn = job(i + DEPTH);
 #pragma unroll
-                for (int k = 0; k < SL; k++) {
-                    if (DEPTH == 2) load(P.seg[jn.y >> 16], jn, (i + DEPTH) & 3, stid + k * FP_NST, q2[k]);
-                    else load(P.seg[jn.y >> 16], jn, (i + DEPTH) & 3, stid + k * FP_NST, q1[k]);
-                }
+                for (int k = 0; k < SL; k++) load(P.seg[jn.y >> 16], jn, (i + DEPTH) & 3, stid + k * FP_NST, q[DEPTH][k]);
             }
             if (!fp_wait(op_empty + b, (u & 1) ^ 1, abort)) break;
             unsigned char *bt = opr + b * LY.ob;
             const int nslot = (fwd_ncp<NLT>(t) >> 1) * (FOLD ? (njc >> 3) : (njc >> 2));
 #pragma unroll
             for (int k = 0; k < SL; k++)
-                if (stid + k * FP_NST < nslot) store(t, p, stid + k * FP_NST, njc, bt, q0[k]);
+                if (stid + k * FP_NST < nslot) store(t, p, stid + k * FP_NST, njc, bt, q[0][k]);
             for (int s = stid + SL * FP_NST; s < nslot; s += FP_NST) {   // beyond the slots in flight
                 F3Slot v;
                 load(A, jb, t, s, v);
@@ -1408,10 +1405,9 @@ __global__ void __launch_bounds__(FP_THREADS, 1) k_tc_forward_pipe(const __grid_
             tc::fence_proxy_async();   // these stores feed the tensor cores
             tc::mbar_arrive(op_full + b);
 #pragma unroll
-            for (int k = 0; k < SL; k++) {
-                q0[k] = q1[k];
-                if (DEPTH == 2) q1[k] = q2[k];
-            }
+            for (int d = 0; d < DEPTH; d++)
+#pragma unroll
+                for (int k = 0; k < SL; k++) q[d][k] = q[d + 1][k];
         }
     }
     tc::fence_before_sync();
