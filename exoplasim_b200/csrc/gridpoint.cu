@@ -12,9 +12,9 @@
 // need the whole column's zvgpg, zvgpg + gd and ztv1 - gt: those three
 // profiles live in shared memory, laid out level-major so that a warp's
 // accesses fall in distinct banks.  The matrices and per-level constants are
-// one small device block that every thread of a warp reads word for word
-// alike (one broadcast load).  The kernel is HBM-bound: (15L+4) values move
-// per column.
+// one small block, staged in shared memory in the step's precision once per
+// block where it fits (every thread of a warp then reads it word for word
+// alike).  The kernel is HBM-bound: (15L+4) values move per column.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -29,15 +29,7 @@ namespace exotx {
 
 exotx_status launch_gridpoint_fp64(const GpArgs<double> &A, cudaStream_t s);
 
-static exotx_status launch_gridpoint_fp32(const GpArgs<float> &A, cudaStream_t s) {
-    const size_t smem = 3 * (size_t)A.L * GP_THREADS * sizeof(float);
-    if (smem > 48 * 1024)
-        EXOTX_CUDA(cudaFuncSetAttribute(k_gridpoint<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const long long nb = (A.ncol + GP_THREADS - 1) / GP_THREADS;
-    k_gridpoint<float><<<(unsigned)nb, GP_THREADS, smem, s>>>(A);
-    EXOTX_CHECK_LAUNCH();
-    return EXOTX_OK;
-}
+static exotx_status launch_gridpoint_fp32(const GpArgs<float> &A, cudaStream_t s) { return gp_launch<float>(A, s); }
 
 }  // namespace exotx
 

@@ -21,12 +21,34 @@ struct GpArgs {
     double akap, rdbrv, adv, psurf, ww;
 };
 
+// the constants block in the step's precision: in shared memory (SK, staged
+// once per block) or read from global memory and rounded at each use
+template <typename T, bool SK>
+struct GpConsts {
+    const T *s;
+    const double *g;
+    __device__ __forceinline__ T operator()(int i) const {
+        if constexpr (SK) return s[i];
+        else return (T)g[i];
+    }
+};
 template <typename T>
+__host__ __device__ inline size_t gp_smem(int L, bool sk) {
+    return sizeof(T) * (3 * (size_t)L * GP_THREADS + (sk ? 6 * (size_t)L + 2 * (size_t)L * L : 0));
+}
+
+template <typename T, bool SK>
 __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
     extern __shared__ __align__(16) unsigned char gsm[];
     T *sv = reinterpret_cast<T *>(gsm);                 // zvgpg      [L][GP_THREADS]
     T *sb = sv + (size_t)A.L * GP_THREADS;              // zvgpg + gd [L][GP_THREADS]
     T *s1 = sb + (size_t)A.L * GP_THREADS;              // ztv1 - gt  [L][GP_THREADS]
+    T *sk = s1 + (size_t)A.L * GP_THREADS;              // constants (SK)
+    if constexpr (SK) {
+        for (int i = threadIdx.x; i < 6 * A.L + 2 * A.L * A.L; i += GP_THREADS) sk[i] = (T)A.k[i];
+        __syncthreads();
+    }
+    const GpConsts<T, SK> K{sk, A.k};
     const long long col = blockIdx.x * (long long)GP_THREADS + threadIdx.x;
     if (col >= A.ncol) return;
     const int L = A.L, tx = threadIdx.x;
@@ -35,8 +57,6 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
     const size_t n = (size_t)A.nhor;
     const T *gin = A.gin + (size_t)inst * (6 * L + 3) * n;
     T *gout = A.gout + (size_t)inst * (9 * L + 1) * n;
-    const double *dsigma = A.k, *sigmah = A.k + L, *rdsig = A.k + 2 * L, *t0 = A.k + 3 * L, *t01s2 = A.k + 4 * L,
-                 *tkp = A.k + 5 * L, *gm = A.k + 6 * L, *cm = A.k + 6 * L + L * L;
 #define IN(f, k) gin[((size_t)(f) * L + (k)) * n + h]
 #define OUT(f, k) gout[((size_t)(f) * L + (k)) * n + h]
 #define SH(a, k) a[(size_t)(k) * GP_THREADS + tx]
@@ -53,12 +73,12 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
         T zq;
         if (A.nqspec == 1) zq = fmax(gq / gp, (T)0.);
         else zq = A.dq ? fmax(A.dq[((size_t)inst * L + k) * n + h], (T)0.) : (T)0.;
-        const T tv1 = (gt + (T)t0[k]) * ((T)1. + rdbrv1 * zq) - (T)t0[k];
+        const T tv1 = (gt + K(3 * L + k)) * ((T)1. + rdbrv1 * zq) - K(3 * L + k);
         SH(sv, k) = zv;
         SH(sb, k) = zv + gd;
         SH(s1, k) = tv1 - gt;
-        if (k == 0) { zsumd = (T)dsigma[0] * gd; gvp = (T)dsigma[0] * zv; }
-        else { zsumd = zsumd + (T)dsigma[k] * gd; gvp = gvp + (T)dsigma[k] * zv; }
+        if (k == 0) { zsumd = K(0) * gd; gvp = K(0) * zv; }
+        else { zsumd = zsumd + K(k) * gd; gvp = gvp + K(k) * zv; }
     }
     const T tot = zsumd + gvp;
     // pass 2, level by level: sigma-dot, vertical advection terms and tendencies
@@ -71,14 +91,14 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
         T zq;
         if (A.nqspec == 1) zq = fmax(gq / gp, (T)0.);
         else zq = A.dq ? fmax(A.dq[((size_t)inst * L + k) * n + h], (T)0.) : (T)0.;
-        const T tv1 = (gt + (T)t0[k]) * ((T)1. + rdbrv1 * zq) - (T)t0[k];
-        const T tv2 = (gt + (T)t0[k]) * ((T)1. + rdbrv1 * zq) / ((T)1. + (T)A.adv * zq) - (T)t0[k];
+        const T tv1 = (gt + K(3 * L + k)) * ((T)1. + rdbrv1 * zq) - K(3 * L + k);
+        const T tv2 = (gt + K(3 * L + k)) * ((T)1. + rdbrv1 * zq) / ((T)1. + (T)A.adv * zq) - K(3 * L + k);
         // this level's products of the sigma-dot flux with the layer differences
         T gtd = 0, gqm = 0, gud = 0, gvd = 0;
         if (k < L - 1) {
-            if (k == 0) { psd = (T)dsigma[0] * gd; psv = (T)dsigma[0] * zv; }
-            else { psd = psd + (T)dsigma[k] * gd; psv = psv + (T)dsigma[k] * zv; }
-            const T zsdotp = ((T)sigmah[k] * tot - (psd + psv));
+            if (k == 0) { psd = K(0) * gd; psv = K(0) * zv; }
+            else { psd = psd + K(k) * gd; psv = psv + K(k) * zv; }
+            const T zsdotp = (K(L + k) * tot - (psd + psv));
             gtd = zsdotp * (IN(2, k + 1) - gt);
             gqm = zsdotp * (IN(5, k + 1) + gq);
             gud = zsdotp * (IN(0, k + 1) - gu);
@@ -86,39 +106,39 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
         }
         T gtn, gqn, guz, gvz, dwv;
         if (k == 0) {
-            zs = zv * (T)dsigma[0];
-            gtn = gt * gd - (T)A.akap * tv2 * gd - (T)rdsig[0] * (gtd + (T)t01s2[0] * ((T)sigmah[0] * gvp - zs));
-            gqn = -(T)rdsig[0] * gqm;
-            guz = -gu * gz - gpj * tv1 - (T)rdsig[0] * gvd;
-            gvz = gv * gz - gpm * tv1 - (T)rdsig[0] * gud;
+            zs = zv * K(0);
+            gtn = gt * gd - (T)A.akap * tv2 * gd - K(2 * L + 0) * (gtd + K(4 * L + 0) * (K(L + 0) * gvp - zs));
+            gqn = -K(2 * L + 0) * gqm;
+            guz = -gu * gz - gpj * tv1 - K(2 * L + 0) * gvd;
+            gvz = gv * gz - gpm * tv1 - K(2 * L + 0) * gud;
             dwv = gd * gp * (T)A.psurf * (T)A.ww;
         } else {
-            T ztpta = (T)cm[0 + L * k] * SH(sv, 0);
-            T ztptb = (T)cm[0 + L * k] * SH(sb, 0);
+            T ztpta = K(6 * L + L * L + 0 + L * k) * SH(sv, 0);
+            T ztptb = K(6 * L + L * L + 0 + L * k) * SH(sb, 0);
             for (int j = 1; j <= k; j++) {
-                ztpta = ztpta + (T)cm[j + L * k] * SH(sv, j);
-                ztptb = ztptb + (T)cm[j + L * k] * SH(sb, j);
+                ztpta = ztpta + K(6 * L + L * L + j + L * k) * SH(sv, j);
+                ztptb = ztptb + K(6 * L + L * L + j + L * k) * SH(sb, j);
             }
             if (k < L - 1) {
-                zs = zs + zv * (T)dsigma[k];
-                gtn = gt * gd + (T)A.akap * tv2 * (zv - ztptb) + (T)tkp[k] * (zv - ztpta) -
-                      (T)rdsig[k] * (gtd + gtd_m + gvp * ((T)t01s2[k] * (T)sigmah[k] + (T)t01s2[k - 1] * (T)sigmah[k - 1]) -
-                                     zs * ((T)t01s2[k - 1] + (T)t01s2[k]) + zv * (T)dsigma[k] * (T)t01s2[k - 1]);
-                gqn = -(T)rdsig[k] * (gqm - gqm_m);
-                guz = -gu * gz - gpj * tv1 - (T)rdsig[k] * (gvd + gvd_m);
-                gvz = gv * gz - gpm * tv1 - (T)rdsig[k] * (gud + gud_m);
+                zs = zs + zv * K(k);
+                gtn = gt * gd + (T)A.akap * tv2 * (zv - ztptb) + K(5 * L + k) * (zv - ztpta) -
+                      K(2 * L + k) * (gtd + gtd_m + gvp * (K(4 * L + k) * K(L + k) + K(4 * L + k - 1) * K(L + k - 1)) -
+                                     zs * (K(4 * L + k - 1) + K(4 * L + k)) + zv * K(k) * K(4 * L + k - 1));
+                gqn = -K(2 * L + k) * (gqm - gqm_m);
+                guz = -gu * gz - gpj * tv1 - K(2 * L + k) * (gvd + gvd_m);
+                gvz = gv * gz - gpm * tv1 - K(2 * L + k) * (gud + gud_m);
             } else {
-                gtn = gt * gd + (T)A.akap * tv2 * (zv - ztptb) + (T)tkp[k] * (zv - ztpta) -
-                      (T)rdsig[k] * (gtd_m + (T)t01s2[k - 1] * ((T)sigmah[k - 1] * gvp - zs));
-                gqn = (T)rdsig[k] * gqm_m;
-                guz = -gu * gz - gpj * tv1 - (T)rdsig[k] * gvd_m;
-                gvz = gv * gz - gpm * tv1 - (T)rdsig[k] * gud_m;
+                gtn = gt * gd + (T)A.akap * tv2 * (zv - ztptb) + K(5 * L + k) * (zv - ztpta) -
+                      K(2 * L + k) * (gtd_m + K(4 * L + k - 1) * (K(L + k - 1) * gvp - zs));
+                gqn = K(2 * L + k) * gqm_m;
+                guz = -gu * gz - gpj * tv1 - K(2 * L + k) * gvd_m;
+                gvz = gv * gz - gpm * tv1 - K(2 * L + k) * gud_m;
             }
             dwv = (zv - ztptb) * gp * (T)A.psurf * (T)A.ww;
         }
         // non-linear geopotential, summed over every level as dot_product does
         T dot = 0;
-        for (int i = 0; i < L; i++) dot = dot + (T)gm[i + L * k] * SH(s1, i);
+        for (int i = 0; i < L; i++) dot = dot + K(6 * L + i + L * k) * SH(s1, i);
         const T gphi = dot * (T)2. / rc;
         T ke = gu * gu + gv * gv;
         ke = ke + gphi;
@@ -138,6 +158,25 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
 #undef IN
 #undef OUT
 #undef SH
+}
+
+// the launch: the constants in shared memory where they fit beside the profiles
+template <typename T>
+inline exotx_status gp_launch(const GpArgs<T> &A, cudaStream_t s) {
+    const bool sk = gp_smem<T>(A.L, true) <= 227 * 1024;
+    const size_t smem = gp_smem<T>(A.L, sk);
+    const long long nb = (A.ncol + GP_THREADS - 1) / GP_THREADS;
+    if (sk) {
+        if (smem > 48 * 1024)
+            EXOTX_CUDA(cudaFuncSetAttribute(k_gridpoint<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_gridpoint<T, true><<<(unsigned)nb, GP_THREADS, smem, s>>>(A);
+    } else {
+        if (smem > 48 * 1024)
+            EXOTX_CUDA(cudaFuncSetAttribute(k_gridpoint<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_gridpoint<T, false><<<(unsigned)nb, GP_THREADS, smem, s>>>(A);
+    }
+    EXOTX_CHECK_LAUNCH();
+    return EXOTX_OK;
 }
 
 }  // namespace exotx

@@ -13,30 +13,16 @@ struct exotx_specconst_s {
     int ntru = 0, nrsp = 0;
     double *d = nullptr;    // constants block (see SpecArgs::k)
     double *sak = nullptr;  // [L][NRSP]
+    float *df = nullptr;    // the same two, rounded to FP32 once, for the FP32 step
+    float *sakf = nullptr;
     int *nidx = nullptr;    // [NRSP]
 };
 
 namespace exotx {
 exotx_status launch_spectral_fp64(const SpecArgs<double> &A, bool d_part, cudaStream_t s);
 
-static int spec_threads(int L, size_t esz) {
-    int t = 128;
-    while (t > 32 && 4 * (size_t)L * t * esz > 160 * 1024) t -= 32;
-    return t;
-}
-
 static exotx_status launch_spectral_fp32(const SpecArgs<float> &A, bool d_part, cudaStream_t s) {
-    if (d_part) {
-        k_spectrald<float><<<(A.nrsp + 127) / 128, 128, 0, s>>>(A);
-    } else {
-        const int nt = spec_threads(A.L, 4);
-        const size_t smem = 4 * (size_t)A.L * nt * sizeof(float);
-        if (smem > 48 * 1024)
-            EXOTX_CUDA(cudaFuncSetAttribute(k_spectrala<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_spectrala<float><<<(A.nrsp + nt - 1) / nt, nt, smem, s>>>(A);
-    }
-    EXOTX_CHECK_LAUNCH();
-    return EXOTX_OK;
+    return spec_launch<float>(A, d_part, s);
 }
 }  // namespace exotx
 
@@ -190,14 +176,19 @@ EXOTX_API exotx_status exotx_specconst_create(exotx_plan pl, const exotx_spec_pa
     sc->h = *p;
     sc->ntru = ntru;
     sc->nrsp = nrsp;
+    const std::vector<float> kf(k.begin(), k.end()), sakf(sak.begin(), sak.end());   // rounded to nearest
     bool ok = cudaMalloc(&sc->d, sizeof(double) * k.size()) == cudaSuccess &&
               cudaMalloc(&sc->sak, sizeof(double) * sak.size()) == cudaSuccess &&
+              cudaMalloc(&sc->df, sizeof(float) * kf.size()) == cudaSuccess &&
+              cudaMalloc(&sc->sakf, sizeof(float) * sakf.size()) == cudaSuccess &&
               cudaMalloc(&sc->nidx, sizeof(int) * nidx.size()) == cudaSuccess &&
               cudaMemcpy(sc->d, k.data(), sizeof(double) * k.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(sc->sak, sak.data(), sizeof(double) * sak.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(sc->df, kf.data(), sizeof(float) * kf.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(sc->sakf, sakf.data(), sizeof(float) * sakf.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMemcpy(sc->nidx, nidx.data(), sizeof(int) * nidx.size(), cudaMemcpyHostToDevice) == cudaSuccess;
     if (!ok) {
-        cudaFree(sc->d); cudaFree(sc->sak); cudaFree(sc->nidx);
+        cudaFree(sc->d); cudaFree(sc->sak); cudaFree(sc->df); cudaFree(sc->sakf); cudaFree(sc->nidx);
         delete sc;
         return EXOTX_NO_MEM;
     }
@@ -207,7 +198,7 @@ EXOTX_API exotx_status exotx_specconst_create(exotx_plan pl, const exotx_spec_pa
 
 EXOTX_API exotx_status exotx_specconst_destroy(exotx_specconst c) {
     if (!c) return EXOTX_BAD_ARG;
-    cudaFree(c->d); cudaFree(c->sak); cudaFree(c->nidx);
+    cudaFree(c->d); cudaFree(c->sak); cudaFree(c->df); cudaFree(c->sakf); cudaFree(c->nidx);
     delete c;
     return EXOTX_OK;
 }
@@ -219,7 +210,9 @@ static SpecArgs<T> spec_args(exotx_specconst c, const exotx_spec_state *s) {
     A.sdm = (T *)s->sdm; A.szm = (T *)s->szm; A.stm = (T *)s->stm; A.sqm = (T *)s->sqm; A.spm = (T *)s->spm;
     A.sdt = (T *)s->sdt; A.szt = (T *)s->szt; A.stt = (T *)s->stt; A.sqt = (T *)s->sqt; A.spt = (T *)s->spt;
     A.sop = (const T *)s->sop; A.srp = (const T *)s->srp;
-    A.k = c->d; A.sak = c->sak; A.nidx = c->nidx;
+    if constexpr (sizeof(T) == 8) { A.k = (const T *)c->d; A.sak = (const T *)c->sak; }
+    else { A.k = (const T *)c->df; A.sak = (const T *)c->sakf; }
+    A.nidx = c->nidx;
     A.L = c->h.nlev; A.nrsp = c->nrsp; A.ntru = c->ntru; A.nqspec = c->h.nqspec; A.nsponge = c->h.nsponge;
     A.delt = c->h.delt; A.delt2 = c->h.delt2; A.pnu = c->h.pnu; A.pnu21 = c->h.pnu21; A.plavor = c->h.plavor;
     A.dampsp = c->h.dampsp;
