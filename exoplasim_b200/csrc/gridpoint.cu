@@ -23,6 +23,7 @@
 struct exotx_gpconst_s {
     exotx_gp_params h;  // host copy
     double *d = nullptr;  // device: dsigma sigmah rdsig t0 t01s2 tkp [L each], g, c [L*L each]
+    int g_lower = 0;      // g(i, k) = 0 for every i < k (initsi's g is)
 };
 
 namespace exotx {
@@ -101,6 +102,10 @@ EXOTX_API exotx_status exotx_gpconst_create(const exotx_gp_params *p, exotx_gpco
     for (int i = 0; i < L * L; i++) { k[6 * L + i] = p->g[i]; k[6 * L + L * L + i] = p->c[i]; }
     exotx_gpconst c = new exotx_gpconst_s();
     c->h = *p;
+    c->g_lower = 1;
+    for (int k = 0; k < L; k++)
+        for (int i = 0; i < k; i++)
+            if (p->g[i + L * k] != 0.0) c->g_lower = 0;
     if (cudaMalloc(&c->d, sizeof(double) * k.size()) != cudaSuccess) { delete c; return EXOTX_NO_MEM; }
     if (cudaMemcpy(c->d, k.data(), sizeof(double) * k.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
         cudaFree(c->d);
@@ -132,14 +137,14 @@ EXOTX_API exotx_status exotx_gridpoint(exotx_plan p, exotx_gpconst c, int prec, 
         GpArgs<double> A;
         A.gin = (const double *)gin; A.gout = (double *)gout; A.dw = (double *)dw; A.dq = (const double *)dq;
         A.sid = p->d_sid; A.k = c->d; A.ncol = nhor * ninst;
-        A.L = L; A.nhor = (int)nhor; A.nlon = p->nlon; A.nqspec = c->h.nqspec;
+        A.L = L; A.nhor = (int)nhor; A.nlon = p->nlon; A.nqspec = c->h.nqspec; A.g_lower = c->g_lower;
         A.akap = c->h.akap; A.rdbrv = c->h.rdbrv; A.adv = c->h.adv; A.psurf = c->h.psurf; A.ww = c->h.ww;
         return launch_gridpoint_fp64(A, (cudaStream_t)s);
     }
     GpArgs<float> A;
     A.gin = (const float *)gin; A.gout = (float *)gout; A.dw = (float *)dw; A.dq = (const float *)dq;
     A.sid = p->d_sid; A.k = c->d; A.ncol = nhor * ninst;
-    A.L = L; A.nhor = (int)nhor; A.nlon = p->nlon; A.nqspec = c->h.nqspec;
+    A.L = L; A.nhor = (int)nhor; A.nlon = p->nlon; A.nqspec = c->h.nqspec; A.g_lower = c->g_lower;
     A.akap = c->h.akap; A.rdbrv = c->h.rdbrv; A.adv = c->h.adv; A.psurf = c->h.psurf; A.ww = c->h.ww;
     return launch_gridpoint_fp32(A, (cudaStream_t)s);
 }

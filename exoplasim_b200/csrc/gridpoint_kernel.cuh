@@ -18,6 +18,7 @@ struct GpArgs {
     const T *dq;            // nqspec == 0: grid humidity [inst][L][nhor]
     long long ncol;         // instances x nhor
     int L, nhor, nlon, nqspec;
+    int g_lower;            // g(i, k) = 0 for every i < k
     double akap, rdbrv, adv, psurf, ww;
 };
 
@@ -37,7 +38,9 @@ __host__ __device__ inline size_t gp_smem(int L, bool sk) {
     return sizeof(T) * (3 * (size_t)L * GP_THREADS + (sk ? 6 * (size_t)L + 2 * (size_t)L * L : 0));
 }
 
-template <typename T, bool SK>
+// LC > 0: the level count fixed at compile time, so the index arithmetic of
+// the profiles and constants folds (the arithmetic, and its order, is the same)
+template <typename T, bool SK, int LC>
 __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
     extern __shared__ __align__(16) unsigned char gsm[];
     T *sv = reinterpret_cast<T *>(gsm);                 // zvgpg      [L][GP_THREADS]
@@ -51,7 +54,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
     const GpConsts<T, SK> K{sk, A.k};
     const long long col = blockIdx.x * (long long)GP_THREADS + threadIdx.x;
     if (col >= A.ncol) return;
-    const int L = A.L, tx = threadIdx.x;
+    const int L = LC > 0 ? LC : A.L, tx = threadIdx.x;
     const long long inst = col / A.nhor;
     const int h = (int)(col - inst * A.nhor);
     const size_t n = (size_t)A.nhor;
@@ -115,6 +118,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
         } else {
             T ztpta = K(6 * L + L * L + 0 + L * k) * SH(sv, 0);
             T ztptb = K(6 * L + L * L + 0 + L * k) * SH(sb, 0);
+#pragma unroll 4
             for (int j = 1; j <= k; j++) {
                 ztpta = ztpta + K(6 * L + L * L + j + L * k) * SH(sv, j);
                 ztptb = ztptb + K(6 * L + L * L + j + L * k) * SH(sb, j);
@@ -136,9 +140,17 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
             }
             dwv = (zv - ztptb) * gp * (T)A.psurf * (T)A.ww;
         }
-        // non-linear geopotential, summed over every level as dot_product does
+        // non-linear geopotential, summed over every level as dot_product does;
+        // initsi's g is lower triangular (g(i, k) = 0 for i < k), and those
+        // exact zero terms leave the partial sum at +0, so they are skipped
         T dot = 0;
-        for (int i = 0; i < L; i++) dot = dot + K(6 * L + i + L * k) * SH(s1, i);
+        if (A.g_lower) {
+#pragma unroll 4
+            for (int i = k; i < L; i++) dot = dot + K(6 * L + i + L * k) * SH(s1, i);
+        } else {
+#pragma unroll 4
+            for (int i = 0; i < L; i++) dot = dot + K(6 * L + i + L * k) * SH(s1, i);
+        }
         const T gphi = dot * (T)2. / rc;
         T ke = gu * gu + gv * gv;
         ke = ke + gphi;
@@ -161,22 +173,26 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
 }
 
 // the launch: the constants in shared memory where they fit beside the profiles
+template <typename T, bool SK, int LC>
+inline exotx_status gp_launch_k(const GpArgs<T> &A, size_t smem, cudaStream_t s) {
+    const long long nb = (A.ncol + GP_THREADS - 1) / GP_THREADS;
+    if (smem > 48 * 1024)
+        EXOTX_CUDA(cudaFuncSetAttribute(k_gridpoint<T, SK, LC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gridpoint<T, SK, LC><<<(unsigned)nb, GP_THREADS, smem, s>>>(A);
+    EXOTX_CHECK_LAUNCH();
+    return EXOTX_OK;
+}
 template <typename T>
 inline exotx_status gp_launch(const GpArgs<T> &A, cudaStream_t s) {
     const bool sk = gp_smem<T>(A.L, true) <= 227 * 1024;
     const size_t smem = gp_smem<T>(A.L, sk);
-    const long long nb = (A.ncol + GP_THREADS - 1) / GP_THREADS;
-    if (sk) {
-        if (smem > 48 * 1024)
-            EXOTX_CUDA(cudaFuncSetAttribute(k_gridpoint<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_gridpoint<T, true><<<(unsigned)nb, GP_THREADS, smem, s>>>(A);
-    } else {
-        if (smem > 48 * 1024)
-            EXOTX_CUDA(cudaFuncSetAttribute(k_gridpoint<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_gridpoint<T, false><<<(unsigned)nb, GP_THREADS, smem, s>>>(A);
+    if (!sk) return gp_launch_k<T, false, 0>(A, smem, s);
+    switch (A.L) {   // the level counts of the standard configurations
+        case 10: return gp_launch_k<T, true, 10>(A, smem, s);
+        case 20: return gp_launch_k<T, true, 20>(A, smem, s);
+        case 25: return gp_launch_k<T, true, 25>(A, smem, s);
+        default: return gp_launch_k<T, true, 0>(A, smem, s);
     }
-    EXOTX_CHECK_LAUNCH();
-    return EXOTX_OK;
 }
 
 }  // namespace exotx
