@@ -58,12 +58,17 @@ __global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrala(const SpecArgs<T>
     const size_t n = (size_t)A.nrsp;
 #define V(a, lv) (a)[(size_t)(lv) * n + j]
 #define SH(a, lv, rr) a[(size_t)(lv) * R + (rr)]
+    // every value of this (real, level) the step reads, loaded at once
+    T v_sdt = 0, v_sdm = 0, v_szm = 0, v_sdp = 0, v_szp = 0, v_stp = 0, v_szt = 0, v_sqm = 0, v_sqp = 0, v_sqt = 0;
     // 0. the values at t-dt and the non-linear divergence tendency, saved
     int jn = 0;
     if (live) {
         jn = A.nidx[j];
         SH(s_stt, l, r) = V(A.stt, l);
         SH(s_atm, l, r) = V(A.stm, l);
+        v_sdt = V(A.sdt, l); v_sdm = V(A.sdm, l); v_szm = V(A.szm, l); v_sdp = V(A.sdp, l);
+        v_szp = V(A.szp, l); v_stp = V(A.stp, l); v_szt = V(A.szt, l);
+        if (A.nqspec == 1) { v_sqm = V(A.sqm, l); v_sqp = V(A.sqp, l); v_sqt = V(A.sqt, l); }
         if (l == 0) {
             s_r[4 * r + 0] = A.spt[j];
             s_r[4 * r + 1] = A.spm[j];
@@ -84,8 +89,8 @@ __global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrala(const SpecArgs<T>
         const T z0 = c_t0[l2];
         const T zt = zgt - z0 * spt0;
         const T zm = zgm + z0 * apm;
-        const T za = V(A.sdt, l2) * zq + sopj;
-        const T zb = V(A.sdm, l2) * zq;
+        const T za = v_sdt * zq + sopj;
+        const T zb = v_sdm * zq;
         SH(s_zz, l2, r) = zb + (T)A.delt * (zm + za + (T)A.delt * zt);
     }
     __syncthreads();
@@ -115,19 +120,19 @@ __global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrala(const SpecArgs<T>
         for (int i = 0; i < L; i++) dot = dot + c_tau[i + L * l] * SH(s_sd, i, r);
         const T stt = SH(s_stt, l, r) - dot;
         const T sd = SH(s_sd, l, r);
-        const T adm = V(A.sdm, l), azm = V(A.szm, l), atm = SH(s_atm, l, r);
+        const T adm = v_sdm, azm = v_szm, atm = SH(s_atm, l, r);
         V(A.stt, l) = stt;
         V(A.sdt, l) = sd;
-        V(A.sdm, l) = pnu21 * V(A.sdp, l) + pnu * adm;
-        V(A.szm, l) = pnu21 * V(A.szp, l) + pnu * azm;
-        V(A.stm, l) = pnu21 * V(A.stp, l) + pnu * atm;
+        V(A.sdm, l) = pnu21 * v_sdp + pnu * adm;
+        V(A.szm, l) = pnu21 * v_szp + pnu * azm;
+        V(A.stm, l) = pnu21 * v_stp + pnu * atm;
         V(A.sdp, l) = (T)2.0 * sd - adm;
         V(A.stp, l) = d2 * stt + atm;
-        V(A.szp, l) = d2 * V(A.szt, l) + azm;
+        V(A.szp, l) = d2 * v_szt + azm;
         if (A.nqspec == 1) {
-            const T aqm = V(A.sqm, l);
-            V(A.sqm, l) = pnu21 * V(A.sqp, l) + pnu * aqm;
-            V(A.sqp, l) = d2 * V(A.sqt, l) + aqm;
+            const T aqm = v_sqm;
+            V(A.sqm, l) = pnu21 * v_sqp + pnu * aqm;
+            V(A.sqp, l) = d2 * v_sqt + aqm;
         }
     }
 #undef V
