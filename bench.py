@@ -278,12 +278,10 @@ def dynamics_step(a, plan, spin64, gin64, B, world, time_graph, dev):
         plan.inverse_set_batch(state, L, precision="mixed", out=ga)
         GP.gridpoint(plan, gpc, ga, gf)
         plan.forward_set_batch(gf, L, precision="mixed", out=tend_a)
-        for st in states_a:
-            SP.spectrala(spc, st)
+        SP.spectrala_batch(spc, states_a)
         plan.inverse_set_d_batch(state, L, "mixed", out=gd)
         plan.forward_set_d_batch(phys, L, "mixed", out=tend_d)
-        for st in states_d:
-            SP.spectrald(spc, st)
+        SP.spectrald_batch(spc, states_d)
 
     ms, nl, st_ms = time_graph(step, a.steps, a.warmup, with_steps=True)
     med = max_over_ranks(statistics.median(st_ms))

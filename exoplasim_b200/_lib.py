@@ -97,6 +97,8 @@ SIGNATURES = {
     "exotx_specconst_destroy": [_P],
     "exotx_spectrala": [_P, _I, _P, _S],
     "exotx_spectrald": [_P, _I, _P, _S],
+    "exotx_spectrala_batch": [_P, _I, _P, _I, _S],
+    "exotx_spectrald_batch": [_P, _I, _P, _I, _S],
     "exotx_raw_pack": [_P, _I, _P, _S],
     "exotx_sets_host": [_P, _I, _P, _P, _P, _P, _I, _I, _S],
     "exotx_sets_host_f64": [_P, _I, _P, _P, _P, _P, _I, _I, _S],

@@ -19,10 +19,10 @@ struct exotx_specconst_s {
 };
 
 namespace exotx {
-exotx_status launch_spectral_fp64(const SpecArgs<double> &A, bool d_part, cudaStream_t s);
+exotx_status launch_spectral_fp64(const SpecBatch<double> &P, int n, bool d_part, cudaStream_t s);
 
-static exotx_status launch_spectral_fp32(const SpecArgs<float> &A, bool d_part, cudaStream_t s) {
-    return spec_launch<float>(A, d_part, s);
+static exotx_status launch_spectral_fp32(const SpecBatch<float> &P, int n, bool d_part, cudaStream_t s) {
+    return spec_launch<float>(P, n, d_part, s);
 }
 }  // namespace exotx
 
@@ -219,21 +219,50 @@ static SpecArgs<T> spec_args(exotx_specconst c, const exotx_spec_state *s) {
     return A;
 }
 
-static exotx_status spec_run(exotx_specconst c, int prec, const exotx_spec_state *s, bool d_part, exotx_stream st) {
-    if (!c || !s || (prec != EXOTX_FP64 && prec != EXOTX_FP32)) return EXOTX_BAD_ARG;
+static bool spec_state_ok(exotx_specconst c, const exotx_spec_state *s, bool d_part) {
     const void *need[] = {s->sdp, s->szp, s->stp, s->spp, s->sdm, s->szm, s->stm, s->spm,
                           s->sdt, s->szt, s->stt, s->spt};
-    for (const void *q : need) if (!q) return EXOTX_BAD_ARG;
-    if (c->h.nqspec == 1 && (!s->sqp || !s->sqm || !s->sqt)) return EXOTX_BAD_ARG;
-    if (!d_part && !s->sop) return EXOTX_BAD_ARG;
-    if (d_part && !s->srp) return EXOTX_BAD_ARG;
-    if (prec == EXOTX_FP64) return launch_spectral_fp64(spec_args<double>(c, s), d_part, (cudaStream_t)st);
-    return launch_spectral_fp32(spec_args<float>(c, s), d_part, (cudaStream_t)st);
+    for (const void *q : need) if (!q) return false;
+    if (c->h.nqspec == 1 && (!s->sqp || !s->sqm || !s->sqt)) return false;
+    if (!d_part && !s->sop) return false;
+    if (d_part && !s->srp) return false;
+    return true;
+}
+
+template <typename T>
+static exotx_status spec_run_t(exotx_specconst c, const exotx_spec_state *s, int n, bool d_part, cudaStream_t st) {
+    for (int i0 = 0; i0 < n; i0 += SPEC_MAXB) {
+        const int nb = n - i0 < SPEC_MAXB ? n - i0 : SPEC_MAXB;
+        SpecBatch<T> P;
+        for (int i = 0; i < nb; i++) P.s[i] = spec_args<T>(c, s + i0 + i);
+        for (int i = nb; i < SPEC_MAXB; i++) P.s[i] = P.s[0];
+        if constexpr (sizeof(T) == 8) EXOTX_TRY(launch_spectral_fp64(P, nb, d_part, st));
+        else EXOTX_TRY(launch_spectral_fp32(P, nb, d_part, st));
+    }
+    return EXOTX_OK;
+}
+
+static exotx_status spec_run(exotx_specconst c, int prec, const exotx_spec_state *s, int n, bool d_part,
+                             exotx_stream st) {
+    if (!c || !s || n < 0 || (prec != EXOTX_FP64 && prec != EXOTX_FP32)) return EXOTX_BAD_ARG;
+    for (int i = 0; i < n; i++)
+        if (!spec_state_ok(c, s + i, d_part)) return EXOTX_BAD_ARG;
+    if (n == 0) return EXOTX_OK;
+    if (prec == EXOTX_FP64) return spec_run_t<double>(c, s, n, d_part, (cudaStream_t)st);
+    return spec_run_t<float>(c, s, n, d_part, (cudaStream_t)st);
 }
 
 EXOTX_API exotx_status exotx_spectrala(exotx_specconst c, int prec, const exotx_spec_state *s, exotx_stream st) {
-    return spec_run(c, prec, s, false, st);
+    return spec_run(c, prec, s, 1, false, st);
 }
 EXOTX_API exotx_status exotx_spectrald(exotx_specconst c, int prec, const exotx_spec_state *s, exotx_stream st) {
-    return spec_run(c, prec, s, true, st);
+    return spec_run(c, prec, s, 1, true, st);
+}
+EXOTX_API exotx_status exotx_spectrala_batch(exotx_specconst c, int prec, const exotx_spec_state *states, int ninst,
+                                             exotx_stream st) {
+    return spec_run(c, prec, states, ninst, false, st);
+}
+EXOTX_API exotx_status exotx_spectrald_batch(exotx_specconst c, int prec, const exotx_spec_state *states, int ninst,
+                                             exotx_stream st) {
+    return spec_run(c, prec, states, ninst, true, st);
 }

@@ -4,7 +4,7 @@
 #include "spectral_kernel.cuh"
 
 namespace exotx {
-exotx_status launch_spectral_fp64(const SpecArgs<double> &A, bool d_part, cudaStream_t s) {
-    return spec_launch<double>(A, d_part, s);
+exotx_status launch_spectral_fp64(const SpecBatch<double> &P, int n, bool d_part, cudaStream_t s) {
+    return spec_launch<double>(P, n, d_part, s);
 }
 }  // namespace exotx

@@ -29,6 +29,13 @@ struct SpecArgs {
     double delt, delt2, pnu, pnu21, plavor, dampsp;
 };
 
+// up to SPEC_MAXB model states in one launch (blockIdx.y: the state)
+constexpr int SPEC_MAXB = 12;
+template <typename T>
+struct SpecBatch {
+    SpecArgs<T> s[SPEC_MAXB];
+};
+
 // Both steps work on a block of R spectral reals (threadIdx.x) by L levels
 // (threadIdx.y): each thread owns one (real, level) value of every array, and
 // the level profiles a real needs across levels sit in shared memory as
@@ -43,7 +50,8 @@ __host__ __device__ inline size_t spec_smem_a(int L) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrala(const SpecArgs<T> A) {
+__global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrala(const __grid_constant__ SpecBatch<T> P) {
+    const SpecArgs<T> &A = P.s[blockIdx.y];
     extern __shared__ __align__(16) unsigned char ssm[];
     const int L = A.L, R = blockDim.x, r = threadIdx.x, l = threadIdx.y;
     T *c_g = reinterpret_cast<T *>(ssm), *c_tau = c_g + (size_t)L * L, *c_t0 = c_tau + (size_t)L * L,
@@ -142,7 +150,8 @@ __global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrala(const SpecArgs<T>
 // spectrald: one thread per (real, level); the sponge's coupling of the top
 // level to the second goes through shared memory
 template <typename T>
-__global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrald(const SpecArgs<T> A) {
+__global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrald(const __grid_constant__ SpecBatch<T> P) {
+    const SpecArgs<T> &A = P.s[blockIdx.y];
     __shared__ T s_stp[2][32];
     const int L = A.L, r = threadIdx.x, l = threadIdx.y;
     const int j = blockIdx.x * blockDim.x + r;
@@ -213,18 +222,20 @@ __global__ void __launch_bounds__(SPEC_MAXTHREADS) k_spectrald(const SpecArgs<T>
 #undef V
 }
 
-// launch shapes: blocks of spec_reals(L) reals by L levels
+// launch shapes: blocks of spec_reals(L) reals by L levels, states along y
+// (every state of a batch has the plan's NRSP and the constants' L)
 template <typename T>
-inline exotx_status spec_launch(const SpecArgs<T> &A, bool d_part, cudaStream_t s) {
+inline exotx_status spec_launch(const SpecBatch<T> &P, int n, bool d_part, cudaStream_t s) {
+    const SpecArgs<T> &A = P.s[0];
     const int R = spec_reals(A.L);
-    const dim3 block((unsigned)R, (unsigned)A.L), grid((unsigned)((A.nrsp + R - 1) / R));
+    const dim3 block((unsigned)R, (unsigned)A.L), grid((unsigned)((A.nrsp + R - 1) / R), (unsigned)n);
     if (d_part) {
-        k_spectrald<T><<<grid, block, 0, s>>>(A);
+        k_spectrald<T><<<grid, block, 0, s>>>(P);
     } else {
         const size_t smem = spec_smem_a<T>(A.L);
         if (smem > 48 * 1024)
             EXOTX_CUDA(cudaFuncSetAttribute(k_spectrala<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_spectrala<T><<<grid, block, smem, s>>>(A);
+        k_spectrala<T><<<grid, block, smem, s>>>(P);
     }
     EXOTX_CHECK_LAUNCH();
     return EXOTX_OK;

@@ -84,3 +84,27 @@ def spectrala(const, st):
 def spectrald(const, st):
     s, prec = _state(st)
     call("exotx_spectrald", const._h, prec, C.byref(s), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+
+def _states(sts):
+    arr = (SpecState * len(sts))()
+    prec = None
+    for i, st in enumerate(sts):
+        s, p = _state(st)
+        if prec is not None and p != prec:
+            raise TypeError("every state of a batch has one precision")
+        prec = p
+        arr[i] = s
+    return arr, prec
+
+
+def spectrala_batch(const, states):
+    """spectrala of several states in one launch per 12 (exotx_spectrala_batch)."""
+    arr, prec = _states(states)
+    call("exotx_spectrala_batch", const._h, prec, arr, len(states), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+
+def spectrald_batch(const, states):
+    """spectrald of several states in one launch per 12 (exotx_spectrald_batch)."""
+    arr, prec = _states(states)
+    call("exotx_spectrald_batch", const._h, prec, arr, len(states), C.c_void_p(torch.cuda.current_stream().cuda_stream))

@@ -342,6 +342,12 @@ typedef struct {
 } exotx_spec_state;
 exotx_status exotx_spectrala(exotx_specconst c, int prec, const exotx_spec_state *s, exotx_stream st);
 exotx_status exotx_spectrald(exotx_specconst c, int prec, const exotx_spec_state *s, exotx_stream st);
+/* the same for ninst states (a HOST array of state structs), in one launch per
+ * 12 states; results equal ninst single calls' */
+exotx_status exotx_spectrala_batch(exotx_specconst c, int prec, const exotx_spec_state *states, int ninst,
+                                   exotx_stream st);
+exotx_status exotx_spectrald_batch(exotx_specconst c, int prec, const exotx_spec_state *states, int ninst,
+                                   exotx_stream st);
 
 /* ---- radiation column pass (radmod.f90 radstep :927-1110) ---- */
 typedef struct {

@@ -72,3 +72,26 @@ def test_spectral_step_matches_oracle(oracle, nlat, nlev, over, prec):
             (("sqp", "sqm", "sqt") if p.nqspec == 1 else ()):
         assert relerr(got[k], ref_d[k]) < tol, ("d", k)
     assert got["spp"][0] == 0.0 and got["spp"][1] == 0.0
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_spectral_batch_equals_single_calls(prec):
+    # exotx_spectrala_batch / exotx_spectrald_batch over 13 states (two
+    # launches of up to 12) give each state what a single call gives
+    from exoplasim_b200.transforms import Plan
+    P = Plan(32)
+    nlev, n = 10, 13
+    const = SP.SpecConst(P, SP.default_params(nlev, nsponge=1, dampsp=0.3))
+    dt = torch.float64 if prec == "fp64" else torch.float32
+    states = [{k: torch.as_tensor(v, device="cuda").to(dt).contiguous() for k, v in _state(P.ntru, nlev, 50 + i).items()}
+              for i in range(n)]
+    single = [{k: v.clone() for k, v in st.items()} for st in states]
+    SP.spectrala_batch(const, states)
+    SP.spectrald_batch(const, states)
+    for st in single:
+        SP.spectrala(const, st)
+        SP.spectrald(const, st)
+    torch.cuda.synchronize()
+    for a, b in zip(states, single):
+        for k in a:
+            assert torch.equal(a[k], b[k]), k
