@@ -88,8 +88,14 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
     T psd = 0, psv = 0;                 // running sums of dsigma * gd and of dsigma * zvgpg
     T gtd_m = 0, gqm_m = 0, gud_m = 0, gvd_m = 0;   // the level above's products
     T zs = 0;                           // zsumd of the tendency loop (plasim.f90:2661, :2692)
+    // the next level's fields are loaded one iteration ahead (n* = level k + 1)
+    T nu = IN(0, 0), nv = IN(1, 0), nt = IN(2, 0), nd = IN(3, 0), nz = IN(4, 0), nq = IN(5, 0);
     for (int k = 0; k < L; k++) {
-        const T gu = IN(0, k), gv = IN(1, k), gt = IN(2, k), gd = IN(3, k), gz = IN(4, k), gq = IN(5, k);
+        const T gu = nu, gv = nv, gt = nt, gd = nd, gz = nz, gq = nq;
+        if (k + 1 < L) {
+            nu = IN(0, k + 1); nv = IN(1, k + 1); nt = IN(2, k + 1);
+            nd = IN(3, k + 1); nz = IN(4, k + 1); nq = IN(5, k + 1);
+        }
         const T zv = SH(sv, k);
         T zq;
         if (A.nqspec == 1) zq = fmax(gq / gp, (T)0.);
@@ -102,10 +108,10 @@ __global__ void __launch_bounds__(GP_THREADS) k_gridpoint(const GpArgs<T> A) {
             if (k == 0) { psd = K(0) * gd; psv = K(0) * zv; }
             else { psd = psd + K(k) * gd; psv = psv + K(k) * zv; }
             const T zsdotp = (K(L + k) * tot - (psd + psv));
-            gtd = zsdotp * (IN(2, k + 1) - gt);
-            gqm = zsdotp * (IN(5, k + 1) + gq);
-            gud = zsdotp * (IN(0, k + 1) - gu);
-            gvd = zsdotp * (IN(1, k + 1) - gv);
+            gtd = zsdotp * (nt - gt);
+            gqm = zsdotp * (nq + gq);
+            gud = zsdotp * (nu - gu);
+            gvd = zsdotp * (nv - gv);
         }
         T gtn, gqn, guz, gvz, dwv;
         if (k == 0) {
