@@ -119,6 +119,7 @@ SIGNATURES = {
     "exotx_mlp_forward": [_P, _P, _P, _I, _S],
     "exotx_mlp_backward": [_P, _P, _P, _I, _P, _S],
     "exotx_mlp_backward_weighted": [_P, _P, _P, _P, _I, _P, _S],
+    "exotx_mlp_check": [_P, _S],
     "exotx_mlp_adam": [_P, C.c_float, C.c_float, C.c_float, C.c_float, _I, _S],
     "exotx_mlp_prepare": [_P, _S],
     "exotx_surr_features": [C.POINTER(RadParams), _I, C.POINTER(RadIO), _P, _S],

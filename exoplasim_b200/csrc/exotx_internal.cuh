@@ -211,6 +211,13 @@ exotx_status tc_ens_run(const EnsSeg *segs, int nseg, int dir, const int4 *d_job
                         int nprod, cudaStream_t s);
 bool tc_ens_fwd_folded(const EnsSeg *segs, int nseg);
 exotx_status tc_ens_n0(const EnsSeg *segs, const float *const *gpin, int nseg, cudaStream_t s);
+// FP32-accurate GEMM on the tensor cores (tc_gemm.cu): C = A B (+ bias), A(m,k) = A[m*am + k*ak],
+// B(k,n) = B[k*bk + n*bn]; work: tc_sgemm_work(M, N, K) floats (0: none needed)
+exotx_status tc_sgemm(int M, int N, int K, const float *A, long long am, long long ak, const float *B, long long bk,
+                      long long bn, float *C, long long ldc, const float *bias, float *work, size_t work_elems,
+                      cudaStream_t s);
+size_t tc_sgemm_work(int M, int N, int K);
+exotx_status tc_sgemm_error(int *err, cudaStream_t s);
 exotx_status tc_error_reset(cudaStream_t s);
 exotx_status tc_error_read(int *err, cudaStream_t s);
 // the same for the FFT kernels' bounded waits (fft.cu)

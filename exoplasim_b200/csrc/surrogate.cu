@@ -40,6 +40,8 @@ struct exotx_mlp_s {
     bool prepared = false;
     int *fb = nullptr;       // [0] = fallback count, [1..] = column list
     int fb_cap = 0;
+    float *split = nullptr;  // split-K workspace of the weight-gradient GEMMs
+    size_t split_elems = 0;
 };
 
 namespace exotx {
@@ -119,69 +121,9 @@ __global__ void k_surr_targets(SurrIn<T> in, const T *dtdt, const T *dfd, const 
 }
 
 // ------------------------------------------------------------ training (FP32)
-// C[m][n] = sum_k A(m,k) B(k,n) (+ bias[n]), A(m,k) = A[m*am + k*ak], B(k,n) = B[k*bk + n*bn].
-// 64x64 tiles, 256 threads, 4x4 outputs per thread (rows ty+16i, columns tx+16j).
-__global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, const float *__restrict__ A, long long am,
-                                               long long ak, const float *__restrict__ B, long long bk,
-                                               long long bn, float *__restrict__ C, long long ldc,
-                                               const float *__restrict__ bias) {
-    __shared__ float As[16][64 + 4], Bs[16][64 + 4];
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const long long m0 = (long long)blockIdx.y * 64, n0 = (long long)blockIdx.x * 64;
-    float acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
-    for (int k0 = 0; k0 < K; k0 += 16) {
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int e = tid + 256 * i;
-            int mm, kk;
-            if (ak == 1) { mm = e >> 4; kk = e & 15; } else { kk = e >> 6; mm = e & 63; }
-            const long long gm = m0 + mm;
-            const int gk = k0 + kk;
-            As[kk][mm] = (gm < M && gk < K) ? A[gm * am + gk * ak] : 0.f;
-            int nn, kb;
-            if (bn == 1) { kb = e >> 6; nn = e & 63; } else { nn = e >> 4; kb = e & 15; }
-            const long long gn = n0 + nn;
-            const int gkb = k0 + kb;
-            Bs[kb][nn] = (gn < N && gkb < K) ? B[gkb * bk + gn * bn] : 0.f;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < 16; kk++) {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = As[kk][ty + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const long long gm = m0 + ty + 16 * i;
-        if (gm >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const long long gn = n0 + tx + 16 * j;
-            if (gn < N) C[gm * ldc + gn] = acc[i][j] + (bias ? bias[gn] : 0.f);
-        }
-    }
-}
-
-static exotx_status sgemm(int M, int N, int K, const float *A, long long am, long long ak, const float *B,
-                          long long bk, long long bn, float *C, long long ldc, const float *bias, cudaStream_t s) {
-    dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
-    k_sgemm<<<grid, 256, 0, s>>>(M, N, K, A, am, ak, B, bk, bn, C, ldc, bias);
-    EXOTX_CHECK_LAUNCH();
-    return EXOTX_OK;
-}
+// The three GEMMs of a layer's forward and backward pass run on the tensor
+// cores in FP32-accurate split form (tc_sgemm, tc_gemm.cu); the element-wise
+// parts are the kernels below.
 
 __device__ __forceinline__ float silu(float z) { return z / (1.f + expf(-z)); }
 __device__ __forceinline__ float silu_grad(float z) {
@@ -267,12 +209,18 @@ static float *ws_dY(exotx_mlp net) { return ws_Y(net) + (size_t)net->maxb * net-
 static float *ws_dA(exotx_mlp net) { return ws_dY(net) + (size_t)net->maxb * net->nout; }
 static float *ws_dZ(exotx_mlp net, int i) { return ws_dA(net) + (size_t)(1 + i) * net->maxb * net->width; }
 
+static exotx_status gemm(exotx_mlp net, int M, int N, int K, const float *A, long long am, long long ak,
+                         const float *B, long long bk, long long bn, float *C, long long ldc, const float *bias,
+                         cudaStream_t s) {
+    return tc_sgemm(M, N, K, A, am, ak, B, bk, bn, C, ldc, bias, net->split, net->split_elems, s);
+}
+
 static exotx_status mlp_forward(exotx_mlp net, const float *X, int n, cudaStream_t s) {
     const float *H = X;
     for (int l = 0; l < net->nl; l++) {
         const int din = net->din[l], dout = net->dout[l];
         float *Z = l < net->nhid ? ws_Z(net, l) : ws_Y(net);
-        EXOTX_TRY(sgemm(n, dout, din, H, din, 1, net->P + net->woff[l], 1, din, Z, dout, net->P + net->boff[l], s));
+        EXOTX_TRY(gemm(net, n, dout, din, H, din, 1, net->P + net->woff[l], 1, din, Z, dout, net->P + net->boff[l], s));
         if (l < net->nhid) {
             k_silu<<<grid_for((long long)n * dout), 256, 0, s>>>(Z, ws_H(net, l), (long long)n * dout);
             EXOTX_CHECK_LAUNCH();
@@ -657,14 +605,17 @@ EXOTX_API exotx_status exotx_mlp_create(int nin, int width, int nhidden, int nou
     net->nparams = off;
     const size_t wsf = (size_t)2 * nhidden * max_batch * width + (size_t)2 * max_batch * nout +
                        (size_t)3 * max_batch * width;
+    net->split_elems = tc_sgemm_work(std::max(width, nout), std::max(nin, width), max_batch);
     bool ok = cudaMalloc(&net->P, off * 4) == cudaSuccess && cudaMalloc(&net->G, off * 4) == cudaSuccess &&
               cudaMalloc(&net->M, off * 4) == cudaSuccess && cudaMalloc(&net->V, off * 4) == cudaSuccess &&
               cudaMalloc(&net->ws, wsf * 4) == cudaSuccess &&
-              cudaMalloc(&net->norm, sizeof(float) * (4 * nin + 2 * nout)) == cudaSuccess;
+              cudaMalloc(&net->norm, sizeof(float) * (4 * nin + 2 * nout)) == cudaSuccess &&
+              (net->split_elems == 0 || cudaMalloc(&net->split, net->split_elems * 4) == cudaSuccess);
     ok = ok && cudaMemset(net->P, 0, off * 4) == cudaSuccess && cudaMemset(net->G, 0, off * 4) == cudaSuccess &&
          cudaMemset(net->M, 0, off * 4) == cudaSuccess && cudaMemset(net->V, 0, off * 4) == cudaSuccess;
     if (!ok) {
         cudaFree(net->P); cudaFree(net->G); cudaFree(net->M); cudaFree(net->V); cudaFree(net->ws); cudaFree(net->norm);
+        cudaFree(net->split);
         delete net;
         return EXOTX_NO_MEM;
     }
@@ -675,7 +626,7 @@ EXOTX_API exotx_status exotx_mlp_create(int nin, int width, int nhidden, int nou
 EXOTX_API exotx_status exotx_mlp_destroy(exotx_mlp net) {
     if (!net) return EXOTX_BAD_ARG;
     cudaFree(net->P); cudaFree(net->G); cudaFree(net->M); cudaFree(net->V); cudaFree(net->ws);
-    cudaFree(net->norm); cudaFree(net->tw); cudaFree(net->fb);
+    cudaFree(net->norm); cudaFree(net->tw); cudaFree(net->fb); cudaFree(net->split);
     delete net;
     return EXOTX_OK;
 }
@@ -732,12 +683,12 @@ EXOTX_API exotx_status exotx_mlp_backward_weighted(exotx_mlp net, const float *X
         const int din = net->din[l], dout = net->dout[l];
         const float *Hp = l > 0 ? ws_H(net, l - 1) : X;
         // dW = dZ^T H_prev, db = column sums of dZ
-        EXOTX_TRY(sgemm(dout, din, n, dZ, 1, dout, Hp, din, 1, net->G + net->woff[l], din, nullptr, s));
+        EXOTX_TRY(gemm(net, dout, din, n, dZ, 1, dout, Hp, din, 1, net->G + net->woff[l], din, nullptr, s));
         k_colsum<<<(dout + 31) / 32, 256, 0, s>>>(dZ, net->G + net->boff[l], n, dout);
         EXOTX_CHECK_LAUNCH();
         if (l > 0) {
             // dH_prev = dZ W, then through the SiLU of layer l-1
-            EXOTX_TRY(sgemm(n, din, dout, dZ, dout, 1, net->P + net->woff[l], din, 1, ws_dA(net), din, nullptr, s));
+            EXOTX_TRY(gemm(net, n, din, dout, dZ, dout, 1, net->P + net->woff[l], din, 1, ws_dA(net), din, nullptr, s));
             float *dZn = ws_dZ(net, cur);
             k_silu_bwd<<<grid_for((long long)n * din), 256, 0, s>>>(ws_dA(net), ws_Z(net, l - 1), dZn,
                                                                   (long long)n * din);
@@ -747,6 +698,13 @@ EXOTX_API exotx_status exotx_mlp_backward_weighted(exotx_mlp net, const float *X
         }
     }
     return EXOTX_OK;
+}
+
+EXOTX_API exotx_status exotx_mlp_check(exotx_mlp net, exotx_stream s) {
+    if (!net) return EXOTX_BAD_ARG;
+    int err = 0;
+    EXOTX_TRY(tc_sgemm_error(&err, (cudaStream_t)s));
+    return err ? EXOTX_TIMEOUT : EXOTX_OK;
 }
 
 EXOTX_API exotx_status exotx_mlp_adam(exotx_mlp net, float lr, float b1, float b2, float eps, int step,

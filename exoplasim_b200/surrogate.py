@@ -134,6 +134,10 @@ class Mlp:
     def prepare(self):
         call("exotx_mlp_prepare", self._h, _stream())
 
+    def check(self):
+        """Raise if a bounded wait of the tensor-core training GEMMs gave up."""
+        call("exotx_mlp_check", self._h, _stream())
+
     def save(self, path, **meta):
         np.savez(path, params=self.params.cpu().numpy(), nin=self.nin, nout=self.nout, width=self.width,
                  nhidden=self.nhidden, **{k: v for k, v in (self.norm or {}).items()}, **meta)
@@ -265,6 +269,7 @@ def train(net, X, Y, epochs=16, batch=4096, lr=1e-3, lr_min=1e-5, seed=0, log=No
             net.backward(xb, yb, loss, wb)
             net.adam(rate, step)
         ep_loss = loss.item() / steps_per_epoch
+        net.check()
         hist.append(ep_loss)
         if log:
             log(f"epoch {ep + 1}/{epochs}  loss {ep_loss:.5f}  {time.time() - t0:.1f} s")

@@ -411,6 +411,9 @@ exotx_status exotx_mlp_backward_weighted(exotx_mlp net, const float *X, const fl
                                          float *loss, exotx_stream s);
 exotx_status exotx_mlp_adam(exotx_mlp net, float lr, float beta1, float beta2, float eps, int step,
                             exotx_stream s);
+/* EXOTX_TIMEOUT if a bounded wait of the training GEMMs (tensor cores, FP32-accurate
+ * 3-term BF16 splits) gave up since the library was loaded; synchronises s */
+exotx_status exotx_mlp_check(exotx_mlp net, exotx_stream s);
 /* BF16 tensor-core copy of the current weights (width 256, nin <= 80, nout <= 32) */
 exotx_status exotx_mlp_prepare(exotx_mlp net, exotx_stream s);
 /* raw features X (nhor x (3L+9)) and targets Y (nhor x (L+4)) of radstep columns:
