@@ -14,8 +14,8 @@
 // the MMAs of the previous chunk (tcgen05.mma, kind::f16, M = 128); a commit
 // per chunk frees its buffer.  Long K (the weight gradient's sum over the
 // batch) is split over CTAs (grid z) into a workspace that a second kernel
-// sums in a fixed order.  Every wait is bounded and reports through the error
-// word read by exotx_surr_error.
+// sums in a fixed order.  Every wait is bounded and reports through an error
+// word that exotx_mlp_check reads.
 #include <algorithm>
 #include "exotx_internal.cuh"
 #include "tc_prims.cuh"
