@@ -48,7 +48,7 @@ def _oracle_step(oracle, p, gin, nlat, nlev, sid, nqspec=1, dq=None):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nlat,nlev,nqspec", [(32, 10, 1), (64, 20, 1), (32, 10, 0), (96, 15, 1)])
+@pytest.mark.parametrize("nlat,nlev,nqspec", [(32, 10, 1), (64, 20, 1), (32, 10, 0), (96, 15, 1), (32, 25, 1)])
 def test_gridpoint_fp64_fp32(oracle, nlat, nlev, nqspec):
     from exoplasim_b200.transforms import Plan
     P = Plan(nlat)
