@@ -36,7 +36,7 @@ def chunk():
     return params, dev, X, Y, cols, out
 
 
-@pytest.mark.parametrize("width,nhid,n", [(32, 2, 64), (256, 6, 256)])
+@pytest.mark.parametrize("width,nhid,n", [(32, 2, 64), (256, 6, 256), (64, 2, 1100)])
 def test_forward_and_gradients_vs_oracle(width, nhid, n):
     from oracle import mlp_oracle as MO
     net = SG.Mlp(NIN, NOUT, width=width, nhidden=nhid, max_batch=n)
