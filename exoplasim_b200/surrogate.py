@@ -2,17 +2,21 @@
 
 An MLP (3L+9 inputs -> 6 hidden layers of 256, SiLU -> L+4 outputs) learns
 radmod's column map (radmod.f90 radstep :927-1110): the heating-rate profile
-(K/day) and the four surface fluxes (dfd, dfu, dftd, dftu at NLEP).  Its
+(K/day) and the four surface fluxes (dfd, dfu, dftd, dftu at NLEP).  The
+inputs are the column's temperatures, humidity (as vertical log-gradients and
+the surface value), cloud cover, surface pressure, albedo, zenith angle, CO2,
+star and latitude.  Its
 training columns come from the plain GPU radstep kernel in FP64; training
 runs on the library's FP32 kernels (exotx_mlp_backward / exotx_mlp_adam);
 inference (exotx_rad_surrogate) runs the network in BF16 on the tensor cores
 and computes every column whose inputs leave the training ranges with the
 plain radstep kernel.
 
-    python -m exoplasim_b200.surrogate --train OUT.npz [--columns 2000000] [--epochs 400]
+    python -m exoplasim_b200.surrogate --train OUT.npz [--columns 16000000] [--epochs 50]
 
 The packaged network (data/rad_surrogate_L20.npz) was trained this way with
-the defaults: 2M columns, 400 epochs of Adam with cosine decay from 1e-3.
+the defaults: 16M structured columns (synthetic.radiation_columns), 50 epochs
+of Adam with cosine decay from 1e-3, the loss in K/day (judged_weights).
 """
 import argparse
 import ctypes as C
@@ -31,6 +35,7 @@ from ._lib import FP32, FP64, call
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 DEFAULT_NET = os.path.join(DATA, "rad_surrogate_L20.npz")
 GRID_NLAT = 64            # training columns are laid out on T42 grids (64 x 128 = 8192 columns)
+PROFILES = "structured"   # vertically coherent training columns (synthetic.radiation_columns)
 
 
 def nin_for(nlev):
@@ -173,9 +178,9 @@ def zsol_for(teff):
     return np.stack([np.interp(teff, t, tab[:, k]) for k in range(3)])
 
 
-def column_chunk(nlev, seed, dtype=torch.float64):
+def column_chunk(nlev, seed, dtype=torch.float64, profiles=PROFILES):
     """One T42 grid of synthetic columns on the device with per-column stars."""
-    cols, g = S.radiation_columns(GRID_NLAT, nlev, seed=seed, teff=True)
+    cols, g = S.radiation_columns(GRID_NLAT, nlev, seed=seed, teff=True, profiles=profiles)
     zsol = zsol_for(cols.pop("teff"))
     dev = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=dtype, device="cuda") for k, v in cols.items()}
     dev["zsol"] = torch.as_tensor(np.ascontiguousarray(zsol), dtype=dtype, device="cuda")
@@ -203,12 +208,12 @@ def plain_targets(params, dev, precision="fp64"):
     return Y, cols, out
 
 
-def dataset(ncols, nlev=20, seed=1000):
+def dataset(ncols, nlev=20, seed=1000, profiles=PROFILES):
     """Features and targets of ncols synthetic columns (a multiple of 8192)."""
     nchunk = max(1, ncols // (2 * GRID_NLAT * GRID_NLAT))
     Xs, Ys = [], []
     for i in range(nchunk):
-        params, dev = column_chunk(nlev, seed + i)
+        params, dev = column_chunk(nlev, seed + i, profiles=profiles)
         Xs.append(features(params, dev))
         Ys.append(plain_targets(params, dev)[0])
     return torch.cat(Xs), torch.cat(Ys)
@@ -294,8 +299,15 @@ def heating_scale(X, nlev, adv):
     divided by this is the heating rate in K/day (X holds raw features)."""
     L = nlev
     ps = torch.exp(X[:, 3 * L + 2].double())
-    q = torch.exp(X[:, L + 1:2 * L + 1].double())
-    return (ps / 1e5)[:, None] * (1.0 + adv * q)
+    return (ps / 1e5)[:, None] * (1.0 + adv * torch.exp(log_humidity(X, L)))
+
+
+def log_humidity(X, nlev):
+    """ln q on the L full levels from the raw features: ln q(L) plus the sum of
+    the log-gradients ln q(j) - ln q(j+1) from the level down to the surface."""
+    L = nlev
+    d = X[:, L + 1:2 * L + 1].double()
+    return X[:, 2 * L + 1].double()[:, None] + torch.flip(torch.cumsum(torch.flip(d, [1]), 1), [1])
 
 
 def heating_rms(pred_dtdt, ref_dtdt):
@@ -303,12 +315,12 @@ def heating_rms(pred_dtdt, ref_dtdt):
     return float(torch.sqrt(torch.mean(((pred_dtdt - ref_dtdt) * 86400.0) ** 2)))
 
 
-def evaluate(net, nlev=20, seed=900000, nchunk=4, precision="fp64"):
+def evaluate(net, nlev=20, seed=900000, nchunk=4, precision="fp64", profiles=PROFILES):
     """Surrogate vs plain radstep on fresh columns: heating RMS (K/day), surface-flux
     RMS (W/m2) and the fallback fraction."""
     se, sf, ncol, nfb = 0.0, 0.0, 0, 0
     for i in range(nchunk):
-        params, dev = column_chunk(nlev, seed + i)
+        params, dev = column_chunk(nlev, seed + i, profiles=profiles)
         Y, pcols, _ = plain_targets(params, dev)
         cols = {k: v.clone() for k, v in dev.items()}
         cols["dtdt"].zero_()
@@ -325,7 +337,7 @@ def evaluate(net, nlev=20, seed=900000, nchunk=4, precision="fp64"):
             "columns": ncol}
 
 
-def fallback_curve(net, ps_min_list, nlev=20, seed=900000, nchunk=4):
+def fallback_curve(net, ps_min_list, nlev=20, seed=900000, nchunk=4, profiles=PROFILES):
     """Heating RMS against the fallback fraction when columns with surface
     pressure below ps_min go to the plain radstep kernel: the range test of
     exotx_rad_surrogate with the lower bound of the ln ps feature raised to
@@ -339,7 +351,7 @@ def fallback_curve(net, ps_min_list, nlev=20, seed=900000, nchunk=4):
             xlo = nrm["xlo"].copy()
             xlo[ips] = max(xlo[ips], math.log(pmin)) if pmin > 0 else xlo[ips]
             net.set_norm(nrm["xm"], nrm["xs"], xlo, nrm["xhi"], nrm["ym"], nrm["ys"])
-            ev = evaluate(net, nlev, seed, nchunk)
+            ev = evaluate(net, nlev, seed, nchunk, profiles=profiles)
             rows.append((pmin, ev["fallback_fraction"], ev["heating_rms_K_per_day"], ev["surface_flux_rms_W_m2"]))
     finally:
         net.set_norm(nrm["xm"], nrm["xs"], nrm["xlo"], nrm["xhi"], nrm["ym"], nrm["ys"])
@@ -349,27 +361,32 @@ def fallback_curve(net, ps_min_list, nlev=20, seed=900000, nchunk=4):
 def main():
     a = argparse.ArgumentParser()
     a.add_argument("--train", required=True, help="output .npz")
-    a.add_argument("--columns", type=int, default=2_000_000)
-    a.add_argument("--epochs", type=int, default=400)
+    a.add_argument("--columns", type=int, default=16_000_000)
+    a.add_argument("--epochs", type=int, default=50)
     a.add_argument("--batch", type=int, default=4096)
     a.add_argument("--lr", type=float, default=1e-3)
     a.add_argument("--nlev", type=int, default=20)
     a.add_argument("--seed", type=int, default=0)
-    a.add_argument("--weighted", action="store_true", help="loss in K/day (and W/m2) instead of normalised units")
+    a.add_argument("--loss", default="kday", choices=("kday", "normalised"),
+                   help="squared error in K/day (and W/m2, judged_weights) or in normalised output units")
+    a.add_argument("--profiles", default=PROFILES, choices=("structured", "independent"),
+                   help="column generator of the training and evaluation columns")
     args = a.parse_args()
     t0 = time.time()
-    X, Y = dataset(args.columns, args.nlev, seed=1000)
+    X, Y = dataset(args.columns, args.nlev, seed=1000, profiles=args.profiles)
     print(f"dataset {X.shape[0]} columns in {time.time() - t0:.1f} s", flush=True)
     net = Mlp(nin_for(args.nlev), nout_for(args.nlev), max_batch=args.batch)
     net.init(args.seed)
     net.set_norm(*norm_stats(X, Y))
     adv = R.default_params(args.nlev, 2 * GRID_NLAT * GRID_NLAT, 2 * GRID_NLAT).adv
     hist = train(net, X, Y, epochs=args.epochs, batch=args.batch, lr=args.lr,
-                 log=lambda s: print(s, flush=True), weighted=args.weighted, adv=adv)
-    ev = evaluate(net, args.nlev)
+                 log=lambda s: print(s, flush=True), weighted=args.loss == "kday", adv=adv)
+    ev = evaluate(net, args.nlev, profiles=args.profiles)
     print(ev, flush=True)
+    other = "independent" if args.profiles == "structured" else "structured"
+    print(f"{other} columns:", evaluate(net, args.nlev, profiles=other), flush=True)
     net.save(args.train, loss=np.array(hist), columns=X.shape[0], epochs=args.epochs,
-             heating_rms=ev["heating_rms_K_per_day"])
+             heating_rms=ev["heating_rms_K_per_day"], profiles=args.profiles)
 
 
 if __name__ == "__main__":

@@ -79,9 +79,10 @@ def sigma_levels(nlev):
     return sigma, sigmah, dsigma
 
 
-def radiation_columns(nlat, nlev, seed=2, teff=False):
+def radiation_columns(nlat, nlev, seed=2, teff=False, profiles="independent"):
     """Synthetic radiation columns on an NLAT x 2NLAT grid (nhor = 2 NLAT^2).
 
+    profiles="independent" (every level drawn on its own):
     T(surface) ~ U(150,350) K, lapse rate ~ U(0,9) K/km over heights
     z = -(R T_s/g) ln(sigma) plus N(0, 5 K) noise, clipped to [150,350];
     q log-uniform [1e-7, 3e-2] kg/kg; cloud cover U(0,1); cloud water
@@ -89,7 +90,18 @@ def radiation_columns(nlat, nlev, seed=2, teff=False):
     log-uniform [1e-5, 1e-1] vmr (as ppmv); cos zenith from a tidally locked
     substellar point at (0 N, 180 E) scaled by U(0.5, 1) (zero on the night
     side); optional Teff U(2500, 6000) K per column.
+
+    profiles="structured" (vertically coherent columns, as a model state has
+    them; the same ranges of surface temperature, humidity, ps, albedo, CO2,
+    zenith angle and Teff): T as above with N(0, 1 K) level noise and an
+    isothermal stratosphere at U(150, 230) K below which T does not fall;
+    q = q_s sigma^lambda exp(N(0, 0.2)) with q_s log-uniform [1e-7, 3e-2] and
+    lambda ~ U(1, 4) (q_s at the surface level); cloud cover one Gaussian
+    layer in sigma, amplitude U(0, 1) (none in 30% of columns), centre
+    U(0.2, 0.95), half-width U(0.05, 0.25).
     """
+    if profiles not in ("independent", "structured"):
+        raise ValueError(f"profiles must be 'independent' or 'structured', not {profiles!r}")
     rng = np.random.default_rng(seed)
     nlon = 2 * nlat
     nhor = nlat * nlon
@@ -102,11 +114,25 @@ def radiation_columns(nlat, nlev, seed=2, teff=False):
     ts = rng.uniform(150.0, 350.0, nhor)
     gam = rng.uniform(0.0, 9.0, nhor)
     zlev = -(287.0 * ts[None, :] / 9.80665) * np.log(sigma[:, None])
-    t = ts[None, :] - gam[None, :] * zlev / 1000.0 + rng.normal(0.0, 5.0, (nlev, nhor))
-    t = np.clip(t, 150.0, 350.0)
+    if profiles == "independent":
+        t = ts[None, :] - gam[None, :] * zlev / 1000.0 + rng.normal(0.0, 5.0, (nlev, nhor))
+        t = np.clip(t, 150.0, 350.0)
+        dq = np.exp(rng.uniform(np.log(1e-7), np.log(3e-2), (nlep, nhor)))
+        dcc = rng.uniform(0.0, 1.0, (nlep, nhor))
+    else:
+        t = ts[None, :] - gam[None, :] * zlev / 1000.0 + rng.normal(0.0, 1.0, (nlev, nhor))
+        t = np.clip(np.maximum(t, rng.uniform(150.0, 230.0, nhor)[None, :]), 150.0, 350.0)
+        qs = np.exp(rng.uniform(np.log(1e-7), np.log(3e-2), nhor))
+        lam = rng.uniform(1.0, 4.0, nhor)
+        dq = np.empty((nlep, nhor))
+        dq[:nlev] = qs[None, :] * sigma[:, None] ** lam[None, :] * np.exp(rng.normal(0.0, 0.2, (nlev, nhor)))
+        dq[nlev] = qs
+        amp = rng.uniform(0.0, 1.0, nhor) * (rng.uniform(0.0, 1.0, nhor) >= 0.3)
+        sc = rng.uniform(0.2, 0.95, nhor)
+        wd = rng.uniform(0.05, 0.25, nhor)
+        dcc = np.zeros((nlep, nhor))
+        dcc[:nlev] = amp[None, :] * np.exp(-((sigma[:, None] - sc[None, :]) / wd[None, :]) ** 2)
     dt = np.concatenate([t, ts[None, :]], axis=0)
-    dq = np.exp(rng.uniform(np.log(1e-7), np.log(3e-2), (nlep, nhor)))
-    dcc = rng.uniform(0.0, 1.0, (nlep, nhor))
     dcc[nlev] = 0.0
     dql = 0.1 * dq * dcc
     dp = np.exp(rng.uniform(np.log(1e4), np.log(1e6), nhor))

@@ -36,6 +36,29 @@ def chunk():
     return params, dev, X, Y, cols, out
 
 
+def test_features_match_numpy(chunk):
+    """exotx_surr_features against the feature list restated in numpy."""
+    params, dev, X, _, _, _ = chunk
+    c = {k: v.cpu().numpy() for k, v in dev.items()}
+    n = params.nhor
+    lq = np.log(np.maximum(c["dq"][:L + 1], 1e-12))
+    ref = np.concatenate([
+        c["dt"][:L + 1],
+        lq[:L] - lq[1:L + 1], lq[L:L + 1],
+        c["dcc"][:L],
+        np.log(np.maximum(c["dp"], 1.0))[None],
+        c["dalb"][None], c["gmu0"][None],
+        np.log(np.maximum(c["dqco2"][0], 1e-6))[None],
+        c["zsol"][0][None], c["zsol"][2][None],
+        c["sid"][np.arange(n) // params.nlon][None],
+    ]).T
+    assert ref.shape == (n, NIN)
+    np.testing.assert_allclose(X.double().cpu().numpy(), ref, rtol=2e-6, atol=5e-5)
+    # ln q on every level comes back from the gradients
+    got = SG.log_humidity(X, L).cpu().numpy()
+    np.testing.assert_allclose(got, lq[:L].T, rtol=0, atol=5e-4)
+
+
 @pytest.mark.parametrize("width,nhid,n", [(32, 2, 64), (256, 6, 256), (64, 2, 1100)])
 def test_forward_and_gradients_vs_oracle(width, nhid, n):
     from oracle import mlp_oracle as MO
