@@ -18,7 +18,6 @@ constexpr int MLP_MAX_LAYERS = 8;
 constexpr int SURR_TILE = 128;          // columns per tile (MMA M)
 constexpr int SURR_THREADS = 512;      // 4 warp groups x the 4 TMEM lane quarters
 constexpr int SURR_WIDTH = 256;         // hidden width of the tensor-core inference path
-constexpr int SURR_HALF = 128;          // hidden units per CTA of a cluster pair
 constexpr int SURR_KIN = 80;            // padded input features (nin <= 80)
 constexpr int SURR_NOUT = 32;           // padded outputs (nout <= 32)
 
@@ -256,46 +255,33 @@ __host__ __device__ inline int surr_layer_K(int l) { return l == 0 ? SURR_KIN : 
 __host__ __device__ inline int surr_layer_KC(int l) { return l == 0 ? SURR_KIN : 128; }
 
 template <typename T>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
+__global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
     extern __shared__ __align__(128) unsigned char sm[];
-    // a pair of CTAs (one cluster) shares each tile of 128 columns: CTA r builds the
-    // features of rows [64r, 64r + 64), computes the hidden units [128r, 128r + 128)
-    // of every hidden layer, and writes the outputs of its 64 rows.  Each CTA stores
-    // its BF16 activations into both CTAs' operand buffers; layers alternate between
-    // two buffers, so one cluster barrier per layer orders every exchange.
-    unsigned char *const abuf = sm;                 // 2 x (128 rows x 256 K, BF16 K-major: 64 KB)
-    unsigned char *wbuf = sm + 131072;              // this CTA's share of a layer's weights (64 KB)
-    uint64_t *bar_w = reinterpret_cast<uint64_t *>(sm + 196608);
+    unsigned char *abuf = sm;                       // 128 rows x 256 K, BF16 K-major (64 KB)
+    unsigned char *wbuf = sm + 65536;               // 2 chunks x 64 KB of layer weights
+    uint64_t *bar_w = reinterpret_cast<uint64_t *>(sm + 65536 + 131072);
     uint64_t *bar_mma = bar_w + 1;
     uint32_t *slot = reinterpret_cast<uint32_t *>(bar_w + 2);
-    int *flags = reinterpret_cast<int *>(bar_w + 3);   // 64 out-of-range flags (this CTA's rows)
-    __shared__ int fpart[8][64];                        // per feature-block group, before the OR
+    int *flags = reinterpret_cast<int *>(bar_w + 3);   // 128 out-of-range flags
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, grp = warp >> 2;
     const int row = quarter * 32 + lane;  // TMEM lane = column of the tile
     const int nhor = A.in.nhor, nl = A.nl;
     const int ntiles = (nhor + SURR_TILE - 1) / SURR_TILE;
-    const uint32_t rank = tc::cluster_rank(), peer = rank ^ 1u;
-    const int cid = blockIdx.x >> 1, ncl = gridDim.x >> 1;
-    const uint32_t pabuf = tc::peer_smem(abuf, peer);   // the same buffers in the peer CTA
-    const bool mine = (quarter >> 1) == (int)rank;      // this warp's TMEM rows are this CTA's outputs
-    if (warp == 0) tc::tmem_alloc(slot, 2 * SURR_HALF);   // two layer accumulators
-    // rows of layer l's weights this CTA multiplies: its half of a hidden layer, all of the output layer
-    auto layer_rows = [&](int l) { return l == nl - 1 ? SURR_NOUT : SURR_HALF; };
+    if (warp == 0) tc::tmem_alloc(slot, 2 * SURR_WIDTH);   // two layer accumulators
     uint32_t wissued = 0;   // weight loads issued (thread 0)
     auto issue_weights = [&](int l) {
-        const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l), Nl = layer_rows(l);
-        const int r0 = l == nl - 1 ? 0 : SURR_HALF * (int)rank;
-        const uint32_t cbytes = (uint32_t)Nl * KC * 2;
+        const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l);
+        const uint32_t cbytes = (uint32_t)N * KC * 2;
         wissued++;
         tc::mbar_arrive_expect_tx(bar_w, cbytes * (K / KC));
         for (int c = 0; c < K / KC; c++)
-            tc::bulk_g2s(wbuf + c * cbytes, A.tw + A.twoff[l] + ((size_t)c * N + r0) * KC * 2, cbytes, bar_w);
+            tc::bulk_g2s(wbuf + c * 65536, A.tw + A.twoff[l] + (size_t)c * cbytes, cbytes, bar_w);
     };
     if (tid == 0) {
         tc::mbar_init(bar_w, 1);
         tc::mbar_init(bar_mma, 1);
         tc::mbar_fence_init();
-        if (cid < ntiles) issue_weights(0);
+        if (blockIdx.x < ntiles) issue_weights(0);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -349,15 +335,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SURR_THREADS) k_surr
         ftab[f].src = src; ftab[f].kind = kd; ftab[f].cst = cv;
     }
     __syncthreads();
-    tc::cluster_sync();   // the peer has started before its shared memory is written
     uint32_t pw = 0, pm = 0;   // completed phases of the weight and MMA barriers
-    bool ok = true;            // the same on every thread of the CTA; false once a wait gave up
+    bool ok = true;  // cleared on every thread when a wait gives up
     // thread 0: MMAs of layer l over the 16-wide K steps [k0, k1) into the layer's
-    // accumulator (layers alternate between two TMEM regions); the layer's first
-    // issue waits for its weights and starts the accumulation; commit arrives on bar_mma
-    auto issue_mma = [&](int l, int k0, int k1, bool first, bool commit) -> bool {
-        const int K = surr_layer_K(l), KC = surr_layer_KC(l), Nl = layer_rows(l);
-        if (first) {
+    // accumulator (layers alternate between two 256-column TMEM regions); the
+    // first step waits for the layer's weights; commit arrives on bar_mma
+    auto issue_mma = [&](int l, int k0, int k1, bool commit) -> bool {
+        const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l);
+        if (k0 == 0) {
             if (!tc::mbar_wait(bar_w, pw & 1)) {
                 atomicExch(&g_surr_error, 1);
                 return false;
@@ -365,30 +350,29 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SURR_THREADS) k_surr
             pw++;
             tc::fence_after_sync();
         }
-        const uint32_t idesc = tc::idesc_bf16(SURR_TILE, Nl);
-        const uint64_t da = tc::smem_desc(abuf + (l & 1) * 65536, 128, (uint32_t)(K / 8) * 128);
+        const uint32_t idesc = tc::idesc_bf16(SURR_TILE, N);
+        const uint64_t da = tc::smem_desc(abuf, 128, (uint32_t)(K / 8) * 128);
         const uint64_t db = tc::smem_desc(wbuf, 128, (uint32_t)(KC / 8) * 128);
-        const uint32_t d = tmem + (uint32_t)((l & 1) * SURR_HALF);
+        const uint32_t d = tmem + (uint32_t)((l & 1) * SURR_WIDTH);
         for (int kc = k0; kc < k1; kc++) {
             const int c = (kc * 16) / KC, kin = (kc * 16) % KC;
-            tc::mma_bf16(d, tc::desc_add(da, kc * 256), tc::desc_add(db, c * Nl * KC * 2 + (kin / 8) * 128), idesc,
-                         !(first && kc == k0));
+            tc::mma_bf16(d, tc::desc_add(da, kc * 256), tc::desc_add(db, c * 65536 + (kin / 8) * 128), idesc, kc > 0);
         }
         if (commit) tc::mma_commit(bar_mma);
         return true;
     };
-    // every CTA runs the same tiles, layers and cluster barriers, whatever ok is
-    for (int tile = cid; tile < ntiles; tile += ncl) {
-        // features of this CTA's 64 rows: thread t builds the 8-input blocks t / 64 and
-        // t / 64 + 8 of row 64 rank + t % 64, normalised, as BF16, into both CTAs' layer-0 operand
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int col = tile * SURR_TILE + row;
+        const bool live = col < nhor;
+        if (grp == 0) flags[row] = 0;
+        __syncthreads();
+        // features: warp group g builds the 8-input blocks g, g+4, ... of its row,
+        // normalised, as BF16; the block's eight raw loads are issued together
         {
-            const int frow = SURR_HALF / 2 * (int)rank + (tid & 63), fb0 = tid >> 6;
-            const int col = tile * SURR_TILE + frow;
-            const bool live = col < nhor;
-            const int crow = col / A.in.nlon;   // latitude row, for the kind-5 feature
             int bad = 0;
+            const int crow = col / A.in.nlon;   // latitude row, for the kind-5 feature
 #pragma unroll 1
-            for (int g = fb0; g < SURR_KIN / 8; g += 8) {
+            for (int g = grp; g < SURR_KIN / 8; g += 4) {
                 const int f0 = 8 * g;
                 float raw[8], below[8];
 #pragma unroll
@@ -418,47 +402,37 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SURR_THREADS) k_surr
                     const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
                     w[i] = *reinterpret_cast<const uint32_t *>(&b2);
                 }
-                const uint4 u = make_uint4(w[0], w[1], w[2], w[3]);
-                const uint32_t off = tc::kmajor_off(frow, f0, SURR_KIN);
-                *reinterpret_cast<uint4 *>(abuf + off) = u;
-                tc::st_cluster_v4(pabuf + off, u);
+                *reinterpret_cast<uint4 *>(abuf + tc::kmajor_off(row, f0, SURR_KIN)) = make_uint4(w[0], w[1], w[2], w[3]);
             }
-            fpart[fb0][tid & 63] = bad;
+            if (bad) atomicOr(&flags[row], 1);
         }
-        tc::fence_proxy_async_cluster();
+        tc::fence_proxy_async();
         tc::fence_before_sync();
         __syncthreads();
-        if (tid < 64) {
-            int b = 0;
-#pragma unroll
-            for (int i = 0; i < 8; i++) b |= fpart[i][tid];
-            flags[tid] = b;
-        }
-        ok = __syncthreads_and(ok) != 0;
-        tc::cluster_sync();   // both halves of the layer-0 operand are in place
         tc::fence_after_sync();
-        if (tid == 0 && ok) ok = issue_mma(0, 0, SURR_KIN / 16, true, true);
+        // layer 0 (the input features) in one go; each hidden epilogue below
+        // issues the next layer's MMAs in two K halves, the first while the
+        // second half of the activations is still being written
+        if (tid == 0 && ok) ok = issue_mma(0, 0, SURR_KIN / 16, true);
         for (int l = 0; l < nl; l++) {
-            const uint32_t acc = tmem + (uint32_t)((l & 1) * SURR_HALF);
-            ok = __syncthreads_and(ok) != 0;
-            const bool mok = ok && __all_sync(0xffffffffu, tc::mbar_wait(bar_mma, pm & 1));
-            if (mok) pm++;
-            if (ok && !mok && lane == 0) atomicExch(&g_surr_error, 2);
-            ok = __syncthreads_and(mok) != 0;
+            const uint32_t acc = tmem + (uint32_t)((l & 1) * SURR_WIDTH);
+            const bool mok = __all_sync(0xffffffffu, tc::mbar_wait(bar_mma, pm & 1));
+            pm++;
+            if (!mok) { if (lane == 0) atomicExch(&g_surr_error, 2); ok = false; }
             tc::fence_after_sync();
             // the weight buffer is free: fetch the next layer (or the next tile's first)
-            if (tid == 0 && ok) {
+            if (tid == 0 && mok) {
                 if (l + 1 < nl) issue_weights(l + 1);
-                else if (tile + ncl < ntiles) issue_weights(0);
+                else if (tile + (int)gridDim.x < ntiles) issue_weights(0);
             }
+            if (!mok) break;
             if (l + 1 < nl) {
-                // hidden epilogue: bias + SiLU, BF16, into both CTAs' next operand; warp
-                // group g takes this CTA's hidden units [128 rank + 32g, 128 rank + 32g + 32)
+                // hidden epilogue: bias + SiLU, BF16, into the next layer's A operand;
+                // in half h warp group g takes columns [128h + 32g, 128h + 32g + 32)
                 const float *b = bias_s[l];
-                const int c0 = 32 * grp, k0 = SURR_HALF * (int)rank + c0;
-                unsigned char *dst = abuf + ((l + 1) & 1) * 65536;
-                const uint32_t pdst = pabuf + ((l + 1) & 1) * 65536;
-                if (ok) {
+#pragma unroll 1
+                for (int h = 0; h < 2; h++) {
+                    const int c0 = 128 * h + 32 * grp;
                     uint32_t r[32];
                     tc::tmem_ld32_nw(acc + lane_addr + (uint32_t)c0, r);
                     tc::tmem_wait_ld();
@@ -468,96 +442,81 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SURR_THREADS) k_surr
 #pragma unroll
                         for (int i = 0; i < 4; i++) {
                             const int c = 8 * q + 2 * i;
-                            const float2 bb = *reinterpret_cast<const float2 *>(b + k0 + c);
+                            const float2 bb = *reinterpret_cast<const float2 *>(b + c0 + c);
                             const float h0 = silu_fast(__uint_as_float(r[c]) + bb.x);
                             const float h1 = silu_fast(__uint_as_float(r[c + 1]) + bb.y);
                             const __nv_bfloat162 b2 = __floats2bfloat162_rn(h0, h1);
                             w[i] = *reinterpret_cast<const uint32_t *>(&b2);
                         }
-                        const uint4 u = make_uint4(w[0], w[1], w[2], w[3]);
-                        const uint32_t off = tc::kmajor_off(row, k0 + 8 * q, SURR_WIDTH);
-                        *reinterpret_cast<uint4 *>(dst + off) = u;
-                        tc::st_cluster_v4(pdst + off, u);
+                        *reinterpret_cast<uint4 *>(abuf + tc::kmajor_off(row, c0 + 8 * q, SURR_WIDTH)) =
+                            make_uint4(w[0], w[1], w[2], w[3]);
                     }
+                    tc::fence_proxy_async();
+                    tc::fence_before_sync();
+                    __syncthreads();
+                    tc::fence_after_sync();
+                    // K half h of the next layer's A operand is complete
+                    constexpr int KH = SURR_WIDTH / 32;   // 16-wide K steps per half
+                    if (tid == 0 && ok) ok = issue_mma(l + 1, KH * h, KH * h + KH, h == 1);
                 }
-                tc::fence_proxy_async_cluster();
-                tc::fence_before_sync();
-                __syncthreads();
-                tc::fence_after_sync();
-                // this CTA's K half of the next operand is complete: its MMAs start
-                // while the peer's half is still arriving
-                constexpr int KH = SURR_HALF / 16;   // 16-wide K steps per half
-                const int kl = KH * (int)rank, kr = KH * (int)peer;
-                if (tid == 0 && ok) ok = issue_mma(l + 1, kl, kl + KH, true, false);
-                ok = __syncthreads_and(ok) != 0;
-                tc::cluster_sync();
-                tc::fence_after_sync();
-                if (tid == 0 && ok) ok = issue_mma(l + 1, kr, kr + KH, false, true);
             } else {
-                // output epilogue (every CTA computed all outputs of the tile): the warps
-                // over this CTA's 64 rows de-normalise and write the in-range columns;
-                // warp group g writes the levels k = g (mod 4), group 0 the surface fluxes
-                const int col = tile * SURR_TILE + row;
-                const bool live = col < nhor;
-                if (ok && mine) {
-                    uint32_t r[32];
-                    tc::tmem_ld32_nw(acc + lane_addr, r);
-                    tc::tmem_wait_ld();
-                    const int flag = flags[row & 63];
-                    if (live && !flag) {
-                        const float *b = bias_s[l];
-                        const int L = A.in.L;
-                        const size_t n = (size_t)nhor;
-                        const float ps = (float)A.in.dp[col] * 1e-5f, adv = (float)A.in.adv;
-                        // this group's levels k = grp (mod 4): their humidities and heating
-                        // rates are read together before the updates
-                        constexpr int KMAX = SURR_NOUT / 4;
-                        T qk[KMAX], hk[KMAX];
+                // output epilogue: de-normalise and write the in-range columns; warp
+                // group g writes the levels k = g (mod 4), group 0 the surface fluxes
+                uint32_t r[32];
+                tc::tmem_ld32_nw(acc + lane_addr, r);
+                tc::tmem_wait_ld();
+                if (live && !flags[row]) {
+                    const float *b = bias_s[l];
+                    const int L = A.in.L;
+                    const size_t n = (size_t)nhor;
+                    const float ps = (float)A.in.dp[col] * 1e-5f, adv = (float)A.in.adv;
+                    // this group's levels k = grp (mod 4): their humidities and heating
+                    // rates are read together before the updates
+                    constexpr int KMAX = SURR_NOUT / 4;
+                    T qk[KMAX], hk[KMAX];
 #pragma unroll
-                        for (int j = 0; j < KMAX; j++) {
-                            const int o = grp + 4 * j;
-                            if (o < L && o < A.nout) {
-                                qk[j] = A.in.dq[(size_t)o * n + col];
-                                hk[j] = A.dtdt[(size_t)o * n + col];
-                            }
-                        }
-#pragma unroll
-                        for (int j = 0; j < KMAX; j++) {
-                            const int o = grp + 4 * j;
-                            if (o < L && o < A.nout) {
-                                // r[4j + grp] with constant register indices
-                                const uint32_t rv = grp == 0 ? r[4 * j] : grp == 1 ? r[4 * j + 1] : grp == 2 ? r[4 * j + 2] : r[4 * j + 3];
-                                const float y = (__uint_as_float(rv) + b[o]) * ys[o] + ym[o];
-                                A.dtdt[(size_t)o * n + col] = hk[j] + (T)__fdividef(y, 86400.f * ps * (1.f + adv * (float)qk[j]));
-                            }
-                        }
-                        if (grp == 0) {
-                            float f4[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                            for (int o = 0; o < SURR_NOUT; o++) {
-                                const int i = o - L;
-                                if (i < 0 || i > 3 || o >= A.nout) continue;
-                                const float y = (__uint_as_float(r[o]) + b[o]) * ys[o] + ym[o];
-                                if (i == 0) f4[0] = y; else if (i == 1) f4[1] = y; else if (i == 2) f4[2] = y; else f4[3] = y;
-                            }
-                            A.dfd[(size_t)L * n + col] = (T)f4[0];
-                            A.dfu[(size_t)L * n + col] = (T)f4[1];
-                            A.dftd[(size_t)L * n + col] = (T)f4[2];
-                            A.dftu[(size_t)L * n + col] = (T)f4[3];
-                            A.dswfl[(size_t)L * n + col] = (T)f4[0] + (T)f4[1];
-                            A.dlwfl[(size_t)L * n + col] = (T)f4[2] + (T)f4[3];
+                    for (int j = 0; j < KMAX; j++) {
+                        const int o = grp + 4 * j;
+                        if (o < L && o < A.nout) {
+                            qk[j] = A.in.dq[(size_t)o * n + col];
+                            hk[j] = A.dtdt[(size_t)o * n + col];
                         }
                     }
-                    if (live && flag && grp == 0) {
-                        const int idx = atomicAdd(A.fb, 1);
-                        A.fb[1 + idx] = col;
+#pragma unroll
+                    for (int j = 0; j < KMAX; j++) {
+                        const int o = grp + 4 * j;
+                        if (o < L && o < A.nout) {
+                            // r[4j + grp] with constant register indices
+                            const uint32_t rv = grp == 0 ? r[4 * j] : grp == 1 ? r[4 * j + 1] : grp == 2 ? r[4 * j + 2] : r[4 * j + 3];
+                            const float y = (__uint_as_float(rv) + b[o]) * ys[o] + ym[o];
+                            A.dtdt[(size_t)o * n + col] = hk[j] + (T)__fdividef(y, 86400.f * ps * (1.f + adv * (float)qk[j]));
+                        }
+                    }
+                    if (grp == 0) {
+                        float f4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                        for (int o = 0; o < SURR_NOUT; o++) {
+                            const int i = o - L;
+                            if (i < 0 || i > 3 || o >= A.nout) continue;
+                            const float y = (__uint_as_float(r[o]) + b[o]) * ys[o] + ym[o];
+                            if (i == 0) f4[0] = y; else if (i == 1) f4[1] = y; else if (i == 2) f4[2] = y; else f4[3] = y;
+                        }
+                        A.dfd[(size_t)L * n + col] = (T)f4[0];
+                        A.dfu[(size_t)L * n + col] = (T)f4[1];
+                        A.dftd[(size_t)L * n + col] = (T)f4[2];
+                        A.dftu[(size_t)L * n + col] = (T)f4[3];
+                        A.dswfl[(size_t)L * n + col] = (T)f4[0] + (T)f4[1];
+                        A.dlwfl[(size_t)L * n + col] = (T)f4[2] + (T)f4[3];
                     }
                 }
-                // both CTAs' output MMAs are done before the next tile's features
-                // overwrite the operands; TMEM and flags are reused
+                if (live && flags[row] && grp == 0) {
+                    const int idx = atomicAdd(A.fb, 1);
+                    A.fb[1 + idx] = col;
+                }
+            }
+            if (l + 1 == nl) {
                 tc::fence_before_sync();
-                ok = __syncthreads_and(ok) != 0;
-                tc::cluster_sync();
+                __syncthreads();  // TMEM and flags reused by the next tile
                 tc::fence_after_sync();
             }
         }
@@ -566,7 +525,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SURR_THREADS) k_surr
     if (tid == 0 && !ok && wissued > pw) tc::mbar_wait(bar_w, pw & 1);
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 2 * SURR_HALF);
+    if (warp == 0) tc::tmem_dealloc(tmem, 2 * SURR_WIDTH);
 }
 
 }  // namespace exotx
@@ -625,10 +584,10 @@ static exotx_status surr_launch(exotx_mlp net, const exotx_rad_params *p, int pr
     A.dtdt = (T *)io->dtdt; A.dfd = (T *)io->dfd; A.dfu = (T *)io->dfu; A.dftd = (T *)io->dftd;
     A.dftu = (T *)io->dftu; A.dswfl = (T *)io->dswfl; A.dlwfl = (T *)io->dlwfl;
     A.fb = net->fb;
-    const size_t smem = 196608 + 1024;   // two operand buffers, a weight buffer, barriers and flags
+    const size_t smem = 65536 + 131072 + 1024;
     EXOTX_CUDA(cudaFuncSetAttribute(k_surr_infer<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int ntiles = (p->nhor + SURR_TILE - 1) / SURR_TILE;
-    const int grid = 2 * std::min(ntiles, std::max(1, sm_count() / 2));   // CTA pairs (clusters of 2)
+    const int grid = std::min(ntiles, sm_count());
     cudaEvent_t ev = ktimer_start(EXOTX_K_SURROGATE, s);
     k_surr_infer<T><<<grid, SURR_THREADS, smem, s>>>(A);
     EXOTX_CHECK_LAUNCH();

@@ -194,3 +194,9 @@ def test_trained_network_beats_baselines():
           f"mean {mean_rms:.4f}; fallback {ev['fallback_fraction']:.4f}")
     assert ev["heating_rms_K_per_day"] < 0.5 * lin_rms
     assert ev["heating_rms_K_per_day"] < 0.2 * mean_rms
+    # the packaged network's bar on the evaluation columns (vertically coherent profiles)
+    assert ev["heating_rms_K_per_day"] < 0.4 and ev["fallback_fraction"] == 0.0
+    # columns drawn level by level lie outside the training profiles: the range test on
+    # the humidity gradients sends them to radstep
+    ind = SG.evaluate(net, L, nchunk=1, profiles="independent")
+    assert ind["fallback_fraction"] > 0.99 and ind["heating_rms_K_per_day"] < 0.05
