@@ -62,32 +62,6 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
 }
 // make generic-proxy shared-memory writes visible to the async proxy (MMA operands)
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// the same for writes into any CTA of the cluster (a peer's MMA operands)
-__device__ __forceinline__ void fence_proxy_async_cluster() {
-    asm volatile("fence.proxy.async.shared::cluster;" ::: "memory");
-}
-
-// ------------------------------------------------------------ clusters
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-// shared::cluster address of this CTA's shared-memory object p in CTA `rank` of the cluster
-__device__ __forceinline__ uint32_t peer_smem(const void *p, uint32_t rank) {
-    uint32_t a;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
-    return a;
-}
-__device__ __forceinline__ void st_cluster_v4(uint32_t addr, uint4 v) {
-    asm volatile("st.shared::cluster.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z),
-                 "r"(v.w)
-                 : "memory");
-}
-// every thread of every CTA in the cluster: writes before it are visible to reads after it
-__device__ __forceinline__ void cluster_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
 
 // -------------------------------------------------------------------- TMEM
 // whole warp: allocate ncols (power of two >= 32) columns; address written to *slot
