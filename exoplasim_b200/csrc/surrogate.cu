@@ -259,26 +259,29 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
     extern __shared__ __align__(128) unsigned char sm[];
     unsigned char *abuf = sm;                       // 128 rows x 256 K, BF16 K-major (64 KB)
     unsigned char *wbuf = sm + 65536;               // 2 chunks x 64 KB of layer weights
-    uint64_t *bar_w = reinterpret_cast<uint64_t *>(sm + 65536 + 131072);
-    uint64_t *bar_mma = bar_w + 1;
-    uint32_t *slot = reinterpret_cast<uint32_t *>(bar_w + 2);
-    int *flags = reinterpret_cast<int *>(bar_w + 3);   // 128 out-of-range flags
+    uint64_t *bar_w = reinterpret_cast<uint64_t *>(sm + 65536 + 131072);   // [2]: weight chunk c arrived
+    uint64_t *bar_mma = bar_w + 2;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar_w + 3);
+    int *flags = reinterpret_cast<int *>(bar_w + 4);   // 128 out-of-range flags
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, quarter = warp & 3, grp = warp >> 2;
     const int row = quarter * 32 + lane;  // TMEM lane = column of the tile
     const int nhor = A.in.nhor, nl = A.nl;
     const int ntiles = (nhor + SURR_TILE - 1) / SURR_TILE;
     if (warp == 0) tc::tmem_alloc(slot, 2 * SURR_WIDTH);   // two layer accumulators
-    uint32_t wissued = 0;   // weight loads issued (thread 0)
+    uint32_t wi0 = 0, wi1 = 0;   // weight chunks 0 and 1 issued (thread 0)
     auto issue_weights = [&](int l) {
         const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l);
         const uint32_t cbytes = (uint32_t)N * KC * 2;
-        wissued++;
-        tc::mbar_arrive_expect_tx(bar_w, cbytes * (K / KC));
-        for (int c = 0; c < K / KC; c++)
-            tc::bulk_g2s(wbuf + c * 65536, A.tw + A.twoff[l] + (size_t)c * cbytes, cbytes, bar_w);
+        // one barrier per K chunk: the MMAs over a chunk start as soon as it is in
+        for (int c = 0; c < K / KC; c++) {
+            (c == 0 ? wi0 : wi1)++;
+            tc::mbar_arrive_expect_tx(bar_w + c, cbytes);
+            tc::bulk_g2s(wbuf + c * 65536, A.tw + A.twoff[l] + (size_t)c * cbytes, cbytes, bar_w + c);
+        }
     };
     if (tid == 0) {
         tc::mbar_init(bar_w, 1);
+        tc::mbar_init(bar_w + 1, 1);
         tc::mbar_init(bar_mma, 1);
         tc::mbar_fence_init();
         if (blockIdx.x < ntiles) issue_weights(0);
@@ -335,19 +338,21 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
         ftab[f].src = src; ftab[f].kind = kd; ftab[f].cst = cv;
     }
     __syncthreads();
-    uint32_t pw = 0, pm = 0;   // completed phases of the weight and MMA barriers
+    uint32_t pw0 = 0, pw1 = 0, pm = 0;   // completed phases of the two weight barriers and the MMA barrier
     bool ok = true;  // cleared on every thread when a wait gives up
-    // thread 0: MMAs of layer l over the 16-wide K steps [k0, k1) into the layer's
-    // accumulator (layers alternate between two 256-column TMEM regions); the
-    // first step waits for the layer's weights; commit arrives on bar_mma
+    // thread 0: MMAs of layer l over the 16-wide K steps [k0, k1) (within one weight
+    // chunk) into the layer's accumulator (layers alternate between two 256-column
+    // TMEM regions); a call that starts a chunk waits for it; commit arrives on bar_mma
     auto issue_mma = [&](int l, int k0, int k1, bool commit) -> bool {
         const int N = surr_layer_N(l, nl), K = surr_layer_K(l), KC = surr_layer_KC(l);
-        if (k0 == 0) {
-            if (!tc::mbar_wait(bar_w, pw & 1)) {
+        if ((k0 * 16) % KC == 0) {
+            const int c = (k0 * 16) / KC;
+            uint32_t &ph = c == 0 ? pw0 : pw1;
+            if (!tc::mbar_wait(bar_w + c, ph & 1)) {
                 atomicExch(&g_surr_error, 1);
                 return false;
             }
-            pw++;
+            ph++;
             tc::fence_after_sync();
         }
         const uint32_t idesc = tc::idesc_bf16(SURR_TILE, N);
@@ -522,7 +527,10 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
         }
     }
     // after a timeout, a weight load still in flight lands before the block leaves
-    if (tid == 0 && !ok && wissued > pw) tc::mbar_wait(bar_w, pw & 1);
+    if (tid == 0 && !ok) {
+        if (wi0 > pw0) tc::mbar_wait(bar_w, pw0 & 1);
+        if (wi1 > pw1) tc::mbar_wait(bar_w + 1, pw1 & 1);
+    }
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(tmem, 2 * SURR_WIDTH);
