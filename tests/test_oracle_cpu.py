@@ -142,6 +142,32 @@ def test_radstep_energy_closure(oracle):
     assert relerr(heat, out["dflux"][0] - out["dflux"][10]) < 1e-12
 
 
+def test_structured_columns(oracle):
+    """The vertically coherent columns the surrogate is trained on: the same
+    ranges as the level-by-level columns, humidity log-gradients bounded (the
+    level-by-level columns reach jumps of ~17), one cloud layer, and radstep's
+    energy closure on them."""
+    from exoplasim_b200 import synthetic as S
+    nlev = 10
+    cols, g = S.radiation_columns(8, nlev, seed=13, profiles="structured")
+    ind, _ = S.radiation_columns(8, nlev, seed=13)
+    assert {k: v.shape for k, v in cols.items()} == {k: v.shape for k, v in ind.items()}
+    assert cols["dt"].min() >= 150.0 and cols["dt"].max() <= 350.0
+    assert cols["dq"].min() > 0 and cols["dq"][nlev].max() <= 3e-2
+    assert cols["dcc"].min() >= 0 and cols["dcc"].max() <= 1 and np.all(cols["dcc"][nlev] == 0)
+    assert cols["dp"].min() >= 1e4 and cols["dp"].max() <= 1e6
+    grad = np.abs(np.diff(np.log(cols["dq"]), axis=0))
+    assert grad.max() < 12 < np.abs(np.diff(np.log(ind["dq"]), axis=0)).max()
+    p = oracle.radpar(nlev, g["nhor"], g["nlon"], g["sigma"], g["sigmah"], g["dsigma"], nsol=0)
+    out = oracle.radstep(p, cols["sid"], cols["cola"], cols)
+    ds = np.array([p.dsigma[i] for i in range(nlev)])[:, None]
+    cp = p.acpd * (1 + p.adv * cols["dq"][:nlev])
+    heat = np.sum(out["dtdt"] * ds * cols["dp"][None, :] * cp / p.ga, axis=0)
+    assert relerr(heat, out["dflux"][0] - out["dflux"][nlev]) < 1e-12
+    with pytest.raises(ValueError):
+        S.radiation_columns(8, nlev, profiles="smooth")
+
+
 def test_radstep_transparent_isothermal_lw(oracle):
     # no absorbers, no clouds, isothermal black surface-like column: the
     # longwave downward flux at the top is zero and the upward flux at the
