@@ -48,12 +48,8 @@ namespace exotx {
 
 // ------------------------------------------------------------ features
 // Raw features of one column (L levels), in this order:
-//   T(k) k<L, T surface, ln q(k) - ln q(k+1) k<L, ln q(L), cc(k) k<L, ln ps,
-//   albedo, cos zenith, ln CO2 (ppmv), zsolar1, rcoeff, sin(latitude)
-//                                                           -> 3L + 9 values
-// The humidity enters as its vertical log-gradients: the same information as
-// ln q on every level, but the range test on them also rejects columns whose
-// humidity profile has a shape the training columns never had.
+//   T(k) k<L, T surface, ln q(k) k<=L, cc(k) k<L, ln ps, albedo, cos zenith,
+//   ln CO2 (ppmv), zsolar1, rcoeff, sin(latitude)          -> 3L + 9 values
 // Targets: per level the heating rate (K/day) times (ps / 1e5 Pa) (1 + ADV q),
 // which removes the exact 1 / (ps (1 + ADV q)) factor of radstep's heating
 // (radmod.f90:1100-1110) from what the network learns; then SW down, SW up,
@@ -75,10 +71,7 @@ __device__ __forceinline__ float surr_feature(const SurrIn<T> &in, int col, int 
     const size_t n = (size_t)in.nhor;
     if (f < L + 1) return (float)in.dt[(size_t)f * n + col];
     f -= L + 1;
-    if (f < L)
-        return surr_log<FAST>(fmaxf((float)in.dq[(size_t)f * n + col], 1e-12f)) -
-               surr_log<FAST>(fmaxf((float)in.dq[(size_t)(f + 1) * n + col], 1e-12f));
-    if (f == L) return surr_log<FAST>(fmaxf((float)in.dq[(size_t)f * n + col], 1e-12f));
+    if (f < L + 1) return surr_log<FAST>(fmaxf((float)in.dq[(size_t)f * n + col], 1e-12f));
     f -= L + 1;
     if (f < L) return (float)in.dcc[(size_t)f * n + col];
     f -= L;
@@ -295,8 +288,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
     const float *ym = A.norm + 4 * A.nin, *ys = ym + A.nout;
     // per input feature: source array (read at the column, or at its latitude
     // row for kind 5), transform kind (0 none, 1-3 log with floors 1e-12, 1,
-    // 1e-6, 6 the log-ratio of the value to the one a level below with floor
-    // 1e-12, -1 a constant), the constant, and 1 / the normalisation scale
+    // 1e-6, -1 a constant), the constant, and 1 / the normalisation scale
     struct __align__(16) Feat {
         const T *src;
         int kind;
@@ -316,7 +308,7 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
         float cv = 0.f;
         if (f < A.nin) {
             if (f < L + 1) { src = A.in.dt + (size_t)f * n; kd = 0; }
-            else if (f < 2 * L + 2) { src = A.in.dq + (size_t)(f - L - 1) * n; kd = f < 2 * L + 1 ? 6 : 1; }
+            else if (f < 2 * L + 2) { src = A.in.dq + (size_t)(f - L - 1) * n; kd = 1; }
             else if (f < 3 * L + 2) { src = A.in.dcc + (size_t)(f - 2 * L - 2) * n; kd = 0; }
             else {
                 switch (f - 3 * L - 2) {
@@ -379,14 +371,12 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
 #pragma unroll 1
             for (int g = grp; g < SURR_KIN / 8; g += 4) {
                 const int f0 = 8 * g;
-                float raw[8], below[8];
+                float raw[8];
 #pragma unroll
                 for (int e = 0; e < 8; e++) {
                     const Feat &F = ftab[f0 + e];
                     raw[e] = F.cst;
-                    below[e] = 1.f;
                     if (live && F.kind >= 0) raw[e] = (float)F.src[F.kind == 5 ? crow : col];
-                    if (live && F.kind == 6) below[e] = (float)F.src[(size_t)nhor + col];
                 }
                 float v[8];
 #pragma unroll
@@ -395,7 +385,6 @@ __global__ void __launch_bounds__(SURR_THREADS) k_surr_infer(SurrArgs<T> A) {
                     const Feat &F = ftab[f];
                     float x = raw[e];
                     if (F.kind == 1) x = __logf(fmaxf(x, 1e-12f));
-                    else if (F.kind == 6) x = __logf(fmaxf(x, 1e-12f)) - __logf(fmaxf(below[e], 1e-12f));
                     else if (F.kind == 2) x = __logf(fmaxf(x, 1.f));
                     else if (F.kind == 3) x = __logf(fmaxf(x, 1e-6f));
                     if (live && f < A.nin) bad |= (x < F.lo) | (x > F.hi) | (x != x);
